@@ -1,0 +1,70 @@
+"""Builds the in-tree shared library libbubble_gw_c.so (C ABI + sm_100a kernels).
+
+    python -m gw_fopt_b200.build [--force] [--ptxas-info]
+
+The library is compiled in place next to this file so that it travels with
+the repository; nothing is installed into site-packages.
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+LIB_NAME = "libbubble_gw_c.so"
+LIB_PATH = os.path.join(HERE, LIB_NAME)
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", "nvcc"):
+        if cand and (os.path.isabs(cand) and os.path.exists(cand) or not os.path.isabs(cand)):
+            return cand
+    return "nvcc"
+
+
+def sources():
+    return sorted(glob.glob(os.path.join(CSRC, "*.cpp")) + glob.glob(os.path.join(CSRC, "*.cu")))
+
+
+def _deps():
+    return sources() + sorted(glob.glob(os.path.join(CSRC, "*.h")) + glob.glob(os.path.join(CSRC, "*.cuh"))
+                              + glob.glob(os.path.join(ROOT, "include", "*.h")))
+
+
+def needs_build() -> bool:
+    if not os.path.exists(LIB_PATH):
+        return True
+    t = os.path.getmtime(LIB_PATH)
+    return any(os.path.getmtime(p) > t for p in _deps())
+
+
+def build(force: bool = False, ptxas_info: bool = False, verbose: bool = False) -> str:
+    if not force and not needs_build() and not ptxas_info:
+        return LIB_PATH
+    cmd = [_nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo",
+           "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math", "-shared",
+           "-I", os.path.join(ROOT, "include"), "-o", LIB_PATH, *sources()]
+    if ptxas_info:
+        cmd.insert(1, "-Xptxas=-v")
+    if verbose:
+        print(" ".join(cmd), file=sys.stderr)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
+    if ptxas_info:
+        sys.stderr.write(res.stderr)
+    return LIB_PATH
+
+
+if __name__ == "__main__":
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--ptxas-info", action="store_true")
+    args = ap.parse_args()
+    print(build(force=args.force, ptxas_info=args.ptxas_info, verbose=True))

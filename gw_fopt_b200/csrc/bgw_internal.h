@@ -1,0 +1,97 @@
+// Internal interfaces shared by the C ABI (capi.cpp), the lattice geometry
+// (lattice.cpp) and the device pipeline (pipeline.cu).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/bubble_gw.h"
+#include "../../include/bubble_gw_b200.h"
+
+namespace bgw {
+
+// Raised inside the library; converted to BGW_STATUS_CALCULATION_ERROR plus
+// the message by the C ABI wrapper (rust/c-bubble-gw/src/lib.rs:119-134).
+struct Error {
+    std::string msg;
+    bool index_error = false;  // GeneralizedBulkFlowError::InvalidIndex
+};
+
+// Rust's `Display` for f64: shortest round-trip digits, positional notation,
+// no trailing ".0" ("1", "0.5", "-0", "inf", "NaN").
+std::string rust_f64(double x);
+
+// Everything the device pipeline needs for one spectrum call.  Host arrays
+// are owned by the caller of run_spectrum.
+struct SpectrumJob {
+    // bubbles: interior then exterior, (n_tot, 4) rows (t, x, y, z)
+    const double* bubbles = nullptr;
+    size_t n_int = 0, n_tot = 0;
+    // angular grid (generalized_bulk_flow.rs:221-238): cos(theta) rows,
+    // phi columns, direction table (n_cos*n_phi, 4) = (1, sx, sy, c)
+    size_t n_cos = 0, n_phi = 0;
+    const double* cos_thetax = nullptr;
+    const double* dirs = nullptr;
+    const double* sin2phi = nullptr;  // sin(2 phi_j)
+    const double* cos2phi = nullptr;  // cos(2 phi_j)
+    // scaling functions
+    size_t n_sets = 0, n_terms = 0;
+    const double* coeffs = nullptr;
+    const double* powers = nullptr;
+    bool has_damping = false;
+    double damping = 0.0;
+    // time grid
+    size_t n_t = 0;
+    const double* t_arr = nullptr;
+    const double* cutoff = nullptr;  // cutoff weight at each t
+    double dt = 0.0;
+    // frequencies
+    size_t n_w = 0;
+    const double* w = nullptr;
+    // radiating bubbles (interior indices, duplicates allowed)
+    const uint32_t* sel = nullptr;
+    size_t n_sel = 0;
+    // k-hat rotations, (K, 9) row-major; nullptr = the unrotated frame (K = 1)
+    const double* rot = nullptr;
+    size_t n_k = 1;
+    BgwxKernel kernel = BGWX_KERNEL_FP64_DIRECT;
+};
+
+struct MaskJob {
+    const double* bubbles = nullptr;
+    size_t n_int = 0, n_tot = 0;
+    size_t n_cos = 0, n_phi = 0;
+    const double* dirs = nullptr;
+    const uint32_t* sel = nullptr;
+    size_t n_sel = 0;
+};
+
+// Device state owned by one handle (one CUDA stream, grow-only buffers).
+struct Device;
+Device* device_create();  // throws Error when no CUDA device is usable
+void device_destroy(Device*);
+
+// Runs the spectrum; out: (n_k, 2, n_sets, n_w) complex as interleaved
+// doubles (host memory).  Throws Error.
+void run_spectrum(Device* dev, const SpectrumJob& job, double* out, BgwxTimings* timings);
+
+// First-collider codes and delays for the selected bubbles at the
+// unrotated frame.  out_codes (n_sel, n_cos*n_phi) int32; out_tau may be null.
+void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_tau, BgwxTimings* timings);
+
+int device_count();
+
+// Lattice geometry (lattice.cpp).
+void lattice_contains(BgwxLatticeKind kind, const double* params, const double* pts, size_t n, uint8_t* out);
+std::vector<double> lattice_exterior(BgwxLatticeKind kind, const double* params, BgwxBoundaryCondition bc,
+                                     const double* interior, size_t n);
+void check_causality(const double* interior, size_t n_int, const double* exterior, size_t n_ext);
+
+// Host reference-arithmetic helpers (no FMA contraction in this library's
+// host translation units: compiled with -ffp-contract=off).
+std::vector<double> linspace(double a, double b, size_t n);
+void rotation_for_khat(double kx, double ky, double kz, double* R);
+
+}  // namespace bgw

@@ -1,0 +1,452 @@
+// The C ABI: reference-compatible bgw_* entry points (rust/c-bubble-gw/src/lib.rs)
+// and the bgwx_* extensions.  Host-side validation and grids live here; all
+// numerical work on the path runs on the GPU (pipeline.cu).  There is no CPU
+// fallback: without a usable CUDA device the compute calls fail with
+// BGW_STATUS_CALCULATION_ERROR.
+
+#include <cmath>
+#include <cstring>
+#include <exception>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "bgw_internal.h"
+
+#define BGW_VERSION_STRING "0.1.0+b200"
+
+using bgw::Error;
+
+// Opaque handle (rust/c-bubble-gw/src/lib.rs:100-102 holds a
+// GeneralizedBulkFlow<EmptyLattice>; generalized_bulk_flow.rs:65-80).
+struct bgw_generalized_bulk_flow {
+    std::vector<double> bubbles;  // interior rows then exterior rows, (n, 4)
+    size_t n_int = 0, n_ext = 0;
+    bool has_res = false;
+    bool precompute = false;
+    size_t n_cos = 0, n_phi = 0;
+    std::vector<double> cos_thetax, phix, dirs, sin2phi, cos2phi;
+    // generalized_bulk_flow.rs:98-99 defaults: coefficients [[1.0]], powers [[3.0]]
+    size_t n_sets = 1, n_terms = 1;
+    std::vector<double> coeffs{1.0}, powers{3.0};
+    bool has_damping = false;
+    double damping = 0.0;
+    size_t num_threads = 1;
+    BgwxKernel kernel = BGWX_KERNEL_FP64_DIRECT;
+    bgw::Device* dev = nullptr;
+    BgwxTimings timings{};
+    ~bgw_generalized_bulk_flow() {
+        if (dev) bgw::device_destroy(dev);
+    }
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+void set_last_error(std::string m) {
+    for (auto& ch : m)
+        if (ch == '\0') ch = ' ';
+    g_last_error = std::move(m);
+}
+
+// rust/c-bubble-gw/src/lib.rs:119-134: Ok -> clear; Err -> CalculationError.
+template <class F>
+BgwStatus run_ffi(F&& f) {
+    try {
+        f();
+        g_last_error.clear();
+        return BGW_STATUS_OK;
+    } catch (const Error& e) {
+        set_last_error(e.msg);
+        return BGW_STATUS_CALCULATION_ERROR;
+    } catch (const std::bad_alloc&) {
+        set_last_error("memory allocation failed");
+        return BGW_STATUS_CALCULATION_ERROR;
+    } catch (const std::exception& e) {
+        set_last_error(std::string("internal error crossed the C ABI boundary: ") + e.what());
+        return BGW_STATUS_PANIC;
+    } catch (...) {
+        set_last_error("internal error crossed the C ABI boundary");
+        return BGW_STATUS_PANIC;
+    }
+}
+
+// rust/c-bubble-gw/src/lib.rs:140-148: a zero-length slice may be NULL.
+template <class T>
+const T* slice(const T* p, size_t len, const char* name) {
+    if (len == 0) return nullptr;
+    if (!p) throw Error{std::string(name) + " must not be null"};
+    return p;
+}
+
+size_t checked_mul(size_t a, size_t b, const char* name) {
+    if (a != 0 && b > (size_t)-1 / a) throw Error{std::string(name) + " length overflow"};
+    return a * b;
+}
+
+bgw_generalized_bulk_flow* handle(bgw_generalized_bulk_flow* h) {
+    if (!h) throw Error{"bulk_flow must not be null"};
+    return h;
+}
+
+bgw_generalized_bulk_flow* make_handle(const double* interior, size_t n_int, const double* exterior, size_t n_ext,
+                                       bool validate) {
+    size_t li = checked_mul(n_int, 4, "interior bubbles");
+    size_t le = checked_mul(n_ext, 4, "exterior bubbles");
+    const double* pi = slice(interior, li, "bubbles_interior");
+    const double* pe = slice(exterior, le, "bubbles_exterior");
+    if (validate) bgw::check_causality(pi, n_int, pe, n_ext);
+    auto* h = new bgw_generalized_bulk_flow();
+    h->bubbles.resize(li + le);
+    if (li) std::memcpy(h->bubbles.data(), pi, li * sizeof(double));
+    if (le) std::memcpy(h->bubbles.data() + li, pe, le * sizeof(double));
+    h->n_int = n_int;
+    h->n_ext = n_ext;
+    return h;
+}
+
+void require_resolution(const bgw_generalized_bulk_flow* h) {
+    if (!h->has_res) throw Error{"Field 'n_cos_thetax' is not initialized"};
+}
+
+bgw::Device* device(bgw_generalized_bulk_flow* h) {
+    if (!h->dev) h->dev = bgw::device_create();
+    return h->dev;
+}
+
+// time_cutoff.rs:15-43.
+struct Cutoff {
+    bool exponential = false;
+    double t_cut = 0, inv_t_0_sq = 0;
+    double eval(double t) const {
+        if (!exponential || t < t_cut) return 1.0;
+        double d = t - t_cut;
+        return std::exp(-(d * d) * inv_t_0_sq);
+    }
+};
+
+Cutoff make_cutoff(const BgwTimeCutoffConfig& c) {
+    Cutoff k;
+    if (c.kind == BGW_TIME_CUTOFF_KIND_UNIT) return k;
+    if (c.kind != BGW_TIME_CUTOFF_KIND_EXPONENTIAL) throw Error{"invalid time cutoff kind"};
+    double rc = std::isnan(c.ratio_t_cut) ? 0.999999999 : c.ratio_t_cut;
+    double r0 = std::isnan(c.ratio_t_0) ? 0.25 : c.ratio_t_0;
+    k.exponential = true;
+    k.t_cut = rc * c.smax;
+    double t0 = r0 * (c.smax - k.t_cut);
+    k.inv_t_0_sq = 1.0 / (t0 * t0);
+    return k;
+}
+
+// Shared body of compute_c_integral (generalized_bulk_flow.rs:928-984) for
+// n_k frames; rot == nullptr means the unrotated frame.
+void compute_common(bgw_generalized_bulk_flow* h, const double* w_arr, size_t n_w, bool has_t_begin, double t_begin,
+                    double t_end, size_t n_t, const size_t* selected, size_t n_selected, bool has_selected,
+                    const BgwTimeCutoffConfig& cutoff, const double* rot, size_t n_k, BgwComplex64* out,
+                    size_t out_len) {
+    const double* w = slice(w_arr, n_w, "w_arr");
+    Cutoff cut = make_cutoff(cutoff);
+    size_t S = h->n_sets;
+    size_t expected = checked_mul(checked_mul(checked_mul(n_k, 2, "out"), S, "out"), n_w, "out");
+    if (n_t < 2) throw Error{"Invalid resolution: n_t must be >= 2 for integration"};
+    std::vector<uint32_t> ids;
+    if (has_selected) {
+        const size_t* sel = slice(selected, n_selected, "selected_bubbles");
+        for (size_t q = 0; q < n_selected; ++q) {
+            if (sel[q] >= h->n_int) {
+                Error e{"Index " + std::to_string(sel[q]) + " out of bounds for max " + std::to_string(h->n_int)};
+                e.index_error = true;
+                throw e;
+            }
+            ids.push_back((uint32_t)sel[q]);
+        }
+    } else {
+        for (size_t a = 0; a < h->n_int; ++a) ids.push_back((uint32_t)a);
+    }
+    std::vector<double> result(2 * expected, 0.0);
+    h->timings = BgwxTimings{};
+    if (!ids.empty()) {
+        double tb = has_t_begin ? t_begin : 0.0;
+        if (tb > t_end)
+            throw Error{"Invalid time range: t_begin=" + bgw::rust_f64(tb) + " > t_end=" + bgw::rust_f64(t_end)};
+        require_resolution(h);
+        if (S > 0 && n_w > 0) {
+            std::vector<double> t_arr = bgw::linspace(tb, t_end, n_t);
+            std::vector<double> cw(n_t);
+            for (size_t k = 0; k < n_t; ++k) cw[k] = cut.eval(t_arr[k]);
+            bgw::SpectrumJob job;
+            job.bubbles = h->bubbles.data();
+            job.n_int = h->n_int;
+            job.n_tot = h->n_int + h->n_ext;
+            job.n_cos = h->n_cos;
+            job.n_phi = h->n_phi;
+            job.cos_thetax = h->cos_thetax.data();
+            job.dirs = h->dirs.data();
+            job.sin2phi = h->sin2phi.data();
+            job.cos2phi = h->cos2phi.data();
+            job.n_sets = S;
+            job.n_terms = h->n_terms;
+            job.coeffs = h->coeffs.data();
+            job.powers = h->powers.data();
+            job.has_damping = h->has_damping;
+            job.damping = h->damping;
+            job.n_t = n_t;
+            job.t_arr = t_arr.data();
+            job.cutoff = cw.data();
+            job.dt = t_arr[1] - t_arr[0];
+            job.n_w = n_w;
+            job.w = w;
+            job.sel = ids.data();
+            job.n_sel = ids.size();
+            job.rot = rot;
+            job.n_k = n_k;
+            job.kernel = h->kernel;
+            bgw::run_spectrum(device(h), job, result.data(), &h->timings);
+        }
+    }
+    if (out_len != expected)
+        throw Error{"out_len=" + std::to_string(out_len) + " does not match expected length " +
+                    std::to_string(expected)};
+    BgwComplex64* o = const_cast<BgwComplex64*>(slice(out, out_len, "out"));
+    for (size_t q = 0; q < expected; ++q) o[q] = BgwComplex64{result[2 * q], result[2 * q + 1]};
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* bgw_version(void) { return BGW_VERSION_STRING; }
+
+const char* bgw_last_error_message(void) { return g_last_error.c_str(); }
+
+BgwStatus bgw_generalized_bulk_flow_empty_lattice_new(bgw_generalized_bulk_flow** out, const double* bubbles_interior,
+                                                      size_t n_interior, const double* bubbles_exterior,
+                                                      size_t n_exterior) {
+    if (!out) {
+        set_last_error("out must not be null");
+        return BGW_STATUS_NULL_POINTER;
+    }
+    *out = nullptr;
+    return run_ffi([&] { *out = make_handle(bubbles_interior, n_interior, bubbles_exterior, n_exterior, true); });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_new_unchecked(bgw_generalized_bulk_flow** out, const double* interior,
+                                                   size_t n_interior, const double* exterior, size_t n_exterior) {
+    if (!out) {
+        set_last_error("out must not be null");
+        return BGW_STATUS_NULL_POINTER;
+    }
+    *out = nullptr;
+    return run_ffi([&] { *out = make_handle(interior, n_interior, exterior, n_exterior, false); });
+}
+
+void bgw_generalized_bulk_flow_free(bgw_generalized_bulk_flow* bulk_flow) { delete bulk_flow; }
+
+BgwStatus bgw_generalized_bulk_flow_set_num_threads(bgw_generalized_bulk_flow* bulk_flow, size_t num_threads) {
+    return run_ffi([&] {
+        if (num_threads == 0) throw Error{"num_threads must be > 0"};
+        handle(bulk_flow)->num_threads = num_threads;
+    });
+}
+
+// generalized_bulk_flow.rs:208-270.  The direction table uses glibc sin/cos
+// on the host so that it is bitwise the reference's.
+BgwStatus bgw_generalized_bulk_flow_set_resolution(bgw_generalized_bulk_flow* bulk_flow, size_t n_cos_thetax,
+                                                   size_t n_phix, bool precompute_first_bubbles) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        if (n_cos_thetax < 2 || n_phix < 2)
+            throw Error{"Invalid resolution: Angular resolutions must be greater than one"};
+        h->n_cos = n_cos_thetax;
+        h->n_phi = n_phix;
+        h->cos_thetax = bgw::linspace(-1.0, 1.0, n_cos_thetax);
+        h->phix = bgw::linspace(0.0, 2.0 * M_PI, n_phix);
+        h->dirs.assign(4 * n_cos_thetax * n_phix, 0.0);
+        for (size_t i = 0; i < n_cos_thetax; ++i) {
+            double c = h->cos_thetax[i];
+            double s = std::fabs(std::sqrt(1.0 - c * c));
+            for (size_t j = 0; j < n_phix; ++j) {
+                double phi = h->phix[j];
+                double sp = std::sin(phi), cp = std::cos(phi);
+                double* d = &h->dirs[4 * (i * n_phix + j)];
+                d[0] = 1.0;
+                d[1] = s * cp;
+                d[2] = s * sp;
+                d[3] = c;
+            }
+        }
+        h->sin2phi.resize(n_phix);
+        h->cos2phi.resize(n_phix);
+        for (size_t j = 0; j < n_phix; ++j) {
+            h->sin2phi[j] = std::sin(2.0 * h->phix[j]);
+            h->cos2phi[j] = std::cos(2.0 * h->phix[j]);
+        }
+        h->precompute = precompute_first_bubbles;
+        h->has_res = true;
+    });
+}
+
+BgwStatus bgw_generalized_bulk_flow_set_gradient_scaling_params(bgw_generalized_bulk_flow* bulk_flow,
+                                                                const double* coefficients, const double* powers,
+                                                                size_t n_sets, size_t n_terms,
+                                                                double damping_width) {
+    // rust/c-bubble-gw/src/lib.rs:465-494: chunks(n_terms) panics for n_terms == 0.
+    if (n_terms == 0) {
+        set_last_error("internal error crossed the C ABI boundary: chunk size must be non-zero");
+        return BGW_STATUS_PANIC;
+    }
+    return run_ffi([&] {
+        size_t len = checked_mul(n_sets, n_terms, "gradient scaling");
+        const double* c = slice(coefficients, len, "coefficients");
+        const double* p = slice(powers, len, "powers");
+        auto* h = handle(bulk_flow);
+        h->n_sets = n_sets;
+        h->n_terms = n_sets ? n_terms : 0;
+        h->coeffs.assign(c, c + len);
+        h->powers.assign(p, p + len);
+        h->has_damping = !std::isnan(damping_width);
+        h->damping = damping_width;
+    });
+}
+
+BgwStatus bgw_generalized_bulk_flow_compute_c_integral(bgw_generalized_bulk_flow* bulk_flow, const double* w_arr,
+                                                       size_t n_w, bool has_t_begin, double t_begin, double t_end,
+                                                       size_t n_t, const size_t* selected_bubbles,
+                                                       size_t n_selected_bubbles, BgwTimeCutoffConfig time_cutoff,
+                                                       BgwComplex64* out, size_t out_len) {
+    return run_ffi([&] {
+        compute_common(handle(bulk_flow), w_arr, n_w, has_t_begin, t_begin, t_end, n_t, selected_bubbles,
+                       n_selected_bubbles, selected_bubbles != nullptr, time_cutoff, nullptr, 1, out, out_len);
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_compute_c_integral_khat(bgw_generalized_bulk_flow* bulk_flow,
+                                                             const double* w_arr, size_t n_w, bool has_t_begin,
+                                                             double t_begin, double t_end, size_t n_t,
+                                                             const double* khat, size_t n_khat,
+                                                             const size_t* selected_bubbles,
+                                                             size_t n_selected_bubbles,
+                                                             BgwTimeCutoffConfig time_cutoff, BgwComplex64* out,
+                                                             size_t out_len) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        const double* k = slice(khat, checked_mul(n_khat, 3, "khat"), "khat");
+        std::vector<double> rot(9 * n_khat);
+        for (size_t q = 0; q < n_khat; ++q) {
+            double kx = k[3 * q], ky = k[3 * q + 1], kz = k[3 * q + 2];
+            double n2 = kx * kx + ky * ky + kz * kz;
+            if (!(std::fabs(n2 - 1.0) <= 1e-9)) throw Error{"khat rows must be unit vectors"};
+            bgw::rotation_for_khat(kx, ky, kz, &rot[9 * q]);
+        }
+        if (n_khat == 0) {
+            if (out_len != 0)
+                throw Error{"out_len=" + std::to_string(out_len) + " does not match expected length 0"};
+            return;
+        }
+        compute_common(h, w_arr, n_w, has_t_begin, t_begin, t_end, n_t, selected_bubbles, n_selected_bubbles,
+                       selected_bubbles != nullptr, time_cutoff, rot.data(), n_khat, out, out_len);
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_set_kernel(bgw_generalized_bulk_flow* bulk_flow, BgwxKernel kernel) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        if (kernel != BGWX_KERNEL_FP64_DIRECT && kernel != BGWX_KERNEL_FP64_FACTORED && kernel != BGWX_KERNEL_MIXED)
+            throw Error{"unknown kernel " + std::to_string((int)kernel)};
+        h->kernel = kernel;
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_first_colliding(bgw_generalized_bulk_flow* bulk_flow, size_t a_begin,
+                                                     size_t a_end, int32_t* out_codes, double* out_delta_tab) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        if (a_end > h->n_int || a_begin > a_end) {
+            Error e{"Index " + std::to_string(a_end > h->n_int ? a_end : a_begin) + " out of bounds for max " +
+                    std::to_string(h->n_int)};
+            e.index_error = true;
+            throw e;
+        }
+        require_resolution(h);
+        size_t n = a_end - a_begin;
+        if (n == 0) return;
+        size_t nd = h->n_cos * h->n_phi;
+        slice(out_codes, checked_mul(n, nd, "out_codes"), "out_codes");
+        std::vector<uint32_t> ids(n);
+        for (size_t q = 0; q < n; ++q) ids[q] = (uint32_t)(a_begin + q);
+        bgw::MaskJob job;
+        job.bubbles = h->bubbles.data();
+        job.n_int = h->n_int;
+        job.n_tot = h->n_int + h->n_ext;
+        job.n_cos = h->n_cos;
+        job.n_phi = h->n_phi;
+        job.dirs = h->dirs.data();
+        job.sel = ids.data();
+        job.n_sel = n;
+        h->timings = BgwxTimings{};
+        bgw::run_masks(device(h), job, out_codes, out_delta_tab, &h->timings);
+    });
+}
+
+void bgwx_rotation_for_khat(double kx, double ky, double kz, double* R) { bgw::rotation_for_khat(kx, ky, kz, R); }
+
+BgwStatus bgwx_generalized_bulk_flow_last_timings(const bgw_generalized_bulk_flow* bulk_flow, BgwxTimings* out) {
+    return run_ffi([&] {
+        if (!bulk_flow) throw Error{"bulk_flow must not be null"};
+        if (!out) throw Error{"out must not be null"};
+        *out = bulk_flow->timings;
+    });
+}
+
+BgwStatus bgwx_lattice_contains(BgwxLatticeKind kind, const double* params, const double* points_xyz,
+                                size_t n_points, uint8_t* out, size_t* n_out) {
+    return run_ffi([&] {
+        if (!n_out) throw Error{"n_out must not be null"};
+        if (kind == BGWX_LATTICE_EMPTY) {
+            *n_out = 0;
+            return;
+        }
+        size_t np = kind == BGWX_LATTICE_SPHERICAL ? 4 : 12;
+        if ((int)kind < 0 || (int)kind > 3) throw Error{"unknown lattice kind"};
+        const double* p = slice(params, np, "params");
+        const double* pts = slice(points_xyz, checked_mul(n_points, 3, "points"), "points");
+        uint8_t* o = const_cast<uint8_t*>(slice(out, n_points, "out"));
+        bgw::lattice_contains(kind, p, pts, n_points, o);
+        *n_out = n_points;
+    });
+}
+
+BgwStatus bgwx_lattice_exterior(BgwxLatticeKind kind, const double* params, BgwxBoundaryCondition bc,
+                                const double* interior, size_t n_interior, double* out, size_t capacity,
+                                size_t* n_out) {
+    return run_ffi([&] {
+        if (!n_out) throw Error{"n_out must not be null"};
+        if ((int)kind < 0 || (int)kind > 3) throw Error{"unknown lattice kind"};
+        if ((int)bc < 0 || (int)bc > 2) throw Error{"unknown boundary condition"};
+        size_t np = kind == BGWX_LATTICE_EMPTY ? 0 : (kind == BGWX_LATTICE_SPHERICAL ? 4 : 12);
+        const double* p = slice(params, np, "params");
+        const double* in = slice(interior, checked_mul(n_interior, 4, "interior"), "interior");
+        std::vector<double> ext = bgw::lattice_exterior(kind, p, bc, in, n_interior);
+        size_t rows = ext.size() / 4;
+        *n_out = rows;
+        if (rows > capacity)
+            throw Error{"capacity " + std::to_string(capacity) + " is smaller than " + std::to_string(rows) +
+                        " exterior rows"};
+        double* o = const_cast<double*>(slice(out, ext.size(), "out"));
+        if (!ext.empty()) std::memcpy(o, ext.data(), ext.size() * sizeof(double));
+    });
+}
+
+BgwStatus bgwx_check_causality(const double* interior, size_t n_interior, const double* exterior,
+                               size_t n_exterior) {
+    return run_ffi([&] {
+        const double* pi = slice(interior, checked_mul(n_interior, 4, "interior"), "bubbles_interior");
+        const double* pe = slice(exterior, checked_mul(n_exterior, 4, "exterior"), "bubbles_exterior");
+        bgw::check_causality(pi, n_interior, pe, n_exterior);
+    });
+}
+
+int bgwx_device_count(void) { return bgw::device_count(); }
+
+}  // extern "C"

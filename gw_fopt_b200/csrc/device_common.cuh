@@ -1,0 +1,75 @@
+// Device-side building blocks shared by the kernels: the spacetime 4-vector,
+// unfused FP64 arithmetic for the collision decisions, buffers and the
+// per-handle device state.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math_constants.h>
+
+#include <string>
+
+#include "bgw_internal.h"
+
+namespace bgw {
+
+#define CUDA_OK(x)                                                                                  \
+    do {                                                                                            \
+        cudaError_t e_ = (x);                                                                       \
+        if (e_ != cudaSuccess)                                                                      \
+            throw ::bgw::Error{std::string("CUDA error: ") + cudaGetErrorString(e_) + " (" #x ")"}; \
+    } while (0)
+
+// Spacetime event / interval (t, x, y, z); 32-byte aligned rows in HBM.
+struct __align__(16) D4 {
+    double t, x, y, z;
+};
+
+// Unfused IEEE operations: the collision decisions must reproduce Rust's
+// f64 arithmetic (no a*b+c contraction), so they never use plain operators.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+// Minkowski scalar product, signature (-,+,+,+), summed left to right
+// (rust/bubble-gw/src/many_bubbles/spacetime.rs:593-600 via nalgebra's U4 dot).
+__device__ __forceinline__ double mdot(const D4& a, const D4& b) {
+    double p0 = dmul(-a.t, b.t);
+    double p1 = dmul(a.x, b.x);
+    double p2 = dmul(a.y, b.y);
+    double p3 = dmul(a.z, b.z);
+    return dadd(dadd(dadd(p0, p1), p2), p3);
+}
+
+__device__ __forceinline__ D4 dsub4(const D4& b, const D4& a) {
+    return D4{dsub(b.t, a.t), dsub(b.x, a.x), dsub(b.y, a.y), dsub(b.z, a.z)};
+}
+
+// Grow-only device buffer.
+struct DevBuf {
+    void* p = nullptr;
+    size_t cap = 0;
+    void ensure(size_t bytes) {
+        if (bytes <= cap) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        cap = 0;
+        size_t want = bytes < 256 ? 256 : bytes;
+        CUDA_OK(cudaMalloc(&p, want));
+        cap = want;
+    }
+    ~DevBuf() {
+        if (p) cudaFree(p);
+    }
+};
+
+struct Device {
+    int id = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[8] = {};
+    DevBuf bub, bubrot, dirs, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, sel, rot;
+    DevBuf tau, codes, partial, out, counters;
+    DevBuf events, aux;  // factored-kernel work arrays
+    ~Device();
+};
+
+}  // namespace bgw

@@ -1,0 +1,675 @@
+// Device pipeline of the generalized bulk-flow spectrum (sm_100a).
+//
+// Stages, per chunk of k-hat frames:
+//   k_rotate       bubbles (t, x, y, z) rotated by R(k)            [optional]
+//   k_masks_full   exact first-collider search per (k, bubble, patch)
+//   k_spec_direct  plain FP64 spectrum: one complex phase per
+//                  (bubble, cos-theta row, t, w), the reference's loop nest
+//   k_reduce       deterministic sum of per-bubble partial spectra
+//
+// Reference: rust/bubble-gw/src/many_bubbles/generalized_bulk_flow.rs (GBF).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "bgw_internal.h"
+#include "device_common.cuh"
+#include "spectrum_factored.cuh"
+
+namespace bgw {
+
+int device_count() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+Device* device_create() {
+    int n = device_count();
+    if (n <= 0)
+        throw Error{"no CUDA device is available: the bulk-flow spectrum runs only on the GPU (no CPU fallback)"};
+    auto* d = new Device();
+    try {
+        CUDA_OK(cudaGetDevice(&d->id));
+        CUDA_OK(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
+        for (auto& e : d->ev) CUDA_OK(cudaEventCreate(&e));
+    } catch (...) {
+        delete d;
+        throw;
+    }
+    return d;
+}
+
+void device_destroy(Device* d) { delete d; }
+
+Device::~Device() {
+    if (stream) {
+        cudaStreamSynchronize(stream);
+        cudaStreamDestroy(stream);
+    }
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+}
+
+// ---------------------------------------------------------------------------
+// k_rotate: x' = R x with x'_i = (R_i0 x + R_i1 y) + R_i2 z, unfused.
+// ---------------------------------------------------------------------------
+__global__ void k_rotate(const D4* __restrict__ bub, const double* __restrict__ rot, size_t n_tot,
+                         D4* __restrict__ out) {
+    size_t b = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int k = blockIdx.y;
+    if (b >= n_tot) return;
+    const double* R = rot + 9 * k;
+    D4 v = bub[b];
+    D4 o;
+    o.t = v.t;
+    o.x = dadd(dadd(dmul(R[0], v.x), dmul(R[1], v.y)), dmul(R[2], v.z));
+    o.y = dadd(dadd(dmul(R[3], v.x), dmul(R[4], v.y)), dmul(R[5], v.z));
+    o.z = dadd(dadd(dmul(R[6], v.x), dmul(R[7], v.y)), dmul(R[8], v.z));
+    out[(size_t)k * n_tot + b] = o;
+}
+
+// ---------------------------------------------------------------------------
+// Exact first-collider search (GBF:127-206, GBF:1003-1018).
+//
+// The reference scans b in index order and accepts b when
+//   d_b = Delta_ab.x > 1e-10,  tau_b = Delta_ab^2 / (2 d_b) in (0, tau_best),
+//   and check(b, c) holds for every c other than a and b.
+// check(b, c) is r(b, c) > 0 with r(b, c) = (Delta_b |Delta_c|^2 -
+// Delta_c |Delta_b|^2) . x; in IEEE arithmetic r(c, b) == -r(b, c) exactly
+// (every product and sum of the negated operands is the negated result), so
+// at most one b passes all of its checks, and the reference returns that b
+// (or None).  This kernel finds it without the O(N^2) scan:
+//   pass 1  m = argmin tau over candidates (d > 1e-10, tau > 0);
+//   pass 2  evaluate check(m, c) for all c, collecting the failures F;
+//   m passes -> m.  Otherwise the passer, if any, lies in F (it passes its
+//   check against m, so m fails against it); each member of F is verified
+//   with a full scan.  More than kMaxFail failures -> the reference loop.
+// All decision arithmetic uses unfused __dmul_rn/__dadd_rn in the reference's
+// operation order, so codes and delays are bitwise the reference's.
+// ---------------------------------------------------------------------------
+constexpr int kMaskThreads = 128;
+constexpr int kMaskTile = 128;
+constexpr int kMaxFail = 8;
+
+__device__ __forceinline__ bool check_point(const D4& dba, double nb, const D4& dca, const D4& x) {
+    double nc = mdot(dca, dca);
+    D4 cv;
+    cv.t = dsub(dmul(dba.t, nc), dmul(dca.t, nb));
+    cv.x = dsub(dmul(dba.x, nc), dmul(dca.x, nb));
+    cv.y = dsub(dmul(dba.y, nc), dmul(dca.y, nb));
+    cv.z = dsub(dmul(dba.z, nc), dmul(dca.z, nb));
+    return mdot(cv, x) > 0.0;
+}
+
+// c passes check(c, e) against every e other than a and c (global memory).
+__device__ bool passes_all(const D4* __restrict__ B, size_t n_tot, uint32_t a, size_t c, const D4& xa, const D4& x) {
+    D4 dc = dsub4(B[c], xa);
+    if (mdot(dc, x) <= 0.0) return false;
+    double nb = mdot(dc, dc);
+    for (size_t e = 0; e < n_tot; ++e) {
+        if (e == a || e == c) continue;
+        if (!check_point(dc, nb, dsub4(B[e], xa), x)) return false;
+    }
+    return true;
+}
+
+// The reference loop verbatim (GBF:162-199), used only when pass 2 overflows.
+__device__ long reference_loop(const D4* __restrict__ B, size_t n_tot, uint32_t a, const D4& xa, const D4& x) {
+    long best = -1;
+    double best_tau = CUDART_INF;
+    for (size_t b = 0; b < n_tot; ++b) {
+        if (b == a) continue;
+        D4 dba = dsub4(B[b], xa);
+        double dsq = mdot(dba, dba);
+        double dot = mdot(dba, x);
+        if (dot <= 1e-10) continue;
+        double tau = __ddiv_rn(dsq, dmul(2.0, dot));
+        if (tau <= 0.0 || tau >= best_tau) continue;
+        bool first = true;
+        for (size_t c = 0; c < n_tot; ++c) {
+            if (c == a || c == b) continue;
+            if (!check_point(dba, dsq, dsub4(B[c], xa), x)) {
+                first = false;
+                break;
+            }
+        }
+        if (first) {
+            best = (long)b;
+            best_tau = tau;
+        }
+    }
+    return best;
+}
+
+__global__ void __launch_bounds__(kMaskThreads)
+    k_masks_full(const D4* __restrict__ bub, size_t n_int, size_t n_tot, const uint32_t* __restrict__ sel,
+                 size_t n_sel, const D4* __restrict__ dirs, size_t nd, unsigned n_dblocks,
+                 double* __restrict__ tau_out, int32_t* __restrict__ code_out,
+                 unsigned long long* __restrict__ counters) {
+    __shared__ D4 tile[kMaskTile];
+    const int k = blockIdx.y;
+    const size_t slot = blockIdx.x / n_dblocks;
+    const size_t d = (size_t)(blockIdx.x % n_dblocks) * kMaskThreads + threadIdx.x;
+    const D4* B = bub + (size_t)k * n_tot;
+    const uint32_t a = sel[slot];
+    const D4 xa = B[a];
+    const bool active = d < nd;
+    const D4 x = active ? dirs[d] : D4{1.0, 0.0, 0.0, 0.0};
+
+    // pass 1: argmin of tau among candidates
+    long best = -1;
+    double best_tau = CUDART_INF;
+    for (size_t base = 0; base < n_tot; base += kMaskTile) {
+        const int nb = (int)min((size_t)kMaskTile, n_tot - base);
+        __syncthreads();
+        for (int q = threadIdx.x; q < nb; q += kMaskThreads) tile[q] = B[base + q];
+        __syncthreads();
+        if (active) {
+            for (int q = 0; q < nb; ++q) {
+                size_t b = base + q;
+                if (b == a) continue;
+                D4 dba = dsub4(tile[q], xa);
+                double dot = mdot(dba, x);
+                if (dot > 1e-10) {
+                    double tau = __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
+                    if (tau > 0.0 && tau < best_tau) {
+                        best_tau = tau;
+                        best = (long)b;
+                    }
+                }
+            }
+        }
+    }
+    // pass 2: check the argmin against everything, collecting failures
+    int nfail = 0;
+    size_t fails[kMaxFail];
+    D4 dbest{};
+    double nbest = 0.0;
+    const bool have = active && best >= 0;
+    if (have) {
+        dbest = dsub4(B[best], xa);
+        nbest = mdot(dbest, dbest);
+    }
+    for (size_t base = 0; base < n_tot; base += kMaskTile) {
+        const int nb = (int)min((size_t)kMaskTile, n_tot - base);
+        __syncthreads();
+        for (int q = threadIdx.x; q < nb; q += kMaskThreads) tile[q] = B[base + q];
+        __syncthreads();
+        if (have) {
+            for (int q = 0; q < nb; ++q) {
+                size_t c = base + q;
+                if (c == a || (long)c == best) continue;
+                if (!check_point(dbest, nbest, dsub4(tile[q], xa), x)) {
+                    if (nfail < kMaxFail) fails[nfail] = c;
+                    ++nfail;
+                }
+            }
+        }
+    }
+    if (!active) return;
+    long result = -1;
+    if (have) {
+        if (nfail == 0) {
+            result = best;
+        } else if (nfail <= kMaxFail) {
+            atomicAdd(counters, 1ull);
+            for (int f = 0; f < nfail && result < 0; ++f) {
+                size_t c = fails[f];
+                D4 dc = dsub4(B[c], xa);
+                double dot = mdot(dc, x);
+                if (!(dot > 1e-10)) continue;
+                double tau = __ddiv_rn(mdot(dc, dc), dmul(2.0, dot));
+                if (!(tau > 0.0)) continue;
+                if (passes_all(B, n_tot, a, c, xa, x)) result = (long)c;
+            }
+        } else {
+            atomicAdd(counters, 1ull);
+            result = reference_loop(B, n_tot, a, xa, x);
+        }
+    }
+    const size_t o = ((size_t)k * n_sel + slot) * nd + d;
+    double tau = 0.0;
+    if (result >= 0) {
+        // compute_delta_tab (GBF:457-466)
+        D4 dba = dsub4(B[result], xa);
+        double dot = mdot(dba, x);
+        tau = fabs(dot) < 1e-10 ? 0.0 : __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
+    }
+    tau_out[o] = tau;
+    if (code_out) {
+        int32_t code = result < 0 ? -1 : ((size_t)result < n_int ? (int32_t)result : -((int32_t)(result - n_int) + 2));
+        code_out[o] = code;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Plain FP64 spectrum (GBF:481-586, 588-664, 775-873), one block per
+// (k-hat, radiating bubble).  Per t: the B stage evaluates every patch of
+// every cos-theta row into shared memory; the A stage gives each thread one w
+// and a stride of rows (rows split across thread groups when n_w < 256) and
+// forms sum_i B_i e^{-i w dt c_i} dc v_i; the C stage multiplies by
+// e^{i w (t - z_a)} u_t cut(t) dt.  The block writes its bubble's
+// (2, S, W) contribution times 1/(6 pi).
+// ---------------------------------------------------------------------------
+constexpr int kSpecThreads = 256;
+constexpr int kSetChunk = 4;
+
+struct SpecArgs {
+    const D4* bub;
+    size_t n_tot;
+    const uint32_t* sel;
+    size_t n_sel;
+    const double* tau;
+    int n_cos, n_phi;
+    const double* cos_thetax;
+    const double* sin2phi;
+    const double* cos2phi;
+    const double* coeffs;
+    const double* powers;
+    int n_sets, n_terms;
+    int has_damping;
+    double damping;
+    const double* t_arr;
+    const double* cutw;
+    int n_t;
+    double dt;
+    const double* w;
+    int n_w;
+    double2* partial;  // (K, n_sel, 2, S, W)
+    int tau_in_smem;
+};
+
+// Combination step of ndarray's unrolled_fold:
+// acc = (((0 + (p0+p4)) + (p1+p5)) + (p2+p6)) + (p3+p7), then + tail.
+__device__ __forceinline__ double unrolled_sum8(const double* p8, double tail) {
+    double acc = 0.0;
+    acc = __dadd_rn(acc, __dadd_rn(p8[0], p8[4]));
+    acc = __dadd_rn(acc, __dadd_rn(p8[1], p8[5]));
+    acc = __dadd_rn(acc, __dadd_rn(p8[2], p8[6]));
+    acc = __dadd_rn(acc, __dadd_rn(p8[3], p8[7]));
+    return __dadd_rn(acc, tail);
+}
+
+__global__ void __launch_bounds__(kSpecThreads) k_spec_direct(SpecArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int k = blockIdx.y;
+    const size_t slot = blockIdx.x;
+    const int nd = A.n_cos * A.n_phi;
+    const double* tau_g = A.tau + ((size_t)k * A.n_sel + slot) * nd;
+    double* tau_s = reinterpret_cast<double*>(smem_raw);
+    // even number of doubles before Bsm keeps the double2 array below 16-byte aligned
+    double* Bsm = tau_s + (A.tau_in_smem ? ((nd + 1) & ~1) : 0);  // [n_cos][kSetChunk][2]
+    double2* red = reinterpret_cast<double2*>(Bsm + (size_t)A.n_cos * kSetChunk * 2);  // [256][kSetChunk][2]
+    const double* tau = A.tau_in_smem ? tau_s : tau_g;
+    if (A.tau_in_smem)
+        for (int q = threadIdx.x; q < nd; q += kSpecThreads) tau_s[q] = tau_g[q];
+    __syncthreads();
+
+    const uint32_t a = A.sel[slot];
+    const D4 xa = A.bub[(size_t)k * A.n_tot + a];
+    const double ta = xa.t, za = xa.z;
+    const int W_eff = min(A.n_w, kSpecThreads);
+    const int n_ig = kSpecThreads / W_eff;
+    const int wl = threadIdx.x % W_eff;
+    const int ig = threadIdx.x / W_eff;
+    const bool wthread = ig < n_ig;
+    const double dphi = 2.0 * CUDART_PI / (double)A.n_phi;
+    const double dcos = 2.0 / (double)(A.n_cos - 1);
+    const double inv6pi = 1.0 / (6.0 * CUDART_PI);
+
+    for (int s0 = 0; s0 < A.n_sets; s0 += kSetChunk) {
+        const int sc = min(kSetChunk, A.n_sets - s0);
+        for (int wb = 0; wb < A.n_w; wb += W_eff) {
+            const int wi = wb + wl;
+            const bool wvalid = wthread && wi < A.n_w;
+            const double wv = wvalid ? A.w[wi] : 0.0;
+            double2 cacc[kSetChunk][2];
+#pragma unroll
+            for (int s = 0; s < kSetChunk; ++s) cacc[s][0] = cacc[s][1] = make_double2(0.0, 0.0);
+
+            for (int kt = 0; kt < A.n_t; ++kt) {
+                const double t = A.t_arr[kt];
+                if (!(ta <= t)) continue;  // GBF:821
+                const double dta = t - ta;
+                // ---- B stage (GBF:481-586) ----
+                for (int i = threadIdx.x; i < A.n_cos; i += kSpecThreads) {
+                    const double c = A.cos_thetax[i];
+                    const double sin_sq = 1.0 - c * c;
+                    const double cubed = dta * (dta * dta);
+                    for (int s = 0; s < sc; ++s) {
+                        double bp = 0.0, bm = 0.0;
+                        if (dta > 0.0) {
+                            const double* trow = tau + (size_t)i * A.n_phi;
+                            const int sidx = (s0 + s) * A.n_terms;
+                            // f(t, t_n, t_nc) for patch j (GBF:549-567)
+                            auto factor = [&](int j) {
+                                const double tj = trow[j];
+                                double f = 1.0;
+                                if (tj > 0.0 && dta >= tj) {
+                                    const double ratio = tj / dta;
+                                    f = 0.0;
+                                    for (int m = 0; m < A.n_terms; ++m)
+                                        f += A.coeffs[sidx + m] * pow(ratio, A.powers[sidx + m]);
+                                    if (A.has_damping) f *= exp(-dta * (1.0 - ratio) / A.damping);
+                                }
+                                return f;
+                            };
+                            // ndarray's eight-way unrolled sum over phi (GBF:578-579)
+                            double pc[8], ps[8];
+#pragma unroll
+                            for (int u = 0; u < 8; ++u) pc[u] = ps[u] = 0.0;
+                            const int nfull = A.n_phi & ~7;
+                            for (int j0 = 0; j0 < nfull; j0 += 8) {
+#pragma unroll
+                                for (int u = 0; u < 8; ++u) {
+                                    const int j = j0 + u;
+                                    const double f = factor(j);
+                                    const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
+                                    pc[u] = __dadd_rn(pc[u], __dmul_rn(__dmul_rn(A.cos2phi[j], f), wj));
+                                    ps[u] = __dadd_rn(ps[u], __dmul_rn(__dmul_rn(A.sin2phi[j], f), wj));
+                                }
+                            }
+                            double sum_c = unrolled_sum8(pc, 0.0);
+                            double sum_s = unrolled_sum8(ps, 0.0);
+                            for (int j = nfull; j < A.n_phi; ++j) {
+                                const double f = factor(j);
+                                const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
+                                sum_c = __dadd_rn(sum_c, __dmul_rn(__dmul_rn(A.cos2phi[j], f), wj));
+                                sum_s = __dadd_rn(sum_s, __dmul_rn(__dmul_rn(A.sin2phi[j], f), wj));
+                            }
+                            bp = 0.5 * sin_sq * (sum_c * dphi * cubed);
+                            bm = 0.5 * sin_sq * (sum_s * dphi * cubed);
+                        }
+                        Bsm[((size_t)i * kSetChunk + s) * 2 + 0] = bp;
+                        Bsm[((size_t)i * kSetChunk + s) * 2 + 1] = bm;
+                    }
+                }
+                __syncthreads();
+                // ---- A stage (GBF:635-661) ----
+                double2 aacc[kSetChunk][2];
+#pragma unroll
+                for (int s = 0; s < kSetChunk; ++s) aacc[s][0] = aacc[s][1] = make_double2(0.0, 0.0);
+                if (wvalid) {
+                    for (int i = ig; i < A.n_cos; i += n_ig) {
+                        const double base_im = -dta * A.cos_thetax[i];
+                        double sn, cs;
+                        sincos(wv * base_im, &sn, &cs);
+                        const double vi = (i == 0 || i == A.n_cos - 1) ? 0.5 : 1.0;
+                        const double pr = (cs * dcos) * vi, pim = (sn * dcos) * vi;
+#pragma unroll
+                        for (int s = 0; s < kSetChunk; ++s) {
+                            if (s < sc) {
+                                const double bp = Bsm[((size_t)i * kSetChunk + s) * 2 + 0];
+                                const double bm = Bsm[((size_t)i * kSetChunk + s) * 2 + 1];
+                                aacc[s][0].x += bp * pr;
+                                aacc[s][0].y += bp * pim;
+                                aacc[s][1].x += bm * pr;
+                                aacc[s][1].y += bm * pim;
+                            }
+                        }
+                    }
+                }
+#pragma unroll
+                for (int s = 0; s < kSetChunk; ++s) {
+                    red[((size_t)threadIdx.x * kSetChunk + s) * 2 + 0] = aacc[s][0];
+                    red[((size_t)threadIdx.x * kSetChunk + s) * 2 + 1] = aacc[s][1];
+                }
+                __syncthreads();
+                // ---- C stage (GBF:832-851) ----
+                if (wvalid && ig == 0) {
+                    double sn, cs;
+                    sincos(wv * (t - za), &sn, &cs);
+                    const double uw = (kt == 0 || kt == A.n_t - 1) ? 0.5 : 1.0;
+                    const double cw = A.cutw[kt];
+                    for (int s = 0; s < sc; ++s) {
+                        for (int g = 0; g < 2; ++g) {
+                            double2 at = make_double2(0.0, 0.0);
+                            for (int q = 0; q < n_ig; ++q) {
+                                const double2 v = red[((size_t)(q * W_eff + wl) * kSetChunk + s) * 2 + g];
+                                at.x += v.x;
+                                at.y += v.y;
+                            }
+                            double re = (at.x * cs - at.y * sn) * uw * cw;
+                            double im = (at.x * sn + at.y * cs) * uw * cw;
+                            cacc[s][g].x += re * A.dt;
+                            cacc[s][g].y += im * A.dt;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+            if (wvalid && ig == 0) {
+                for (int s = 0; s < sc; ++s)
+                    for (int g = 0; g < 2; ++g) {
+                        size_t o = ((((size_t)k * A.n_sel + slot) * 2 + g) * A.n_sets + (s0 + s)) * A.n_w + wi;
+                        A.partial[o] = make_double2(cacc[s][g].x * inv6pi, cacc[s][g].y * inv6pi);
+                    }
+            }
+        }
+    }
+}
+
+// Sum over radiating bubbles in index order (GBF:971-981).
+__global__ void k_reduce(const double2* __restrict__ partial, size_t n_sel, size_t per, size_t kc,
+                         double2* __restrict__ out) {
+    size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    size_t k = blockIdx.y;
+    if (q >= per || k >= kc) return;
+    double2 acc = make_double2(0.0, 0.0);
+    const double2* p = partial + k * n_sel * per + q;
+    for (size_t s = 0; s < n_sel; ++s) {
+        double2 v = p[s * per];
+        acc.x += v.x;
+        acc.y += v.y;
+    }
+    out[k * per + q] = acc;
+}
+
+// ---------------------------------------------------------------------------
+// Host orchestration.
+// ---------------------------------------------------------------------------
+namespace {
+
+template <class T>
+T* upload(Device* dev, DevBuf& buf, const T* host, size_t n, BgwxTimings* tm) {
+    buf.ensure(n * sizeof(T));
+    if (n) {
+        CUDA_OK(cudaMemcpyAsync(buf.p, host, n * sizeof(T), cudaMemcpyHostToDevice, dev->stream));
+        if (tm) tm->h2d_bytes += (double)(n * sizeof(T));
+    }
+    return static_cast<T*>(buf.p);
+}
+
+size_t mask_budget_bytes() {
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return (size_t)1 << 30;
+    size_t b = free_b / 3;
+    const size_t cap = (size_t)24 << 30;
+    return std::max<size_t>((size_t)256 << 20, std::min(b, cap));
+}
+
+void launch_masks(Device* dev, const D4* bub, size_t n_int, size_t n_tot, const uint32_t* sel, size_t n_sel,
+                  const D4* dirs, size_t nd, size_t kc, double* tau, int32_t* codes, unsigned long long* counters) {
+    unsigned n_dblocks = (unsigned)((nd + kMaskThreads - 1) / kMaskThreads);
+    size_t gx = (size_t)n_dblocks * n_sel;
+    if (gx > 0x7fffffffULL) throw Error{"too many (bubble, patch) pairs for one launch"};
+    dim3 grid((unsigned)gx, (unsigned)kc);
+    k_masks_full<<<grid, kMaskThreads, 0, dev->stream>>>(bub, n_int, n_tot, sel, n_sel, dirs, nd, n_dblocks, tau,
+                                                          codes, counters);
+    CUDA_OK(cudaGetLastError());
+}
+
+}  // namespace
+
+void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_tau, BgwxTimings* tm) {
+    CUDA_OK(cudaSetDevice(dev->id));
+    const size_t nd = job.n_cos * job.n_phi;
+    D4* bub = reinterpret_cast<D4*>(upload(dev, dev->bub, job.bubbles, 4 * job.n_tot, tm));
+    D4* dirs = reinterpret_cast<D4*>(upload(dev, dev->dirs, job.dirs, 4 * nd, tm));
+    uint32_t* sel = upload(dev, dev->sel, job.sel, job.n_sel, tm);
+    dev->tau.ensure(job.n_sel * nd * sizeof(double));
+    dev->codes.ensure(job.n_sel * nd * sizeof(int32_t));
+    dev->counters.ensure(64);
+    CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
+    CUDA_OK(cudaEventRecord(dev->ev[0], dev->stream));
+    launch_masks(dev, bub, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, 1, (double*)dev->tau.p,
+                 (int32_t*)dev->codes.p, (unsigned long long*)dev->counters.p);
+    CUDA_OK(cudaEventRecord(dev->ev[1], dev->stream));
+    CUDA_OK(cudaMemcpyAsync(out_codes, dev->codes.p, job.n_sel * nd * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            dev->stream));
+    if (out_tau)
+        CUDA_OK(cudaMemcpyAsync(out_tau, dev->tau.p, job.n_sel * nd * sizeof(double), cudaMemcpyDeviceToHost,
+                                dev->stream));
+    unsigned long long fb = 0;
+    CUDA_OK(cudaMemcpyAsync(&fb, dev->counters.p, sizeof fb, cudaMemcpyDeviceToHost, dev->stream));
+    CUDA_OK(cudaStreamSynchronize(dev->stream));
+    float ms = 0;
+    CUDA_OK(cudaEventElapsedTime(&ms, dev->ev[0], dev->ev[1]));
+    if (tm) {
+        tm->masks_ms += ms;
+        tm->total_ms += ms;
+        tm->launches += 1;
+        tm->directions += job.n_sel * nd;
+        tm->fallbacks += fb;
+        tm->d2h_bytes += (double)(job.n_sel * nd * (sizeof(int32_t) + (out_tau ? sizeof(double) : 0)));
+    }
+}
+
+void run_spectrum(Device* dev, const SpectrumJob& job, double* out, BgwxTimings* tm) {
+    CUDA_OK(cudaSetDevice(dev->id));
+    const size_t nd = job.n_cos * job.n_phi;
+    const size_t S = job.n_sets, W = job.n_w, K = job.n_k;
+    const size_t per = 2 * S * W;
+    if (job.n_cos > 4096 || job.n_phi > 65536) throw Error{"angular resolution too large for the GPU kernels"};
+    if (job.n_t > (size_t)0x7fffffff || W > (size_t)0x7fffffff) throw Error{"n_t or n_w too large"};
+
+    D4* bub = reinterpret_cast<D4*>(upload(dev, dev->bub, job.bubbles, 4 * job.n_tot, tm));
+    D4* dirs = reinterpret_cast<D4*>(upload(dev, dev->dirs, job.dirs, 4 * nd, tm));
+    double* cos_t = upload(dev, dev->cos_t, job.cos_thetax, job.n_cos, tm);
+    double* sin2 = upload(dev, dev->sin2, job.sin2phi, job.n_phi, tm);
+    double* cos2 = upload(dev, dev->cos2, job.cos2phi, job.n_phi, tm);
+    double* coeffs = upload(dev, dev->coeffs, job.coeffs, S * job.n_terms, tm);
+    double* powers = upload(dev, dev->powers, job.powers, S * job.n_terms, tm);
+    double* t_arr = upload(dev, dev->t_arr, job.t_arr, job.n_t, tm);
+    double* cutw = upload(dev, dev->cutw, job.cutoff, job.n_t, tm);
+    double* w = upload(dev, dev->w, job.w, W, tm);
+    uint32_t* sel = upload(dev, dev->sel, job.sel, job.n_sel, tm);
+    double* rot = job.rot ? upload(dev, dev->rot, job.rot, 9 * K, tm) : nullptr;
+
+    // frames per chunk: bounded by the mask buffer budget
+    const size_t per_k = job.n_sel * nd * sizeof(double) + job.n_sel * per * sizeof(double2);
+    size_t kc = std::max<size_t>(1, std::min(K, mask_budget_bytes() / std::max<size_t>(per_k, 1)));
+    kc = std::min<size_t>(kc, 65535);
+    dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
+    dev->partial.ensure(kc * job.n_sel * per * sizeof(double2));
+    dev->out.ensure(K * per * sizeof(double2));
+    if (rot) dev->bubrot.ensure(kc * job.n_tot * sizeof(D4));
+    dev->counters.ensure(64);
+    CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
+
+    // shared memory of the direct kernel
+    size_t smem_fixed = (size_t)job.n_cos * kSetChunk * 2 * sizeof(double) +
+                        (size_t)kSpecThreads * kSetChunk * 2 * sizeof(double2);
+    size_t smem_tau = ((nd + 1) & ~(size_t)1) * sizeof(double);
+    int max_optin = 0;
+    CUDA_OK(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev->id));
+    int tau_in_smem = smem_fixed + smem_tau <= (size_t)max_optin ? 1 : 0;
+    size_t smem = smem_fixed + (tau_in_smem ? smem_tau : 0);
+    if (smem > (size_t)max_optin) throw Error{"n_cos_thetax too large for the shared-memory layout"};
+    CUDA_OK(cudaFuncSetAttribute(k_spec_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+
+    float ms_masks = 0, ms_spec = 0;
+    uint64_t launches = 0;
+    CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
+    for (size_t k0 = 0; k0 < K; k0 += kc) {
+        const size_t kn = std::min(kc, K - k0);
+        const D4* fb = bub;
+        if (rot) {
+            dim3 g((unsigned)((job.n_tot + 255) / 256), (unsigned)kn);
+            k_rotate<<<g, 256, 0, dev->stream>>>(bub, rot + 9 * k0, job.n_tot, (D4*)dev->bubrot.p);
+            CUDA_OK(cudaGetLastError());
+            ++launches;
+            fb = (const D4*)dev->bubrot.p;
+        }
+        CUDA_OK(cudaEventRecord(dev->ev[0], dev->stream));
+        launch_masks(dev, fb, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, kn, (double*)dev->tau.p, nullptr,
+                     (unsigned long long*)dev->counters.p);
+        ++launches;
+        CUDA_OK(cudaEventRecord(dev->ev[1], dev->stream));
+        if (job.kernel == BGWX_KERNEL_FP64_DIRECT) {
+            SpecArgs A;
+            A.bub = fb;
+            A.n_tot = job.n_tot;
+            A.sel = sel;
+            A.n_sel = job.n_sel;
+            A.tau = (const double*)dev->tau.p;
+            A.n_cos = (int)job.n_cos;
+            A.n_phi = (int)job.n_phi;
+            A.cos_thetax = cos_t;
+            A.sin2phi = sin2;
+            A.cos2phi = cos2;
+            A.coeffs = coeffs;
+            A.powers = powers;
+            A.n_sets = (int)S;
+            A.n_terms = (int)job.n_terms;
+            A.has_damping = job.has_damping ? 1 : 0;
+            A.damping = job.damping;
+            A.t_arr = t_arr;
+            A.cutw = cutw;
+            A.n_t = (int)job.n_t;
+            A.dt = job.dt;
+            A.w = w;
+            A.n_w = (int)W;
+            A.partial = (double2*)dev->partial.p;
+            A.tau_in_smem = tau_in_smem;
+            if (job.n_sel > 0x7fffffffULL) throw Error{"too many radiating bubbles"};
+            dim3 g((unsigned)job.n_sel, (unsigned)kn);
+            k_spec_direct<<<g, kSpecThreads, smem, dev->stream>>>(A);
+            CUDA_OK(cudaGetLastError());
+            ++launches;
+            dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
+            k_reduce<<<gr, 256, 0, dev->stream>>>((const double2*)dev->partial.p, job.n_sel, per, kn,
+                                                  (double2*)dev->out.p + k0 * per);
+            CUDA_OK(cudaGetLastError());
+            ++launches;
+        } else {
+            launches += launch_factored(dev, job, fb, sel, (const double*)dev->tau.p, cos_t, sin2, cos2, coeffs,
+                                        powers, t_arr, cutw, w, kn, (double2*)dev->out.p + k0 * per);
+        }
+        CUDA_OK(cudaEventRecord(dev->ev[2], dev->stream));
+        CUDA_OK(cudaEventSynchronize(dev->ev[2]));
+        float a = 0, b = 0;
+        CUDA_OK(cudaEventElapsedTime(&a, dev->ev[0], dev->ev[1]));
+        CUDA_OK(cudaEventElapsedTime(&b, dev->ev[1], dev->ev[2]));
+        ms_masks += a;
+        ms_spec += b;
+    }
+    CUDA_OK(cudaEventRecord(dev->ev[5], dev->stream));
+    CUDA_OK(cudaMemcpyAsync(out, dev->out.p, K * per * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
+    unsigned long long fbk = 0;
+    CUDA_OK(cudaMemcpyAsync(&fbk, dev->counters.p, sizeof fbk, cudaMemcpyDeviceToHost, dev->stream));
+    CUDA_OK(cudaStreamSynchronize(dev->stream));
+    float total = 0;
+    CUDA_OK(cudaEventElapsedTime(&total, dev->ev[4], dev->ev[5]));
+    if (tm) {
+        tm->masks_ms += ms_masks;
+        tm->spectrum_ms += ms_spec;
+        tm->total_ms += total;
+        tm->launches += launches;
+        tm->directions += K * job.n_sel * nd;
+        tm->fallbacks += fbk;
+        tm->d2h_bytes += (double)(K * per * sizeof(double2));
+    }
+}
+
+}  // namespace bgw

@@ -1,0 +1,131 @@
+/*
+ * bubble_gw_b200.h -- extensions of the bubble_gw C ABI for the B200 build.
+ *
+ * Everything here is additive: the reference-compatible surface is
+ * bubble_gw.h.  Each entry point names the reference interface it serves
+ * (file:line in the reference tree) or says that it has no counterpart.
+ * Status codes, error messages and array conventions are those of
+ * bubble_gw.h.
+ */
+#pragma once
+#ifndef BUBBLE_GW_B200_H
+#define BUBBLE_GW_B200_H
+
+#include "bubble_gw.h"
+
+#include <stdint.h>
+
+/* Lattice kinds (rust/bubble-gw/src/many_bubbles/lattice/built_in_lattice.rs:20).
+ * Parameters (LatticeGeometry::parameters):
+ *   PARALLELEPIPED / CARTESIAN: origin(3), e1(3), e2(3), e3(3)   (12 doubles)
+ *   SPHERICAL: center(3), radius                                  (4 doubles)
+ *   EMPTY: none                                                   (0 doubles) */
+typedef enum BgwxLatticeKind {
+    BGWX_LATTICE_PARALLELEPIPED = 0,
+    BGWX_LATTICE_CARTESIAN = 1,
+    BGWX_LATTICE_SPHERICAL = 2,
+    BGWX_LATTICE_EMPTY = 3,
+} BgwxLatticeKind;
+
+/* rust/bubble-gw/src/many_bubbles/lattice/boundary_condition.rs:3 */
+typedef enum BgwxBoundaryCondition {
+    BGWX_BC_PERIODIC = 0,
+    BGWX_BC_REFLECTION = 1,
+    BGWX_BC_NONE = 2,
+} BgwxBoundaryCondition;
+
+/* Spectrum kernels.  FP64_DIRECT: plain FP64, one complex phase per
+ * (bubble, cos-theta row, t, w), as the reference's loop nest.
+ * FP64_FACTORED: FP64 with the time phase shared across bubbles (register
+ * tiled).  MIXED: FP64 phase arguments with range reduction and FP64 final
+ * sums, FP32 sincos/weights/compensated partial sums. */
+typedef enum BgwxKernel {
+    BGWX_KERNEL_FP64_DIRECT = 0,
+    BGWX_KERNEL_FP64_FACTORED = 1,
+    BGWX_KERNEL_MIXED = 2,
+} BgwxKernel;
+
+/* Per-call device timings (milliseconds, CUDA events on the handle's stream). */
+typedef struct BgwxTimings {
+    double masks_ms;    /* first-collider search (all k-hat chunks) */
+    double spectrum_ms; /* spectrum kernels (all k-hat chunks) */
+    double total_ms;    /* whole device section of the last call */
+    double h2d_bytes;   /* host->device bytes copied by the last call */
+    double d2h_bytes;   /* device->host bytes copied by the last call */
+    uint64_t launches;  /* kernels launched by the last call */
+    uint64_t directions;/* patch directions searched by the mask kernel */
+    uint64_t fallbacks; /* directions resolved by the exact slow path */
+} BgwxTimings;
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Lattice containment, one byte per point (1 = inside).  EMPTY reports
+ * n_points = 0 semantics: out is left untouched and *n_out = 0.
+ * Replaces LatticeGeometry::contains (parallelepiped_lattice.rs:161-186,
+ * spherical_lattice.rs, empty_lattice.rs:31). */
+BgwStatus bgwx_lattice_contains(BgwxLatticeKind kind, const double *params, const double *points_xyz,
+                                size_t n_points, uint8_t *out, size_t *n_out);
+
+/* Boundary images of interior bubbles: periodic = 6 face shifts, reflection
+ * = 6 face mirrors (parallelepiped) or 2 tangent-plane mirrors (sphere).
+ * Writes at most `capacity` rows of (t, x, y, z) and the row count to *n_out.
+ * Replaces GenerateBubblesExterior (parallelepiped_lattice.rs:189-299,
+ * spherical_lattice.rs:72-131, empty_lattice.rs:38-46). */
+BgwStatus bgwx_lattice_exterior(BgwxLatticeKind kind, const double *params, BgwxBoundaryCondition bc,
+                                const double *interior, size_t n_interior, double *out, size_t capacity,
+                                size_t *n_out);
+
+/* Causality check of LatticeBubbles::new (lattice_bubbles.rs:71-119): no
+ * interior-interior or interior-exterior pair may have a negative interval. */
+BgwStatus bgwx_check_causality(const double *interior, size_t n_interior, const double *exterior,
+                               size_t n_exterior);
+
+/* As bgw_generalized_bulk_flow_empty_lattice_new without the causality check:
+ * the Python LatticeBubbles validates at construction and adds boundary
+ * images afterwards without re-validating (lattice_bubbles.rs:323-365), and
+ * GeneralizedBulkFlow::new (generalized_bulk_flow.rs:86-108) checks nothing. */
+BgwStatus bgwx_generalized_bulk_flow_new_unchecked(bgw_generalized_bulk_flow **out, const double *interior,
+                                                   size_t n_interior, const double *exterior, size_t n_exterior);
+
+/* Selects the spectrum kernel used by every compute call on this handle.
+ * No counterpart in the reference (it has one f64 CPU path). */
+BgwStatus bgwx_generalized_bulk_flow_set_kernel(bgw_generalized_bulk_flow *bulk_flow, BgwxKernel kernel);
+
+/* First-collider codes (-1 None, i Interior(i), -(i+2) Exterior(i)) and the
+ * collision delays of compute_delta_tab for interior bubbles [a_begin, a_end)
+ * at k-hat = z, computed on the GPU.  out_codes: (a_end-a_begin, n_cos, n_phi)
+ * int32; out_delta_tab (may be NULL): same shape, f64.
+ * Replaces GeneralizedBulkFlow::compute_first_colliding_bubble and
+ * compute_delta_tab (generalized_bulk_flow.rs:127-206, 421-471). */
+BgwStatus bgwx_generalized_bulk_flow_first_colliding(bgw_generalized_bulk_flow *bulk_flow, size_t a_begin,
+                                                     size_t a_end, int32_t *out_codes, double *out_delta_tab);
+
+/* Spectrum for K directions k-hat (row-major (K, 3), unit vectors).  For each
+ * k-hat the configuration is rotated by the Rodrigues rotation R(k) taking
+ * k-hat to z (about k x z; identity for +z; pi about x for -z), and the
+ * result equals bgw_generalized_bulk_flow_compute_c_integral on the rotated
+ * configuration with the same `selected_bubbles` (NULL = all interior
+ * bubbles).  out: (K, 2, n_sets, n_w); out_len = K*2*n_sets*n_w.
+ * Serves the reference's per-direction recipe of rotating LatticeBubbles
+ * (lattice_bubbles.rs:144-197) and recomputing (generalized_bulk_flow.rs:928-984). */
+BgwStatus bgwx_generalized_bulk_flow_compute_c_integral_khat(
+    bgw_generalized_bulk_flow *bulk_flow, const double *w_arr, size_t n_w, bool has_t_begin, double t_begin,
+    double t_end, size_t n_t, const double *khat, size_t n_khat, const size_t *selected_bubbles,
+    size_t n_selected_bubbles, BgwTimeCutoffConfig time_cutoff, BgwComplex64 *out, size_t out_len);
+
+/* The rotation R(k) used above, row-major 3x3.  No counterpart in the reference. */
+void bgwx_rotation_for_khat(double kx, double ky, double kz, double *R);
+
+/* Device timings of the last compute call on this handle.  No counterpart. */
+BgwStatus bgwx_generalized_bulk_flow_last_timings(const bgw_generalized_bulk_flow *bulk_flow, BgwxTimings *out);
+
+/* Number of CUDA devices visible (0 on a machine without a GPU).  No counterpart. */
+int bgwx_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* BUBBLE_GW_B200_H */

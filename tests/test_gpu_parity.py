@@ -1,0 +1,160 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Masks (first-collider codes and collision delays) must be bitwise equal to
+the oracle's; spectra must agree to 1e-12 relative (norm over (+/x, sets) at
+each w, max over w) for the FP64 kernels.  Cases follow the reference's own
+tests and examples: the two-bubble C-ABI test (rust/c-bubble-gw/tests/c_api.rs:137-141),
+the five-bubble bench geometry (rust/benches/bulk_flow_bench.rs:9-15), confY
+with periodic images (docs/examples/generalized_bulkflow.py:743-757) and the
+synthetic benchmark configurations.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from gw_fopt_b200 import many_bubbles as mb
+from gw_fopt_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+FP64_TOL = 1e-12
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_small.npz")
+
+
+def err_per_w(got, ref):
+    """max over w of ||got - ref||_2 / ||ref||_2 over all leading axes."""
+    g = got.reshape(-1, got.shape[-1])
+    r = ref.reshape(-1, ref.shape[-1])
+    num = np.linalg.norm(g - r, axis=0)
+    den = np.linalg.norm(r, axis=0)
+    scale = np.linalg.norm(r)
+    return float(np.max(num / np.maximum(den, 1e-300 + 1e-13 * scale)))
+
+
+def golden_cases():
+    g = np.load(GOLDEN)
+    names = sorted({k.split("__")[0] for k in g.files})
+    out = {}
+    for n in names:
+        out[n] = {k.split("__", 1)[1]: g[k] for k in g.files if k.startswith(n + "__")}
+    return out
+
+
+def make_flow(interior, exterior, n_cos, n_phi, coeffs=((1.0,),), powers=((3.0,),), damping=None,
+              kernel="fp64_direct"):
+    lb = mb.LatticeBubbles(mb.EmptyLattice(), np.asarray(interior, dtype=np.float64),
+                           np.asarray(exterior, dtype=np.float64))
+    g = mb.GeneralizedBulkFlow(lb)
+    g.set_resolution(n_cos, n_phi)
+    g.set_gradient_scaling_params([list(r) for r in coeffs], [list(r) for r in powers],
+                                  None if damping is None or np.isnan(damping) else float(damping))
+    g.set_kernel(kernel)
+    return g
+
+
+@pytest.mark.parametrize("name", ["capi2", "bench5", "confY", "cfg1_damped"])
+def test_masks_bitwise_vs_golden(gpu_available, name):
+    p = golden_cases()[name]
+    g = make_flow(p["interior"], p["exterior"], int(p["n_cos"]), int(p["n_phi"]))
+    for a in range(p["interior"].shape[0]):
+        assert np.array_equal(g.compute_first_colliding_bubble(a), p["codes"][a]), (name, a)
+
+
+def test_delta_tab_bitwise(gpu_available):
+    import ctypes as C
+    from gw_fopt_b200 import _lib as L
+    c = W.config(2)
+    n_cos = n_phi = 48
+    lb = mb.LatticeBubbles(mb.EmptyLattice(), c.interior, c.exterior)
+    g = mb.GeneralizedBulkFlow(lb)
+    g.set_resolution(n_cos, n_phi)
+    a0, a1 = 10, 26
+    codes = np.empty((a1 - a0, n_cos, n_phi), dtype=np.int32)
+    tau = np.empty((a1 - a0, n_cos, n_phi))
+    L.check(L.lib().bgwx_generalized_bulk_flow_first_colliding(
+        g._h, a0, a1, codes.ctypes.data_as(C.POINTER(C.c_int32)), tau.ctypes.data_as(C.POINTER(C.c_double))))
+    rc, rt = O.first_colliding(c.interior, c.exterior, n_cos, n_phi, a0, a1, with_delta_tab=True)
+    assert np.array_equal(codes, rc)
+    assert np.array_equal(tau, rt)
+
+
+@pytest.mark.parametrize("name", ["capi2", "bench5", "confY", "cfg1_damped"])
+def test_spectrum_fp64_vs_golden(gpu_available, name):
+    p = golden_cases()[name]
+    g = make_flow(p["interior"], p["exterior"], int(p["n_cos"]), int(p["n_phi"]), p["coeffs"], p["powers"],
+                  float(p["damping"]))
+    out = g.compute_c_integral(p["w"], t_begin=float(p["t_begin"]), t_end=float(p["t_end"]), n_t=int(p["n_t"]))
+    assert out.shape == p["out"].shape and out.dtype == np.complex128
+    assert err_per_w(out, p["out"]) < FP64_TOL
+
+
+def test_capi_case_matches_reference_test_shape(gpu_available):
+    # rust/c-bubble-gw/tests/c_api.rs:135-218 through the reference-named C ABI
+    p = golden_cases()["capi2"]
+    g = make_flow(p["interior"], p["exterior"], 4, 5, [[0.0], [1.0]], [[3.0], [3.0]])
+    out = g.compute_c_integral([0.5, 1.0], t_begin=0.0, t_end=8.0, n_t=40)
+    np.testing.assert_allclose(out, p["out"], rtol=1e-10, atol=1e-10)
+
+
+def test_selected_duplicates_and_late_bubbles(gpu_available):
+    c = W.config(1)
+    interior = c.interior.copy()
+    interior[3, 0] = 2.0  # nucleates after t_end: contributes nothing
+    ext = W.periodic_images(interior, 1.0)
+    g = make_flow(interior, ext, 12, 14, [[1.0]], [[5.0]])
+    sel = np.array([1, 3, 1, 5])
+    out = g.compute_c_integral(c.w, t_begin=0.0, t_end=1.5, n_t=64, selected_bubbles=sel)
+    ref = O.compute_c_integral(interior, ext, 12, 14, c.w, 1.5, 64, t_begin=0.0, coefficients=[[1.0]],
+                               powers=[[5.0]], selected=sel)
+    assert err_per_w(out, ref) < FP64_TOL
+
+
+def test_exponential_cutoff_and_t_begin(gpu_available):
+    c = W.config(1)
+    g = make_flow(c.interior, c.exterior, 16, 16, [[1.0], [0.5]], [[5.0], [2.5]])
+    cut = mb.ExponentialTimeCutoff(1.5, 0.6, 0.3)
+    out = g.compute_c_integral(c.w, t_begin=0.05, t_end=1.5, n_t=96, time_cutoff=cut)
+    ref = O.compute_c_integral(c.interior, c.exterior, 16, 16, c.w, 1.5, 96, t_begin=0.05,
+                               coefficients=[[1.0], [0.5]], powers=[[5.0], [2.5]], cutoff=(1.5, 0.6, 0.3))
+    assert err_per_w(out, ref) < FP64_TOL
+
+
+def test_config1_all_khat_fp64(gpu_available):
+    c = W.config(1)
+    g = make_flow(c.interior, c.exterior, c.n_cos, c.n_phi, c.coefficients, c.powers)
+    out = g.compute_c_integral_khat(c.w, c.khat, t_begin=c.t_begin, t_end=c.t_end, n_t=c.n_t)
+    ref = O.compute_c_integral_khat(c.interior, c.exterior, c.khat, c.n_cos, c.n_phi, c.w, c.t_begin, c.t_end,
+                                    c.n_t, coefficients=c.coefficients, powers=c.powers)
+    assert out.shape == (16, 2, 1, 32)
+    assert err_per_w(out, ref) < FP64_TOL
+
+
+def test_config2_subset_fp64(gpu_available):
+    """Config 2 geometry (512 bubbles, 3584 with images, 128x128 patches, T=512, W=128),
+    a slice of radiating bubbles: with all colliders present, any subset of
+    radiators is an exact partial sum (generalized_bulk_flow.rs:953-981)."""
+    c = W.config(2)
+    sel = np.arange(0, 512, 97)
+    g = make_flow(c.interior, c.exterior, c.n_cos, c.n_phi, c.coefficients, c.powers)
+    kh = c.khat[[0, 17]]
+    out = g.compute_c_integral_khat(c.w, kh, t_begin=0.0, t_end=c.t_end, n_t=c.n_t, selected_bubbles=sel)
+    for q, k in enumerate(kh):
+        R = O.rotation_for_khat(k)
+        ri, re = O.rotate(R, c.interior), O.rotate(R, c.exterior)
+        ref = O.compute_c_integral(ri, re, c.n_cos, c.n_phi, c.w, c.t_end, c.n_t, t_begin=0.0,
+                                   coefficients=c.coefficients, powers=c.powers, selected=sel)
+        assert err_per_w(out[q], ref) < FP64_TOL, q
+
+
+def test_python_fixed_bubble_and_masks(gpu_available):
+    p = golden_cases()["bench5"]
+    g = make_flow(p["interior"], p["exterior"], int(p["n_cos"]), int(p["n_phi"]), p["coeffs"], p["powers"])
+    one = g.compute_c_integral_fixed_bubble(2, p["w"], 0.0, 15.0, 200)
+    ref = O.compute_c_integral(p["interior"], p["exterior"], int(p["n_cos"]), int(p["n_phi"]), p["w"], 15.0, 200,
+                               t_begin=0.0, coefficients=p["coeffs"], powers=p["powers"], selected=[2])
+    assert err_per_w(one, ref) < FP64_TOL
+    with pytest.raises(IndexError):
+        g.compute_c_integral_fixed_bubble(9, p["w"], 0.0, 15.0, 200)
