@@ -1,0 +1,336 @@
+#!/usr/bin/env python
+"""Benchmark of the generalized bulk-flow many-bubble GW spectrum on B200.
+
+Metric: patch-time evaluations per second, PTE = K * N * n_cos * n_phi * n_t
+for one complete spectrum (all k-hat directions, all bubbles, all t, all w),
+masks included.  One step = one complete spectrum of the named synthetic
+workload (seeded; no dataset exists for this path).
+
+    python bench.py [--gpus N --steps K --warmup W] [--config 3] [--kernel mixed]
+    python bench.py --impl reference ...   # the CPU restatement of the reference
+
+value: device-resident inputs, result left in HBM (CUDA events on the
+       launching stream, L2 flushed between steps by a 256 MiB write).
+e2e:   the public Python API with host buffers, every input copied to the
+       device and the result copied back each step.
+Multi-GPU (torchrun): each rank computes its own k-hat directions of a
+K*N-direction Fibonacci sphere (weak scaling, no data-path collective);
+timing is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "patch-time evals/s: mixed-prec vs FP64 on one B200 at <=1e-6 rel err; CPU ref"
+UNIT = "patch-time evals/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--config", type=int, default=2)
+    ap.add_argument("--kernel", default="fp64_direct", choices=["fp64_direct", "fp64_factored", "mixed"])
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample budget")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                if int(f[0]) != self.index:
+                    continue
+                rows.append(f)
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": []}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = max(float(r[2]) for r in rows)
+        load = [v for v in sm if v > 0.5 * mx] or sm
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in rows for q in range(4) if r[5 + q].lower() == "active"})
+        return {"sm_mhz": statistics.median(load), "sm_max_mhz": mx, "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+def make_flow(cfg, kernel):
+    from gw_fopt_b200 import many_bubbles as mb
+    lb = mb.LatticeBubbles(mb.EmptyLattice(), cfg.interior, cfg.exterior)
+    g = mb.GeneralizedBulkFlow(lb)
+    g.set_resolution(cfg.n_cos, cfg.n_phi)
+    g.set_gradient_scaling_params(cfg.coefficients.tolist(), cfg.powers.tolist())
+    g.set_kernel(kernel)
+    return g
+
+
+def cpu_baseline(cfg, seconds: float, threads: int | None = None):
+    """The oracle (CPU f64 restatement, reference loop structure) on a bounded sample:
+    the first k-hat direction and as many radiating bubbles as fit in ~`seconds`."""
+    from oracle import oracle as O
+    threads = threads or O.max_threads()
+    R = O.rotation_for_khat(cfg.khat[0])
+    ri, re = O.rotate(R, cfg.interior), O.rotate(R, cfg.exterior)
+
+    def run(sel):
+        t0 = time.perf_counter()
+        O.compute_c_integral(ri, re, cfg.n_cos, cfg.n_phi, cfg.w, cfg.t_end, cfg.n_t, t_begin=cfg.t_begin,
+                             coefficients=cfg.coefficients, powers=cfg.powers, selected=sel, threads=threads)
+        return time.perf_counter() - t0
+
+    order = np.random.default_rng(0).permutation(cfg.n)
+    t1 = run(order[:1])
+    n_sel = int(max(1, min(cfg.n, seconds / max(t1, 1e-3))))
+    sel = order[:n_sel]
+    dt = run(sel)
+    pte = n_sel * cfg.n_cos * cfg.n_phi * cfg.n_t
+    return {"value": pte / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n_sel} radiating bubbles x 1 k-hat of {cfg.name} (all {cfg.interior.shape[0] + cfg.exterior.shape[0]}"
+                      f" colliders), {dt:.1f} s", "seconds": dt}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def run_b200(args):
+    import torch
+    from gw_fopt_b200 import _lib as L
+    from gw_fopt_b200 import many_bubbles as mb
+    from gw_fopt_b200 import workloads as W
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+
+    cfg = W.config(args.config)
+    K = cfg.khat.shape[0]
+    cfg.khat = W.fibonacci_khat(K * world)[rank::world]
+    g = make_flow(cfg, args.kernel)
+    lib = L.lib()
+    S, Wn = cfg.coefficients.shape[0], cfg.w.size
+    stream = torch.cuda.current_stream()
+    L.check(lib.bgwx_generalized_bulk_flow_set_stream(g._h, C.c_void_p(stream.cuda_stream)))
+    out_dev = torch.empty((K, 2, S, Wn), dtype=torch.complex128, device="cuda")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    w = np.ascontiguousarray(cfg.w)
+    kh = np.ascontiguousarray(cfg.khat)
+    cut = mb._UNIT_CUTOFF
+
+    def step():
+        L.check(lib.bgwx_generalized_bulk_flow_compute_c_integral_khat_device(
+            g._h, L.ptr(w), Wn, True, cfg.t_begin, cfg.t_end, cfg.n_t, L.ptr(kh), K, None, 0, cut,
+            C.c_void_p(out_dev.data_ptr()), out_dev.numel()))
+        flush.zero_()  # L2 flush between timed iterations
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1)
+    if pg is not None:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    pte_total = cfg.pte * world
+    value = pte_total / (ms_step * 1e-3)
+
+    # one synchronous call on the library's own stream for per-kernel timings
+    L.check(lib.bgwx_generalized_bulk_flow_set_stream(g._h, None))
+    res = g.compute_c_integral_khat(cfg.w, cfg.khat, t_begin=cfg.t_begin, t_end=cfg.t_end, n_t=cfg.n_t)
+    tm = g.last_timings()
+    launches_per_step = int(tm["launches"])
+
+    # end to end through the public API with host buffers
+    e2e = None
+    if not args.no_e2e:
+        L.check(lib.bgwx_generalized_bulk_flow_set_stream(g._h, C.c_void_p(stream.cuda_stream)))
+        h2d = d2h = 0.0
+        barrier()
+        torch.cuda.synchronize()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            L.check(lib.bgwx_generalized_bulk_flow_drop_resident_inputs(g._h))
+            host_out = g.compute_c_integral_khat(cfg.w, cfg.khat, t_begin=cfg.t_begin, t_end=cfg.t_end,
+                                                 n_t=cfg.n_t)
+            t2 = g.last_timings()
+            h2d, d2h = t2["h2d_bytes"], t2["d2h_bytes"]
+        f1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+        ms_e = f0.elapsed_time(f1)
+        if pg is not None:
+            t = torch.tensor([ms_e], device="cuda", dtype=torch.float64)
+            pg.all_reduce(t, op=pg.ReduceOp.MAX)
+            ms_e = float(t.item())
+        e2e = {"value": pte_total / (ms_e / args.steps * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e / args.steps}
+        assert np.array_equal(host_out, res)
+
+    # roofline of the dominant kernel (counted-flop convention F = 6 PTE + 8 Phi + 20 Phi_t)
+    p64, p32, psfu = C.c_double(), C.c_double(), C.c_double()
+    L.check(lib.bgwx_measure_compute_peaks(C.byref(p64), C.byref(p32), C.byref(psfu)))
+    peaks = {"fp64_tflops": p64.value / 1e12, "fp32_tflops": p32.value / 1e12, "sfu_tops": psfu.value / 1e12}
+    spec_s = tm["spectrum_ms"] * 1e-3
+    masks_s = tm["masks_ms"] * 1e-3
+    dominant = "spectrum" if spec_s >= masks_s else "masks"
+    achieved = cfg.counted_flops / spec_s / 1e12 if spec_s > 0 else None
+    if args.kernel == "mixed":
+        peak = p32.value / 1e12
+        bound = "fp32"
+    else:
+        peak = p64.value / 1e12
+        bound = "fp64"
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(f"config{args.config}:{args.kernel}")
+        except Exception:
+            traffic = None
+    roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "kernel": f"spectrum ({args.kernel})", "dominant_kernel": dominant,
+                "spectrum_ms": tm["spectrum_ms"], "masks_ms": tm["masks_ms"],
+                "peak_source": "measured on this GPU by bgwx_measure_compute_peaks (FMA chains); "
+                               "MEASURED_PEAKS.json has HBM/bf16 only", "peaks": peaks}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64" if args.kernel != "mixed" else "f32+f64", "data": "synthetic",
+            "config": {"workload": cfg.name, "bubbles": int(cfg.n), "colliders": int(cfg.n + cfg.exterior.shape[0]),
+                       "n_cos": cfg.n_cos, "n_phi": cfg.n_phi, "n_t": cfg.n_t, "n_w": int(Wn),
+                       "n_khat_per_gpu": int(K), "kernel": args.kernel, "pte_per_step": pte_total,
+                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"khat-shard x{world}"},
+            "roofline": roofline, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clocks}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(cfg, args.cpu_seconds)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+def run_reference(args):
+    rank, world, local = dist_env()
+    if rank != 0:
+        return
+    from gw_fopt_b200 import workloads as W
+    from oracle import oracle as O
+    cfg = W.config(args.config)
+    threads = O.max_threads()
+    per_step = max(2.0, 40.0 / max(args.steps + args.warmup, 1))
+    base = cpu_baseline(cfg, per_step, threads)
+    n_sel = int(base["sample"].split()[0])
+    R = O.rotation_for_khat(cfg.khat[0])
+    ri, re = O.rotate(R, cfg.interior), O.rotate(R, cfg.exterior)
+    sel = np.random.default_rng(0).permutation(cfg.n)[:n_sel]
+
+    def step():
+        O.compute_c_integral(ri, re, cfg.n_cos, cfg.n_phi, cfg.w, cfg.t_end, cfg.n_t, t_begin=cfg.t_begin,
+                             coefficients=cfg.coefficients, powers=cfg.powers, selected=sel, threads=threads)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+    dt = (time.perf_counter() - t0) / args.steps
+    pte = n_sel * cfg.n_cos * cfg.n_phi * cfg.n_t
+    v = pte / dt
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": cfg.name, "bubbles": int(cfg.n), "n_cos": cfg.n_cos, "n_phi": cfg.n_phi,
+                       "n_t": cfg.n_t, "n_w": int(cfg.w.size), "n_khat": int(cfg.khat.shape[0]),
+                       "sample_radiating_bubbles": n_sel, "sample_khat": 1},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{n_sel} radiating bubbles x 1 k-hat per step (all colliders present)"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -61,6 +61,12 @@ SIGNATURES = {
     "bgwx_generalized_bulk_flow_compute_c_integral_khat": (
         C.c_int, [_hp, _dp, C.c_size_t, C.c_bool, C.c_double, C.c_double, C.c_size_t, _dp, C.c_size_t, _szp,
                   C.c_size_t, BgwTimeCutoffConfig, C.POINTER(BgwComplex64), C.c_size_t]),
+    "bgwx_generalized_bulk_flow_compute_c_integral_khat_device": (
+        C.c_int, [_hp, _dp, C.c_size_t, C.c_bool, C.c_double, C.c_double, C.c_size_t, _dp, C.c_size_t, _szp,
+                  C.c_size_t, BgwTimeCutoffConfig, C.c_void_p, C.c_size_t]),
+    "bgwx_generalized_bulk_flow_set_stream": (C.c_int, [_hp, C.c_void_p]),
+    "bgwx_generalized_bulk_flow_drop_resident_inputs": (C.c_int, [_hp]),
+    "bgwx_measure_compute_peaks": (C.c_int, [_dp, _dp, _dp]),
     "bgwx_rotation_for_khat": (None, [C.c_double, C.c_double, C.c_double, _dp]),
     "bgwx_generalized_bulk_flow_last_timings": (C.c_int, [_hp, C.POINTER(BgwxTimings)]),
     "bgwx_device_count": (C.c_int, []),

@@ -74,8 +74,16 @@ Device* device_create();  // throws Error when no CUDA device is usable
 void device_destroy(Device*);
 
 // Runs the spectrum; out: (n_k, 2, n_sets, n_w) complex as interleaved
-// doubles (host memory).  Throws Error.
-void run_spectrum(Device* dev, const SpectrumJob& job, double* out, BgwxTimings* timings);
+// doubles.  With out_is_device the result is written to device memory and
+// the call returns without synchronising (timings are then not filled).
+// Throws Error.
+void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_device, BgwxTimings* timings);
+
+// Uses `stream` (a cudaStream_t) for all later work; nullptr = own stream.
+void device_set_stream(Device* dev, void* stream);
+
+// Marks every uploaded input as stale (the next call copies it again).
+void device_drop_resident(Device* dev);
 
 // First-collider codes and delays for the selected bubbles at the
 // unrotated frame.  out_codes (n_sel, n_cos*n_phi) int32; out_tau may be null.

@@ -144,7 +144,7 @@ Cutoff make_cutoff(const BgwTimeCutoffConfig& c) {
 void compute_common(bgw_generalized_bulk_flow* h, const double* w_arr, size_t n_w, bool has_t_begin, double t_begin,
                     double t_end, size_t n_t, const size_t* selected, size_t n_selected, bool has_selected,
                     const BgwTimeCutoffConfig& cutoff, const double* rot, size_t n_k, BgwComplex64* out,
-                    size_t out_len) {
+                    size_t out_len, void* out_device = nullptr) {
     const double* w = slice(w_arr, n_w, "w_arr");
     Cutoff cut = make_cutoff(cutoff);
     size_t S = h->n_sets;
@@ -164,8 +164,12 @@ void compute_common(bgw_generalized_bulk_flow* h, const double* w_arr, size_t n_
     } else {
         for (size_t a = 0; a < h->n_int; ++a) ids.push_back((uint32_t)a);
     }
-    std::vector<double> result(2 * expected, 0.0);
+    if (out_device && out_len != expected)
+        throw Error{"out_len=" + std::to_string(out_len) + " does not match expected length " +
+                    std::to_string(expected)};
+    std::vector<double> result(out_device ? 0 : 2 * expected, 0.0);
     h->timings = BgwxTimings{};
+    bool device_written = false;
     if (!ids.empty()) {
         double tb = has_t_begin ? t_begin : 0.0;
         if (tb > t_end)
@@ -202,8 +206,18 @@ void compute_common(bgw_generalized_bulk_flow* h, const double* w_arr, size_t n_
             job.rot = rot;
             job.n_k = n_k;
             job.kernel = h->kernel;
-            bgw::run_spectrum(device(h), job, result.data(), &h->timings);
+            if (out_device) {
+                bgw::run_spectrum(device(h), job, static_cast<double*>(out_device), true, &h->timings);
+                device_written = true;
+            } else {
+                bgw::run_spectrum(device(h), job, result.data(), false, &h->timings);
+            }
         }
+    }
+    if (out_device) {
+        if (!device_written && expected)
+            throw Error{"nothing to compute for a device output (empty selection, n_sets or n_w)"};
+        return;
     }
     if (out_len != expected)
         throw Error{"out_len=" + std::to_string(out_len) + " does not match expected length " +
@@ -347,6 +361,38 @@ BgwStatus bgwx_generalized_bulk_flow_compute_c_integral_khat(bgw_generalized_bul
         compute_common(h, w_arr, n_w, has_t_begin, t_begin, t_end, n_t, selected_bubbles, n_selected_bubbles,
                        selected_bubbles != nullptr, time_cutoff, rot.data(), n_khat, out, out_len);
     });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_compute_c_integral_khat_device(
+    bgw_generalized_bulk_flow* bulk_flow, const double* w_arr, size_t n_w, bool has_t_begin, double t_begin,
+    double t_end, size_t n_t, const double* khat, size_t n_khat, const size_t* selected_bubbles,
+    size_t n_selected_bubbles, BgwTimeCutoffConfig time_cutoff, void* out_device, size_t out_len) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        if (!out_device) throw Error{"out_device must not be null"};
+        const double* k = slice(khat, checked_mul(n_khat, 3, "khat"), "khat");
+        if (n_khat == 0) throw Error{"khat must hold at least one direction"};
+        std::vector<double> rot(9 * n_khat);
+        for (size_t q = 0; q < n_khat; ++q) {
+            double kx = k[3 * q], ky = k[3 * q + 1], kz = k[3 * q + 2];
+            double n2 = kx * kx + ky * ky + kz * kz;
+            if (!(std::fabs(n2 - 1.0) <= 1e-9)) throw Error{"khat rows must be unit vectors"};
+            bgw::rotation_for_khat(kx, ky, kz, &rot[9 * q]);
+        }
+        compute_common(h, w_arr, n_w, has_t_begin, t_begin, t_end, n_t, selected_bubbles, n_selected_bubbles,
+                       selected_bubbles != nullptr, time_cutoff, rot.data(), n_khat, nullptr, out_len, out_device);
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_drop_resident_inputs(bgw_generalized_bulk_flow* bulk_flow) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        if (h->dev) bgw::device_drop_resident(h->dev);
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_set_stream(bgw_generalized_bulk_flow* bulk_flow, void* stream) {
+    return run_ffi([&] { bgw::device_set_stream(device(handle(bulk_flow)), stream); });
 }
 
 BgwStatus bgwx_generalized_bulk_flow_set_kernel(bgw_generalized_bulk_flow* bulk_flow, BgwxKernel kernel) {

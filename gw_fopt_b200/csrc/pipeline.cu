@@ -40,7 +40,8 @@ Device* device_create() {
     auto* d = new Device();
     try {
         CUDA_OK(cudaGetDevice(&d->id));
-        CUDA_OK(cudaStreamCreateWithFlags(&d->stream, cudaStreamNonBlocking));
+        CUDA_OK(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
+        d->stream = d->own_stream;
         for (auto& e : d->ev) CUDA_OK(cudaEventCreate(&e));
     } catch (...) {
         delete d;
@@ -51,12 +52,23 @@ Device* device_create() {
 
 void device_destroy(Device* d) { delete d; }
 
+void device_set_stream(Device* d, void* stream) {
+    CUDA_OK(cudaStreamSynchronize(d->stream));
+    d->stream = stream ? static_cast<cudaStream_t>(stream) : d->own_stream;
+}
+
+void device_drop_resident(Device* d) {
+    for (DevBuf* b : {&d->bub, &d->dirs, &d->cos_t, &d->sin2, &d->cos2, &d->coeffs, &d->powers, &d->t_arr,
+                      &d->cutw, &d->w, &d->sel, &d->rot})
+        b->shadow_valid = false;
+}
+
 Device::~Device() {
-    if (stream) {
-        cudaStreamSynchronize(stream);
-        cudaStreamDestroy(stream);
-    }
+    if (stream) cudaStreamSynchronize(stream);
+    if (own_stream) cudaStreamDestroy(own_stream);
     for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : chunk_ev)
         if (e) cudaEventDestroy(e);
 }
 
@@ -480,12 +492,20 @@ __global__ void k_reduce(const double2* __restrict__ partial, size_t n_sel, size
 // ---------------------------------------------------------------------------
 namespace {
 
+// Host -> device copy that is skipped when the bytes equal those of the
+// previous upload into the same buffer (inputs stay resident in HBM).
 template <class T>
 T* upload(Device* dev, DevBuf& buf, const T* host, size_t n, BgwxTimings* tm) {
-    buf.ensure(n * sizeof(T));
-    if (n) {
-        CUDA_OK(cudaMemcpyAsync(buf.p, host, n * sizeof(T), cudaMemcpyHostToDevice, dev->stream));
-        if (tm) tm->h2d_bytes += (double)(n * sizeof(T));
+    const size_t bytes = n * sizeof(T);
+    buf.ensure(bytes);
+    if (bytes) {
+        const unsigned char* hb = reinterpret_cast<const unsigned char*>(host);
+        if (buf.shadow_valid && buf.shadow.size() == bytes && std::memcmp(buf.shadow.data(), hb, bytes) == 0)
+            return static_cast<T*>(buf.p);
+        buf.shadow.assign(hb, hb + bytes);
+        CUDA_OK(cudaMemcpyAsync(buf.p, buf.shadow.data(), bytes, cudaMemcpyHostToDevice, dev->stream));
+        buf.shadow_valid = true;
+        if (tm) tm->h2d_bytes += (double)bytes;
     }
     return static_cast<T*>(buf.p);
 }
@@ -545,7 +565,7 @@ void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_
     }
 }
 
-void run_spectrum(Device* dev, const SpectrumJob& job, double* out, BgwxTimings* tm) {
+void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_device, BgwxTimings* tm) {
     CUDA_OK(cudaSetDevice(dev->id));
     const size_t nd = job.n_cos * job.n_phi;
     const size_t S = job.n_sets, W = job.n_w, K = job.n_k;
@@ -572,7 +592,17 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, BgwxTimings*
     kc = std::min<size_t>(kc, 65535);
     dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
     dev->partial.ensure(kc * job.n_sel * per * sizeof(double2));
-    dev->out.ensure(K * per * sizeof(double2));
+    double2* final_out = out_is_device ? reinterpret_cast<double2*>(out) : nullptr;
+    if (!final_out) {
+        dev->out.ensure(K * per * sizeof(double2));
+        final_out = (double2*)dev->out.p;
+    }
+    const size_t n_chunks = (K + kc - 1) / kc;
+    while (dev->chunk_ev.size() < 3 * n_chunks) {
+        cudaEvent_t e;
+        CUDA_OK(cudaEventCreate(&e));
+        dev->chunk_ev.push_back(e);
+    }
     if (rot) dev->bubrot.ensure(kc * job.n_tot * sizeof(D4));
     dev->counters.ensure(64);
     CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
@@ -588,11 +618,11 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, BgwxTimings*
     if (smem > (size_t)max_optin) throw Error{"n_cos_thetax too large for the shared-memory layout"};
     CUDA_OK(cudaFuncSetAttribute(k_spec_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
-    float ms_masks = 0, ms_spec = 0;
     uint64_t launches = 0;
     CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
-    for (size_t k0 = 0; k0 < K; k0 += kc) {
+    for (size_t k0 = 0, ci = 0; k0 < K; k0 += kc, ++ci) {
         const size_t kn = std::min(kc, K - k0);
+        cudaEvent_t* cev = &dev->chunk_ev[3 * ci];
         const D4* fb = bub;
         if (rot) {
             dim3 g((unsigned)((job.n_tot + 255) / 256), (unsigned)kn);
@@ -601,11 +631,11 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, BgwxTimings*
             ++launches;
             fb = (const D4*)dev->bubrot.p;
         }
-        CUDA_OK(cudaEventRecord(dev->ev[0], dev->stream));
+        CUDA_OK(cudaEventRecord(cev[0], dev->stream));
         launch_masks(dev, fb, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, kn, (double*)dev->tau.p, nullptr,
                      (unsigned long long*)dev->counters.p);
         ++launches;
-        CUDA_OK(cudaEventRecord(dev->ev[1], dev->stream));
+        CUDA_OK(cudaEventRecord(cev[1], dev->stream));
         if (job.kernel == BGWX_KERNEL_FP64_DIRECT) {
             SpecArgs A;
             A.bub = fb;
@@ -639,28 +669,33 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, BgwxTimings*
             ++launches;
             dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
             k_reduce<<<gr, 256, 0, dev->stream>>>((const double2*)dev->partial.p, job.n_sel, per, kn,
-                                                  (double2*)dev->out.p + k0 * per);
+                                                  final_out + k0 * per);
             CUDA_OK(cudaGetLastError());
             ++launches;
         } else {
             launches += launch_factored(dev, job, fb, sel, (const double*)dev->tau.p, cos_t, sin2, cos2, coeffs,
-                                        powers, t_arr, cutw, w, kn, (double2*)dev->out.p + k0 * per);
+                                        powers, t_arr, cutw, w, kn, final_out + k0 * per);
         }
-        CUDA_OK(cudaEventRecord(dev->ev[2], dev->stream));
-        CUDA_OK(cudaEventSynchronize(dev->ev[2]));
-        float a = 0, b = 0;
-        CUDA_OK(cudaEventElapsedTime(&a, dev->ev[0], dev->ev[1]));
-        CUDA_OK(cudaEventElapsedTime(&b, dev->ev[1], dev->ev[2]));
-        ms_masks += a;
-        ms_spec += b;
+        CUDA_OK(cudaEventRecord(cev[2], dev->stream));
     }
     CUDA_OK(cudaEventRecord(dev->ev[5], dev->stream));
-    CUDA_OK(cudaMemcpyAsync(out, dev->out.p, K * per * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
+    if (out_is_device) {
+        if (tm) tm->launches += launches;
+        return;
+    }
+    CUDA_OK(cudaMemcpyAsync(out, final_out, K * per * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
     unsigned long long fbk = 0;
     CUDA_OK(cudaMemcpyAsync(&fbk, dev->counters.p, sizeof fbk, cudaMemcpyDeviceToHost, dev->stream));
     CUDA_OK(cudaStreamSynchronize(dev->stream));
-    float total = 0;
+    float total = 0, ms_masks = 0, ms_spec = 0;
     CUDA_OK(cudaEventElapsedTime(&total, dev->ev[4], dev->ev[5]));
+    for (size_t ci = 0; ci < n_chunks; ++ci) {
+        float a = 0, b = 0;
+        CUDA_OK(cudaEventElapsedTime(&a, dev->chunk_ev[3 * ci], dev->chunk_ev[3 * ci + 1]));
+        CUDA_OK(cudaEventElapsedTime(&b, dev->chunk_ev[3 * ci + 1], dev->chunk_ev[3 * ci + 2]));
+        ms_masks += a;
+        ms_spec += b;
+    }
     if (tm) {
         tm->masks_ms += ms_masks;
         tm->spectrum_ms += ms_spec;

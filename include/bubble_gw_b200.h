@@ -115,6 +115,31 @@ BgwStatus bgwx_generalized_bulk_flow_compute_c_integral_khat(
     double t_end, size_t n_t, const double *khat, size_t n_khat, const size_t *selected_bubbles,
     size_t n_selected_bubbles, BgwTimeCutoffConfig time_cutoff, BgwComplex64 *out, size_t out_len);
 
+/* As bgwx_generalized_bulk_flow_compute_c_integral_khat with the result
+ * written to device memory `out_device` ((K, 2, n_sets, n_w) complex128,
+ * out_len elements) and the work left in flight on the handle's stream: the
+ * call returns after enqueueing, inputs that did not change since the previous
+ * call are not copied again (they stay resident in HBM).  No counterpart in
+ * the reference. */
+BgwStatus bgwx_generalized_bulk_flow_compute_c_integral_khat_device(
+    bgw_generalized_bulk_flow *bulk_flow, const double *w_arr, size_t n_w, bool has_t_begin, double t_begin,
+    double t_end, size_t n_t, const double *khat, size_t n_khat, const size_t *selected_bubbles,
+    size_t n_selected_bubbles, BgwTimeCutoffConfig time_cutoff, void *out_device, size_t out_len);
+
+/* Runs this handle's device work on `stream` (a cudaStream_t; NULL = the
+ * handle's own stream).  No counterpart in the reference. */
+BgwStatus bgwx_generalized_bulk_flow_set_stream(bgw_generalized_bulk_flow *bulk_flow, void *stream);
+
+/* Forgets which inputs are resident on the device, so that the next call
+ * copies every input from the host again (used to measure end-to-end cost).
+ * No counterpart in the reference. */
+BgwStatus bgwx_generalized_bulk_flow_drop_resident_inputs(bgw_generalized_bulk_flow *bulk_flow);
+
+/* Measured device throughput of FP64 FMA (flop/s), FP32 FMA (flop/s) and the
+ * SFU (sin/cos operations/s), the peaks of the spectrum kernels' roofline.
+ * No counterpart in the reference. */
+BgwStatus bgwx_measure_compute_peaks(double *fp64_flops, double *fp32_flops, double *sfu_ops);
+
 /* The rotation R(k) used above, row-major 3x3.  No counterpart in the reference. */
 void bgwx_rotation_for_khat(double kx, double ky, double kz, double *R);
 

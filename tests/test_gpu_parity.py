@@ -101,14 +101,17 @@ def test_capi_case_matches_reference_test_shape(gpu_available):
 
 def test_selected_duplicates_and_late_bubbles(gpu_available):
     c = W.config(1)
-    interior = c.interior.copy()
-    interior[3, 0] = 2.0  # nucleates after t_end: contributes nothing
-    ext = W.periodic_images(interior, 1.0)
+    interior, ext = c.interior, c.exterior
+    t_end = float(np.median(interior[:, 0]))  # half of the bubbles nucleate after t_end
+    late = np.flatnonzero(interior[:, 0] > t_end)
+    early = np.flatnonzero(interior[:, 0] < t_end)
     g = make_flow(interior, ext, 12, 14, [[1.0]], [[5.0]])
-    sel = np.array([1, 3, 1, 5])
-    out = g.compute_c_integral(c.w, t_begin=0.0, t_end=1.5, n_t=64, selected_bubbles=sel)
-    ref = O.compute_c_integral(interior, ext, 12, 14, c.w, 1.5, 64, t_begin=0.0, coefficients=[[1.0]],
+    sel = np.array([early[0], late[0], early[0], early[1]])
+    out = g.compute_c_integral(c.w, t_begin=0.0, t_end=t_end, n_t=64, selected_bubbles=sel)
+    ref = O.compute_c_integral(interior, ext, 12, 14, c.w, t_end, 64, t_begin=0.0, coefficients=[[1.0]],
                                powers=[[5.0]], selected=sel)
+    only_late = g.compute_c_integral(c.w, t_begin=0.0, t_end=t_end, n_t=64, selected_bubbles=late)
+    assert not only_late.any()
     assert err_per_w(out, ref) < FP64_TOL
 
 
