@@ -165,7 +165,10 @@ def run_b200(args):
     g = make_flow(cfg, args.kernel)
     lib = L.lib()
     S, Wn = cfg.coefficients.shape[0], cfg.w.size
-    stream = torch.cuda.current_stream()
+    # a created stream: handle 0 (torch's legacy default stream) would mean "library's own stream"
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    assert stream.cuda_stream != 0
     L.check(lib.bgwx_generalized_bulk_flow_set_stream(g._h, C.c_void_p(stream.cuda_stream)))
     out_dev = torch.empty((K, 2, S, Wn), dtype=torch.complex128, device="cuda")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")

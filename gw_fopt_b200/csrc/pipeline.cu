@@ -587,11 +587,13 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     double* rot = job.rot ? upload(dev, dev->rot, job.rot, 9 * K, tm) : nullptr;
 
     // frames per chunk: bounded by the mask buffer budget
-    const size_t per_k = job.n_sel * nd * sizeof(double) + job.n_sel * per * sizeof(double2);
+    const size_t per_k = job.n_sel * nd * sizeof(double) +
+                         (job.kernel == BGWX_KERNEL_FP64_DIRECT ? job.n_sel * per * sizeof(double2)
+                                                                : factored_bytes_per_frame(job));
     size_t kc = std::max<size_t>(1, std::min(K, mask_budget_bytes() / std::max<size_t>(per_k, 1)));
     kc = std::min<size_t>(kc, 65535);
     dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
-    dev->partial.ensure(kc * job.n_sel * per * sizeof(double2));
+    if (job.kernel == BGWX_KERNEL_FP64_DIRECT) dev->partial.ensure(kc * job.n_sel * per * sizeof(double2));
     double2* final_out = out_is_device ? reinterpret_cast<double2*>(out) : nullptr;
     if (!final_out) {
         dev->out.ensure(K * per * sizeof(double2));

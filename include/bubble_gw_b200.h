@@ -126,8 +126,9 @@ BgwStatus bgwx_generalized_bulk_flow_compute_c_integral_khat_device(
     double t_end, size_t n_t, const double *khat, size_t n_khat, const size_t *selected_bubbles,
     size_t n_selected_bubbles, BgwTimeCutoffConfig time_cutoff, void *out_device, size_t out_len);
 
-/* Runs this handle's device work on `stream` (a cudaStream_t; NULL = the
- * handle's own stream).  No counterpart in the reference. */
+/* Runs this handle's device work on `stream` (a cudaStream_t created by the
+ * caller; NULL selects the handle's own non-blocking stream, so the legacy
+ * default stream cannot be chosen).  No counterpart in the reference. */
 BgwStatus bgwx_generalized_bulk_flow_set_stream(bgw_generalized_bulk_flow *bulk_flow, void *stream);
 
 /* Forgets which inputs are resident on the device, so that the next call
