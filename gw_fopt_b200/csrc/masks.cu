@@ -1,0 +1,448 @@
+// First-collider search with per-bubble candidate lists (exact).
+//
+// For interior bubble a and a collider c with Delta = x_c - x_a (t, x, y, z),
+// the collision delay along any direction x-hat = (1, n) is
+//   tau_c(n) = s_c / (2 d_c),  s_c = -dt^2 + |dx|^2,  d_c = -dt + dx.n,
+// and because d_c <= D_c = |dx| - dt and s_c = D_c (|dx| + dt),
+//   tau_c(n) >= key_c = (|dx| + dt) / 2        for every n with d_c > 0.
+// k_neighbors builds, once per radiating bubble (frame independent, the keys
+// are rotation invariant), the list of the colliders with the smallest keys
+// (radix select on the float keys, then a bitonic sort by (key, index)),
+// kmax = a lower bound of every key outside the list, and
+//   rho1 = max_c (dt^2 + |dx|^2) / D_c,  rho2 = max_c (|dt| + |dx|) / D_c.
+//
+// k_masks_list then decides each direction exactly as the reference
+// (generalized_bulk_flow.rs:127-206, 1003-1018) does -- the unique b passing
+// check(b, c) against every c, or None -- but evaluates only what can matter:
+//   1. argmin m of tau over the list in key order, stopping once
+//      key > tau_best (1 + 1e-12): no later collider can have a smaller tau;
+//   2. check(m, c) for the listed c with key_c <= theta_m, where
+//        theta_m = tau_m (1 + 1e-12) + 64 u (A_m rho1 + Q_m rho2) / d_m
+//      (u = 2^-53).  The rounding error of the reference's check expression is
+//      below 20 u (A_m Q_c + A_c Q_m) while its exact value is at least
+//      2 d_m D_c (key_c - tau_m), so every c with key_c > theta_m passes in
+//      floating point as well and needs no evaluation;
+//   3. if m fails, the passer (if any) is one of the c that m failed against
+//      (r(c, m) = -r(m, c) exactly in IEEE arithmetic); each is verified the
+//      same way.
+// Whenever a bound reaches past the list (or the list has no candidate and is
+// not complete) the direction falls back to the exhaustive scan over all
+// colliders.  Colliders with a near-lightlike interval (D_c tiny) are kept in
+// a small always-checked set; too many of them make the bubble use the
+// exhaustive scan for every direction.
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+
+#include "bgw_internal.h"
+#include "device_common.cuh"
+#include "masks.cuh"
+
+namespace bgw {
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ bool check_pt(const D4& dba, double nb, const D4& dca, const D4& x) {
+    const double nc = mdot(dca, dca);
+    D4 cv;
+    cv.t = dsub(dmul(dba.t, nc), dmul(dca.t, nb));
+    cv.x = dsub(dmul(dba.x, nc), dmul(dca.x, nb));
+    cv.y = dsub(dmul(dba.y, nc), dmul(dca.y, nb));
+    cv.z = dsub(dmul(dba.z, nc), dmul(dca.z, nb));
+    return mdot(cv, x) > 0.0;
+}
+
+// Exhaustive decision for one direction (global memory): argmin, check it
+// against everything, then the failures; the reference loop if more than
+// kMaxFail failures.
+__device__ long exhaustive(const D4* __restrict__ B, size_t n_tot, uint32_t a, const D4& xa, const D4& x) {
+    long best = -1;
+    double best_tau = CUDART_INF;
+    for (size_t b = 0; b < n_tot; ++b) {
+        if (b == a) continue;
+        const D4 dba = dsub4(B[b], xa);
+        const double dot = mdot(dba, x);
+        if (dot > 1e-10) {
+            const double tau = __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
+            if (tau > 0.0 && tau < best_tau) {
+                best_tau = tau;
+                best = (long)b;
+            }
+        }
+    }
+    if (best < 0) return -1;
+    const D4 dm = dsub4(B[best], xa);
+    const double nm = mdot(dm, dm);
+    size_t fails[kMaxFail];
+    int nfail = 0;
+    for (size_t c = 0; c < n_tot; ++c) {
+        if (c == a || (long)c == best) continue;
+        if (!check_pt(dm, nm, dsub4(B[c], xa), x)) {
+            if (nfail < kMaxFail) fails[nfail] = c;
+            ++nfail;
+        }
+    }
+    if (nfail == 0) return best;
+    if (nfail > kMaxFail) {
+        // the reference loop (GBF:162-199)
+        long r = -1;
+        double rt = CUDART_INF;
+        for (size_t b = 0; b < n_tot; ++b) {
+            if (b == a) continue;
+            const D4 dba = dsub4(B[b], xa);
+            const double dsq = mdot(dba, dba);
+            const double dot = mdot(dba, x);
+            if (dot <= 1e-10) continue;
+            const double tau = __ddiv_rn(dsq, dmul(2.0, dot));
+            if (tau <= 0.0 || tau >= rt) continue;
+            bool first = true;
+            for (size_t c = 0; c < n_tot && first; ++c) {
+                if (c == a || c == b) continue;
+                first = check_pt(dba, dsq, dsub4(B[c], xa), x);
+            }
+            if (first) {
+                r = (long)b;
+                rt = tau;
+            }
+        }
+        return r;
+    }
+    for (int f = 0; f < nfail; ++f) {
+        const size_t c = fails[f];
+        const D4 dc = dsub4(B[c], xa);
+        const double dot = mdot(dc, x);
+        if (!(dot > 1e-10)) continue;
+        const double nc = mdot(dc, dc);
+        if (!(__ddiv_rn(nc, dmul(2.0, dot)) > 0.0)) continue;
+        bool ok = true;
+        for (size_t e = 0; e < n_tot && ok; ++e) {
+            if (e == a || e == c) continue;
+            ok = check_pt(dc, nc, dsub4(B[e], xa), x);
+        }
+        if (ok) return (long)c;
+    }
+    return -1;
+}
+
+// ------------------------------------------------------------ k_neighbors
+__device__ __forceinline__ void collider_bounds(const D4& d, double& key, double& D, double& Q, double& A) {
+    const double dx = sqrt(d.x * d.x + d.y * d.y + d.z * d.z);
+    key = fmax(0.5 * (dx + d.t), 0.0);
+    D = dx - d.t;
+    Q = d.t * d.t + dx * dx;
+    A = fabs(d.t) + dx;
+}
+
+__global__ void __launch_bounds__(kNbThreads)
+    k_neighbors(const D4* __restrict__ bub, size_t n_tot, const uint32_t* __restrict__ sel, NbList* __restrict__ out) {
+    __shared__ unsigned hist[2048];
+    __shared__ unsigned s_prefix, s_mask, s_need, s_count, s_nout;
+    __shared__ double s_key[kList];
+    __shared__ int s_idx[kList];
+    __shared__ double s_r1[kNbThreads], s_r2[kNbThreads];
+    const int slot = blockIdx.x;
+    const uint32_t a = sel[slot];
+    const D4 xa = bub[a];
+    NbList* L = out + slot;
+    const size_t n_c = n_tot - 1;  // colliders other than a
+    const bool complete = n_c <= (size_t)kList;
+    auto fbits = [&](size_t c) -> unsigned {
+        double key, D, Q, A;
+        collider_bounds(dsub4(bub[c], xa), key, D, Q, A);
+        return __float_as_uint(__double2float_rd(key));
+    };
+    if (threadIdx.x == 0) {
+        s_prefix = 0;
+        s_mask = 0;
+        s_need = kList;  // rank of the cut value (1-based)
+        s_count = 0;
+        s_nout = 0;
+    }
+    __syncthreads();
+    unsigned cut = 0xffffffffu;  // list = {c : fbits(c) < cut}
+    if (!complete) {
+        const int shifts[3] = {21, 10, 0};
+        const unsigned widths[3] = {11, 11, 10};
+        for (int p = 0; p < 3; ++p) {
+            const unsigned dmask = (1u << widths[p]) - 1u;
+            for (int q = threadIdx.x; q < 2048; q += kNbThreads) hist[q] = 0;
+            __syncthreads();
+            const unsigned pre = s_prefix, pm = s_mask;
+            for (size_t c = threadIdx.x; c < n_tot; c += kNbThreads) {
+                if (c == a) continue;
+                const unsigned v = fbits(c);
+                if ((v & pm) == pre) atomicAdd(&hist[(v >> shifts[p]) & dmask], 1u);
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                unsigned need = s_need, acc = 0, dsel = 0;
+                for (unsigned dg = 0; dg <= dmask; ++dg) {
+                    if (acc + hist[dg] >= need) {
+                        dsel = dg;
+                        break;
+                    }
+                    acc += hist[dg];
+                }
+                s_need = need - acc;
+                s_prefix = pre | (dsel << shifts[p]);
+                s_mask = pm | (dmask << shifts[p]);
+            }
+            __syncthreads();
+        }
+        cut = s_prefix;  // the kList-th smallest float key (bits)
+    }
+    // collect the list (unordered), then sort by (key, index)
+    for (size_t c = threadIdx.x; c < n_tot; c += kNbThreads) {
+        if (c == a) continue;
+        double key, D, Q, A;
+        collider_bounds(dsub4(bub[c], xa), key, D, Q, A);
+        if (complete || __float_as_uint(__double2float_rd(key)) < cut) {
+            const unsigned pos = atomicAdd(&s_count, 1u);
+            if (pos < (unsigned)kList) {
+                s_key[pos] = key;
+                s_idx[pos] = (int)c;
+            }
+        }
+    }
+    __syncthreads();
+    const int n = (int)min(s_count, (unsigned)kList);
+    for (int q = n + threadIdx.x; q < kList; q += kNbThreads) {
+        s_key[q] = CUDART_INF;
+        s_idx[q] = 0x7fffffff;
+    }
+    __syncthreads();
+    // bitonic sort of kList entries (kList a power of two <= 2 * kNbThreads)
+    for (int size = 2; size <= kList; size <<= 1) {
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            for (int q = threadIdx.x; q < kList; q += kNbThreads) {
+                const int p = q ^ stride;
+                if (p > q) {
+                    const bool up = (q & size) == 0;
+                    const double kq = s_key[q], kp = s_key[p];
+                    const int iq = s_idx[q], ip = s_idx[p];
+                    const bool gt = kq > kp || (kq == kp && iq > ip);
+                    if (gt == up) {
+                        s_key[q] = kp;
+                        s_key[p] = kq;
+                        s_idx[q] = ip;
+                        s_idx[p] = iq;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    }
+    // rho bounds over every collider; near-lightlike colliders are kept aside
+    double r1 = 0.0, r2 = 0.0;
+    for (size_t c = threadIdx.x; c < n_tot; c += kNbThreads) {
+        if (c == a) continue;
+        double key, D, Q, A;
+        collider_bounds(dsub4(bub[c], xa), key, D, Q, A);
+        if (D > 1e-6 * A) {
+            r1 = fmax(r1, Q / D);
+            r2 = fmax(r2, A / D);
+        } else {
+            const unsigned pos = atomicAdd(&s_nout, 1u);
+            if (pos < (unsigned)kMaxOutliers) L->outlier[pos] = (int)c;
+        }
+    }
+    s_r1[threadIdx.x] = r1;
+    s_r2[threadIdx.x] = r2;
+    __syncthreads();
+    for (int q = threadIdx.x; q < kList; q += kNbThreads) {
+        L->key[q] = s_key[q];
+        L->idx[q] = s_idx[q];
+    }
+    if (threadIdx.x == 0) {
+        double m1 = 0.0, m2 = 0.0;
+        for (int q = 0; q < kNbThreads; ++q) {
+            m1 = fmax(m1, s_r1[q]);
+            m2 = fmax(m2, s_r2[q]);
+        }
+        L->rho1 = m1 * (1.0 + 1e-12);
+        L->rho2 = m2 * (1.0 + 1e-12);
+        L->count = n;
+        L->kmax = complete ? CUDART_INF : (double)__uint_as_float(cut);
+        const unsigned no = s_nout;
+        L->n_outliers = no <= (unsigned)kMaxOutliers ? (int)no : -1;
+    }
+}
+
+// ------------------------------------------------------------ k_masks_list
+__global__ void __launch_bounds__(kMaskListThreads)
+    k_masks_list(const D4* __restrict__ bub, size_t n_int, size_t n_tot, const uint32_t* __restrict__ sel,
+                 size_t n_sel, const NbList* __restrict__ lists, const D4* __restrict__ dirs, size_t nd,
+                 unsigned n_dblocks, double* __restrict__ tau_out, int32_t* __restrict__ code_out,
+                 unsigned long long* __restrict__ counters) {
+    __shared__ D4 s_pos[kList];
+    __shared__ double s_key[kList];
+    __shared__ int s_idx[kList];
+    __shared__ D4 s_opos[kMaxOutliers];
+    __shared__ int s_oidx[kMaxOutliers];
+    const int k = blockIdx.y;
+    const size_t slot = blockIdx.x / n_dblocks;
+    const size_t d = (size_t)(blockIdx.x % n_dblocks) * kMaskListThreads + threadIdx.x;
+    const D4* B = bub + (size_t)k * n_tot;
+    const uint32_t a = sel[slot];
+    const NbList* L = lists + slot;
+    const int n = L->count;
+    const int no = L->n_outliers;
+    for (int q = threadIdx.x; q < n; q += kMaskListThreads) {
+        const int c = L->idx[q];
+        s_idx[q] = c;
+        s_key[q] = L->key[q];
+        s_pos[q] = B[c];
+    }
+    for (int q = threadIdx.x; q < no; q += kMaskListThreads) {
+        s_oidx[q] = L->outlier[q];
+        s_opos[q] = B[L->outlier[q]];
+    }
+    __syncthreads();
+    if (d >= nd) return;
+    const D4 xa = B[a];
+    const D4 x = dirs[d];
+    const double kmax = L->kmax, rho1 = L->rho1, rho2 = L->rho2;
+    const double u64 = 64.0 * 1.1102230246251565e-16;
+    long result = -1;
+    bool full = no < 0;
+
+    // verifies candidate c (position pc) against the list up to key theta and the outliers
+    auto verify = [&](int c, const D4& dc, double nc, double theta, int* fails, int& nfail) -> bool {
+        bool ok = true;
+        for (int e = 0; e < n; ++e) {
+            if (s_key[e] > theta) break;
+            const int ce = s_idx[e];
+            if (ce == c) continue;
+            if (!check_pt(dc, nc, dsub4(s_pos[e], xa), x)) {
+                ok = false;
+                if (fails) {
+                    if (nfail < kMaxFail) fails[nfail] = e;
+                    ++nfail;
+                } else {
+                    return false;
+                }
+            }
+        }
+        for (int e = 0; e < no; ++e) {
+            const int ce = s_oidx[e];
+            if (ce == c) continue;
+            bool in_list = false;  // already checked above when listed with key <= theta
+            for (int q = 0; q < n && s_key[q] <= theta; ++q) in_list |= (s_idx[q] == ce);
+            if (in_list) continue;
+            if (!check_pt(dc, nc, dsub4(s_opos[e], xa), x)) {
+                ok = false;
+                if (!fails) return false;
+                nfail = kMaxFail + 1;  // outliers are resolved by the exhaustive path
+            }
+        }
+        return ok;
+    };
+    auto theta_of = [&](const D4& dc, double tau, double dot) {
+        const double dx = sqrt(dc.x * dc.x + dc.y * dc.y + dc.z * dc.z);
+        const double A = fabs(dc.t) + dx, Q = dc.t * dc.t + dx * dx;
+        return tau * (1.0 + 1e-12) + u64 * (A * rho1 + Q * rho2) / dot;
+    };
+
+    if (!full) {
+        // 1. argmin of tau in key order
+        double best = CUDART_INF;
+        int bi = -1;
+        bool ended = true;
+        for (int e = 0; e < n; ++e) {
+            if (s_key[e] > best * (1.0 + 1e-12)) {
+                ended = false;
+                break;
+            }
+            const D4 dba = dsub4(s_pos[e], xa);
+            const double dot = mdot(dba, x);
+            if (dot > 1e-10) {
+                const double tau = __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
+                if (tau > 0.0 && tau < best) {
+                    best = tau;
+                    bi = e;
+                }
+            }
+        }
+        if (ended && !(kmax > best * (1.0 + 1e-12))) full = !(bi < 0 && kmax == CUDART_INF);
+        if (!full && bi >= 0) {
+            // 2. verify the argmin
+            const D4 dm = dsub4(s_pos[bi], xa);
+            const double nm = mdot(dm, dm), dotm = mdot(dm, x);
+            const double th = theta_of(dm, best, dotm);
+            if (!(th < kmax)) {
+                full = true;
+            } else {
+                int fails[kMaxFail];
+                int nfail = 0;
+                if (verify(s_idx[bi], dm, nm, th, fails, nfail)) {
+                    result = s_idx[bi];
+                } else if (nfail > kMaxFail) {
+                    full = true;
+                } else {
+                    // 3. the passer, if any, is among the failures
+                    for (int f = 0; f < nfail && result < 0 && !full; ++f) {
+                        const int e = fails[f];
+                        const D4 dc = dsub4(s_pos[e], xa);
+                        const double dot = mdot(dc, x);
+                        if (!(dot > 1e-10)) continue;
+                        const double nc = mdot(dc, dc);
+                        const double tau = __ddiv_rn(nc, dmul(2.0, dot));
+                        if (!(tau > 0.0)) continue;
+                        const double thf = theta_of(dc, tau, dot);
+                        if (!(thf < kmax)) {
+                            full = true;
+                            break;
+                        }
+                        int dummy = 0;
+                        if (verify(s_idx[e], dc, nc, thf, nullptr, dummy)) result = s_idx[e];
+                    }
+                }
+            }
+        }
+    }
+    if (full) {
+        atomicAdd(counters, 1ull);
+        result = exhaustive(B, n_tot, a, xa, x);
+    }
+    const size_t o = ((size_t)k * n_sel + slot) * nd + d;
+    double tau = 0.0;
+    if (result >= 0) {
+        // compute_delta_tab (GBF:457-466)
+        const D4 dba = dsub4(B[result], xa);
+        const double dot = mdot(dba, x);
+        tau = fabs(dot) < 1e-10 ? 0.0 : __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
+    }
+    tau_out[o] = tau;
+    if (code_out)
+        code_out[o] = result < 0 ? -1 : ((size_t)result < n_int ? (int32_t)result : -((int32_t)(result - n_int) + 2));
+}
+
+// ------------------------------------------------------------------ host
+void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames, size_t n_int, size_t n_tot,
+                          const uint32_t* sel, size_t n_sel, const D4* dirs, size_t nd, size_t kn, double* tau,
+                          int32_t* codes, unsigned long long* counters, bool build_lists, uint64_t* launches) {
+    if (n_tot < 2) {
+        // a lone bubble has no collider: every direction is None
+        CUDA_OK(cudaMemsetAsync(tau, 0, kn * n_sel * nd * sizeof(double), dev->stream));
+        if (codes) CUDA_OK(cudaMemsetAsync(codes, 0xff, kn * n_sel * nd * sizeof(int32_t), dev->stream));
+        return;
+    }
+    dev->nblists.ensure(n_sel * sizeof(NbList));
+    if (build_lists) {
+        if (n_sel > 0x7fffffffULL) throw Error{"too many radiating bubbles"};
+        k_neighbors<<<(unsigned)n_sel, kNbThreads, 0, dev->stream>>>(bub_unrot, n_tot, sel, (NbList*)dev->nblists.p);
+        CUDA_OK(cudaGetLastError());
+        if (launches) ++*launches;
+    }
+    const unsigned n_dblocks = (unsigned)((nd + kMaskListThreads - 1) / kMaskListThreads);
+    const size_t gx = (size_t)n_dblocks * n_sel;
+    if (gx > 0x7fffffffULL || kn > 65535) throw Error{"too many (bubble, patch) pairs for one launch"};
+    dim3 grid((unsigned)gx, (unsigned)kn);
+    k_masks_list<<<grid, kMaskListThreads, 0, dev->stream>>>(bub_frames, n_int, n_tot, sel, n_sel,
+                                                             (const NbList*)dev->nblists.p, dirs, nd, n_dblocks, tau,
+                                                             codes, counters);
+    CUDA_OK(cudaGetLastError());
+    if (launches) ++*launches;
+}
+
+}  // namespace bgw

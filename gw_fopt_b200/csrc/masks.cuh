@@ -1,0 +1,31 @@
+// First-collider search with per-bubble candidate lists (masks.cu).
+#pragma once
+
+#include "device_common.cuh"
+
+namespace bgw {
+
+constexpr int kList = 128;           // candidate colliders per radiating bubble
+constexpr int kMaxOutliers = 8;      // always-checked near-lightlike colliders
+constexpr int kMaxFail = 8;          // failures of the argmin resolved without the reference loop
+constexpr int kNbThreads = 256;
+constexpr int kMaskListThreads = 128;
+
+// Candidate list of one radiating bubble (frame independent).
+struct NbList {
+    double key[kList];   // lower bounds (|dx| + dt) / 2 of tau, ascending
+    int idx[kList];      // collider indices (interior then exterior numbering)
+    int outlier[kMaxOutliers];
+    double kmax;         // every collider outside the list has key >= kmax (inf: list complete)
+    double rho1, rho2;   // max (dt^2+|dx|^2)/D and (|dt|+|dx|)/D over the colliders
+    int count;           // entries in the list
+    int n_outliers;      // -1: too many near-lightlike colliders, use the exhaustive scan
+};
+
+// Builds the lists (when build_lists) from the unrotated bubbles and runs the
+// list-based exact search for kn frames.  tau/codes: (kn, n_sel, nd).
+void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames, size_t n_int, size_t n_tot,
+                          const uint32_t* sel, size_t n_sel, const D4* dirs, size_t nd, size_t kn, double* tau,
+                          int32_t* codes, unsigned long long* counters, bool build_lists, uint64_t* launches);
+
+}  // namespace bgw

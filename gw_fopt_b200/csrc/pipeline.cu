@@ -2,7 +2,8 @@
 //
 // Stages, per chunk of k-hat frames:
 //   k_rotate       bubbles (t, x, y, z) rotated by R(k)            [optional]
-//   k_masks_full   exact first-collider search per (k, bubble, patch)
+//   k_neighbors, k_masks_list (masks.cu)
+//                  exact first-collider search per (k, bubble, patch)
 //   k_spec_direct  plain FP64 spectrum: one complex phase per
 //                  (bubble, cos-theta row, t, w), the reference's loop nest
 //   k_reduce       deterministic sum of per-bubble partial spectra
@@ -20,6 +21,7 @@
 
 #include "bgw_internal.h"
 #include "device_common.cuh"
+#include "masks.cuh"
 #include "spectrum_factored.cuh"
 
 namespace bgw {
@@ -88,180 +90,6 @@ __global__ void k_rotate(const D4* __restrict__ bub, const double* __restrict__ 
     o.y = dadd(dadd(dmul(R[3], v.x), dmul(R[4], v.y)), dmul(R[5], v.z));
     o.z = dadd(dadd(dmul(R[6], v.x), dmul(R[7], v.y)), dmul(R[8], v.z));
     out[(size_t)k * n_tot + b] = o;
-}
-
-// ---------------------------------------------------------------------------
-// Exact first-collider search (GBF:127-206, GBF:1003-1018).
-//
-// The reference scans b in index order and accepts b when
-//   d_b = Delta_ab.x > 1e-10,  tau_b = Delta_ab^2 / (2 d_b) in (0, tau_best),
-//   and check(b, c) holds for every c other than a and b.
-// check(b, c) is r(b, c) > 0 with r(b, c) = (Delta_b |Delta_c|^2 -
-// Delta_c |Delta_b|^2) . x; in IEEE arithmetic r(c, b) == -r(b, c) exactly
-// (every product and sum of the negated operands is the negated result), so
-// at most one b passes all of its checks, and the reference returns that b
-// (or None).  This kernel finds it without the O(N^2) scan:
-//   pass 1  m = argmin tau over candidates (d > 1e-10, tau > 0);
-//   pass 2  evaluate check(m, c) for all c, collecting the failures F;
-//   m passes -> m.  Otherwise the passer, if any, lies in F (it passes its
-//   check against m, so m fails against it); each member of F is verified
-//   with a full scan.  More than kMaxFail failures -> the reference loop.
-// All decision arithmetic uses unfused __dmul_rn/__dadd_rn in the reference's
-// operation order, so codes and delays are bitwise the reference's.
-// ---------------------------------------------------------------------------
-constexpr int kMaskThreads = 128;
-constexpr int kMaskTile = 128;
-constexpr int kMaxFail = 8;
-
-__device__ __forceinline__ bool check_point(const D4& dba, double nb, const D4& dca, const D4& x) {
-    double nc = mdot(dca, dca);
-    D4 cv;
-    cv.t = dsub(dmul(dba.t, nc), dmul(dca.t, nb));
-    cv.x = dsub(dmul(dba.x, nc), dmul(dca.x, nb));
-    cv.y = dsub(dmul(dba.y, nc), dmul(dca.y, nb));
-    cv.z = dsub(dmul(dba.z, nc), dmul(dca.z, nb));
-    return mdot(cv, x) > 0.0;
-}
-
-// c passes check(c, e) against every e other than a and c (global memory).
-__device__ bool passes_all(const D4* __restrict__ B, size_t n_tot, uint32_t a, size_t c, const D4& xa, const D4& x) {
-    D4 dc = dsub4(B[c], xa);
-    if (mdot(dc, x) <= 0.0) return false;
-    double nb = mdot(dc, dc);
-    for (size_t e = 0; e < n_tot; ++e) {
-        if (e == a || e == c) continue;
-        if (!check_point(dc, nb, dsub4(B[e], xa), x)) return false;
-    }
-    return true;
-}
-
-// The reference loop verbatim (GBF:162-199), used only when pass 2 overflows.
-__device__ long reference_loop(const D4* __restrict__ B, size_t n_tot, uint32_t a, const D4& xa, const D4& x) {
-    long best = -1;
-    double best_tau = CUDART_INF;
-    for (size_t b = 0; b < n_tot; ++b) {
-        if (b == a) continue;
-        D4 dba = dsub4(B[b], xa);
-        double dsq = mdot(dba, dba);
-        double dot = mdot(dba, x);
-        if (dot <= 1e-10) continue;
-        double tau = __ddiv_rn(dsq, dmul(2.0, dot));
-        if (tau <= 0.0 || tau >= best_tau) continue;
-        bool first = true;
-        for (size_t c = 0; c < n_tot; ++c) {
-            if (c == a || c == b) continue;
-            if (!check_point(dba, dsq, dsub4(B[c], xa), x)) {
-                first = false;
-                break;
-            }
-        }
-        if (first) {
-            best = (long)b;
-            best_tau = tau;
-        }
-    }
-    return best;
-}
-
-__global__ void __launch_bounds__(kMaskThreads)
-    k_masks_full(const D4* __restrict__ bub, size_t n_int, size_t n_tot, const uint32_t* __restrict__ sel,
-                 size_t n_sel, const D4* __restrict__ dirs, size_t nd, unsigned n_dblocks,
-                 double* __restrict__ tau_out, int32_t* __restrict__ code_out,
-                 unsigned long long* __restrict__ counters) {
-    __shared__ D4 tile[kMaskTile];
-    const int k = blockIdx.y;
-    const size_t slot = blockIdx.x / n_dblocks;
-    const size_t d = (size_t)(blockIdx.x % n_dblocks) * kMaskThreads + threadIdx.x;
-    const D4* B = bub + (size_t)k * n_tot;
-    const uint32_t a = sel[slot];
-    const D4 xa = B[a];
-    const bool active = d < nd;
-    const D4 x = active ? dirs[d] : D4{1.0, 0.0, 0.0, 0.0};
-
-    // pass 1: argmin of tau among candidates
-    long best = -1;
-    double best_tau = CUDART_INF;
-    for (size_t base = 0; base < n_tot; base += kMaskTile) {
-        const int nb = (int)min((size_t)kMaskTile, n_tot - base);
-        __syncthreads();
-        for (int q = threadIdx.x; q < nb; q += kMaskThreads) tile[q] = B[base + q];
-        __syncthreads();
-        if (active) {
-            for (int q = 0; q < nb; ++q) {
-                size_t b = base + q;
-                if (b == a) continue;
-                D4 dba = dsub4(tile[q], xa);
-                double dot = mdot(dba, x);
-                if (dot > 1e-10) {
-                    double tau = __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
-                    if (tau > 0.0 && tau < best_tau) {
-                        best_tau = tau;
-                        best = (long)b;
-                    }
-                }
-            }
-        }
-    }
-    // pass 2: check the argmin against everything, collecting failures
-    int nfail = 0;
-    size_t fails[kMaxFail];
-    D4 dbest{};
-    double nbest = 0.0;
-    const bool have = active && best >= 0;
-    if (have) {
-        dbest = dsub4(B[best], xa);
-        nbest = mdot(dbest, dbest);
-    }
-    for (size_t base = 0; base < n_tot; base += kMaskTile) {
-        const int nb = (int)min((size_t)kMaskTile, n_tot - base);
-        __syncthreads();
-        for (int q = threadIdx.x; q < nb; q += kMaskThreads) tile[q] = B[base + q];
-        __syncthreads();
-        if (have) {
-            for (int q = 0; q < nb; ++q) {
-                size_t c = base + q;
-                if (c == a || (long)c == best) continue;
-                if (!check_point(dbest, nbest, dsub4(tile[q], xa), x)) {
-                    if (nfail < kMaxFail) fails[nfail] = c;
-                    ++nfail;
-                }
-            }
-        }
-    }
-    if (!active) return;
-    long result = -1;
-    if (have) {
-        if (nfail == 0) {
-            result = best;
-        } else if (nfail <= kMaxFail) {
-            atomicAdd(counters, 1ull);
-            for (int f = 0; f < nfail && result < 0; ++f) {
-                size_t c = fails[f];
-                D4 dc = dsub4(B[c], xa);
-                double dot = mdot(dc, x);
-                if (!(dot > 1e-10)) continue;
-                double tau = __ddiv_rn(mdot(dc, dc), dmul(2.0, dot));
-                if (!(tau > 0.0)) continue;
-                if (passes_all(B, n_tot, a, c, xa, x)) result = (long)c;
-            }
-        } else {
-            atomicAdd(counters, 1ull);
-            result = reference_loop(B, n_tot, a, xa, x);
-        }
-    }
-    const size_t o = ((size_t)k * n_sel + slot) * nd + d;
-    double tau = 0.0;
-    if (result >= 0) {
-        // compute_delta_tab (GBF:457-466)
-        D4 dba = dsub4(B[result], xa);
-        double dot = mdot(dba, x);
-        tau = fabs(dot) < 1e-10 ? 0.0 : __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
-    }
-    tau_out[o] = tau;
-    if (code_out) {
-        int32_t code = result < 0 ? -1 : ((size_t)result < n_int ? (int32_t)result : -((int32_t)(result - n_int) + 2));
-        code_out[o] = code;
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -518,17 +346,6 @@ size_t mask_budget_bytes() {
     return std::max<size_t>((size_t)256 << 20, std::min(b, cap));
 }
 
-void launch_masks(Device* dev, const D4* bub, size_t n_int, size_t n_tot, const uint32_t* sel, size_t n_sel,
-                  const D4* dirs, size_t nd, size_t kc, double* tau, int32_t* codes, unsigned long long* counters) {
-    unsigned n_dblocks = (unsigned)((nd + kMaskThreads - 1) / kMaskThreads);
-    size_t gx = (size_t)n_dblocks * n_sel;
-    if (gx > 0x7fffffffULL) throw Error{"too many (bubble, patch) pairs for one launch"};
-    dim3 grid((unsigned)gx, (unsigned)kc);
-    k_masks_full<<<grid, kMaskThreads, 0, dev->stream>>>(bub, n_int, n_tot, sel, n_sel, dirs, nd, n_dblocks, tau,
-                                                          codes, counters);
-    CUDA_OK(cudaGetLastError());
-}
-
 }  // namespace
 
 void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_tau, BgwxTimings* tm) {
@@ -542,8 +359,9 @@ void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_
     dev->counters.ensure(64);
     CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
     CUDA_OK(cudaEventRecord(dev->ev[0], dev->stream));
-    launch_masks(dev, bub, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, 1, (double*)dev->tau.p,
-                 (int32_t*)dev->codes.p, (unsigned long long*)dev->counters.p);
+    uint64_t nl = 0;
+    launch_mask_pipeline(dev, bub, bub, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, 1, (double*)dev->tau.p,
+                         (int32_t*)dev->codes.p, (unsigned long long*)dev->counters.p, true, &nl);
     CUDA_OK(cudaEventRecord(dev->ev[1], dev->stream));
     CUDA_OK(cudaMemcpyAsync(out_codes, dev->codes.p, job.n_sel * nd * sizeof(int32_t), cudaMemcpyDeviceToHost,
                             dev->stream));
@@ -558,7 +376,7 @@ void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_
     if (tm) {
         tm->masks_ms += ms;
         tm->total_ms += ms;
-        tm->launches += 1;
+        tm->launches += nl;
         tm->directions += job.n_sel * nd;
         tm->fallbacks += fb;
         tm->d2h_bytes += (double)(job.n_sel * nd * (sizeof(int32_t) + (out_tau ? sizeof(double) : 0)));
@@ -634,9 +452,8 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             fb = (const D4*)dev->bubrot.p;
         }
         CUDA_OK(cudaEventRecord(cev[0], dev->stream));
-        launch_masks(dev, fb, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, kn, (double*)dev->tau.p, nullptr,
-                     (unsigned long long*)dev->counters.p);
-        ++launches;
+        launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, kn, (double*)dev->tau.p,
+                             nullptr, (unsigned long long*)dev->counters.p, k0 == 0, &launches);
         CUDA_OK(cudaEventRecord(cev[1], dev->stream));
         if (job.kernel == BGWX_KERNEL_FP64_DIRECT) {
             SpecArgs A;

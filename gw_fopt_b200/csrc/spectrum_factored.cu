@@ -278,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_spec_factored(FactArgs A) {
             E_re[wl * 32 + b] = c;
             E_im[wl * 32 + b] = s;
         }
-        for (int q = tid; q < A.bpt * NQ; q += kThreads) Pst[q] = 0.0;
+        for (int q = tid; q < 32 * kMaxQ; q += kThreads) Pst[q] = 0.0;  // layout [bubble][kMaxQ]
         double acc[kTM][kTN];
         Real cacc[kTM][kTN];
 #pragma unroll
