@@ -14,13 +14,15 @@
 // beta comes from the collision structure without evaluating every patch at
 // every t: with q_j = w_j g(phi_j) (g = cos 2phi, sin 2phi) and
 //   f = sum_m a_m (tau_j / dt)^{p_m} exp(-(dt - tau_j) / width)   (collided),
-//   dt^3 sum_j q_j f_j = dt^3 (G - P0(k)) + sum_m a_m dt^{3-p_m} e^{-dt/width} Pm(k),
-// where G = sum_j q_j and P0, Pm are prefix sums over the patches already
-// collided at step k of q_j and q_j tau_j^{p_m} e^{tau_j/width}.  k_events
+//   dt^3 sum_j q_j f_j = dt^3 U(k) + sum_m a_m dt^{3-p_m} e^{-dt/width} Pm(k),
+// where U(k) sums q_j over the patches not yet collided at step k and Pm(k)
+// sums q_j tau_j^{p_m} e^{tau_j/width} over those already collided.  k_events
 // sorts each row's collided patches by the first time step at which the
 // reference's test (t_k - t_a) >= tau_j holds (exact FP64 comparisons), in
-// buckets of kKC steps; the GEMM kernel turns running prefix sums into beta
-// tile by tile.
+// buckets of kKC steps, and stores U at every bucket boundary as a backward
+// sum of the remaining terms (forming it as total minus collided cancels
+// catastrophically once most patches have collided); the GEMM kernel turns
+// running prefix sums into beta tile by tile.
 //
 // Kernels:
 //   k_time_tables   per bubble and t: dt^3 and dt^{3-p} e^{-dt/width}
@@ -79,11 +81,12 @@ __global__ void __launch_bounds__(256)
              int n_sel, int n_cos, int n_phi, const double* __restrict__ t_arr, int n_t,
              const double* __restrict__ cos2, const double* __restrict__ sin2, const double* __restrict__ powers,
              int SM, int has_damp, double damp, long n_rows, int NB, int* __restrict__ ev_off,
-             int* __restrict__ ev_k, Real* __restrict__ ev_q) {
+             int* __restrict__ ev_k, Real* __restrict__ ev_q, double2* __restrict__ ev_unc) {
     extern __shared__ int sm_ev[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long row = (long)blockIdx.x * (blockDim.x >> 5) + warp;
-    int* hist = sm_ev + warp * 2 * (NB + 1);
+    const int per_warp = 2 * (NB + 1) + 4 * NB + 2;  // ints: hist, run, then 2*NB doubles (8-byte aligned)
+    int* hist = sm_ev + warp * per_warp;
     int* run = hist + (NB + 1);
     if (row >= n_rows) return;
     const int slot = (int)((row / n_cos) % n_sel);
@@ -155,6 +158,60 @@ __global__ void __launch_bounds__(256)
             }
         }
     }
+    __syncwarp();
+    // Uncollided sums U[c] = sum of q over the patches not collided before
+    // bucket c: the never-colliding patches plus the events of buckets >= c,
+    // accumulated backwards (a sum of the remaining terms, never a difference
+    // of two large sums).  Per-bucket sums are formed in lane order.
+    double* bsum = reinterpret_cast<double*>(run + (NB + 1));  // [NB][2] after hist/run
+    for (int b = lane; b < NB; b += 32) {
+        bsum[2 * b] = 0.0;
+        bsum[2 * b + 1] = 0.0;
+    }
+    __syncwarp();
+    double nc = 0.0, ns = 0.0;  // never collided within the grid (lane 0 accumulates)
+    for (int j0 = 0; j0 < n_phi; j0 += 32) {
+        const int j = j0 + lane;
+        int kj;
+        const int b = bucket_of(j, kj);
+        double qc = 0.0, qs = 0.0;
+        if (j < n_phi) {
+            const double wj = (j == 0 || j == n_phi - 1) ? 0.5 : 1.0;
+            qc = wj * cos2[j];
+            qs = wj * sin2[j];
+        }
+        const unsigned m = __match_any_sync(full, b);
+        const bool leader = lane == __ffs(m) - 1;
+        double gc = 0.0, gs = 0.0;
+        for (int l = 0; l < 32; ++l) {
+            const double vc = __shfl_sync(full, qc, l), vs = __shfl_sync(full, qs, l);
+            const int bl = __shfl_sync(full, b, l);
+            const bool valid_l = j0 + l < n_phi;
+            if (leader && valid_l && bl == b) {
+                gc += vc;
+                gs += vs;
+            }
+            if (lane == 0 && valid_l && bl < 0) {
+                nc += vc;
+                ns += vs;
+            }
+        }
+        if (leader && b >= 0) {
+            bsum[2 * b] += gc;
+            bsum[2 * b + 1] += gs;
+        }
+        __syncwarp();
+    }
+    if (lane == 0) {
+        double2* U = ev_unc + (size_t)row * (NB + 1);
+        double uc = nc, us = ns;
+        U[NB] = make_double2(uc, us);
+        for (int c = NB - 1; c >= 0; --c) {
+            uc += bsum[2 * c];
+            us += bsum[2 * c + 1];
+            U[c] = make_double2(uc, us);
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -175,8 +232,8 @@ struct FactArgs {
     const int* ev_off;     // (rows, NB+1)
     const int* ev_k;       // (rows, n_phi)
     const void* ev_q;      // (rows, n_phi, NQ) Real
+    const double2* ev_unc; // (rows, NB+1): uncollided sums of q before bucket c
     int NB;
-    double G_cos, G_sin;   // sum_j w_j cos/sin(2 phi_j)
     double dt, dphi, dcos;
     int bpt;               // bubbles per column tile
     int tiles_per_frame;
@@ -323,15 +380,20 @@ __global__ void __launch_bounds__(kThreads, 1) k_spec_factored(FactArgs A) {
                         const int e0 = off[ch], e1 = off[ch + 1];
                         const int* ek = A.ev_k + (size_t)row * A.n_phi;
                         const Real* eq = evq + (size_t)row * A.n_phi * NQ;
-                        double p0 = Pst[b * kMaxQ + g];
+                        // uncollided patches: those of later buckets plus this bucket's with k_e > k
+                        double unc = g ? A.ev_unc[(size_t)row * (A.NB + 1) + ch + 1].y
+                                       : A.ev_unc[(size_t)row * (A.NB + 1) + ch + 1].x;
                         double pm[8];
                         for (int m = 0; m < A.M; ++m) pm[m] = Pst[b * kMaxQ + 2 + 2 * (s * A.M + m) + g];
                         for (int e = e0; e < e1; ++e) {
-                            if (ek[e] > k) continue;
-                            p0 += (double)eq[(size_t)e * NQ + g];
-                            for (int m = 0; m < A.M; ++m) pm[m] += (double)eq[(size_t)e * NQ + 2 + 2 * (s * A.M + m) + g];
+                            if (ek[e] > k) {
+                                unc += (double)eq[(size_t)e * NQ + g];
+                            } else {
+                                for (int m = 0; m < A.M; ++m)
+                                    pm[m] += (double)eq[(size_t)e * NQ + 2 + 2 * (s * A.M + m) + g];
+                            }
                         }
-                        double v = d3 * ((g ? A.G_sin : A.G_cos) - p0);
+                        double v = d3 * unc;
                         for (int m = 0; m < A.M; ++m) v += A.coeffs[s * A.M + m] * Drow[1 + s * A.M + m] * pm[m];
                         beta = row_factor * A.cutw[k] * ((k == 0 || k == A.n_t - 1) ? 0.5 : 1.0) * v;
                     }
@@ -478,15 +540,17 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     dev->ev_off.ensure((size_t)rows * (NB + 1) * sizeof(int));
     dev->ev_k.ensure((size_t)rows * n_phi * sizeof(int));
     dev->ev_q.ensure((size_t)rows * n_phi * NQ * sizeof(Real));
+    dev->ev_unc.ensure((size_t)rows * (NB + 1) * sizeof(double2));
     {
         const int warps = 8;
-        size_t smem = (size_t)warps * 2 * (NB + 1) * sizeof(int);
+        size_t smem = (size_t)warps * (2 * (NB + 1) + 4 * NB + 2) * sizeof(int);
         if (smem > 200 * 1024) throw Error{"n_t too large for the event kernel"};
         CUDA_OK(cudaFuncSetAttribute(k_events<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         unsigned blocks = (unsigned)((rows + warps - 1) / warps);
         k_events<Real><<<blocks, warps * 32, smem, dev->stream>>>(
             tau, bub_frames, sel, n_sel, n_cos, n_phi, t_arr, n_t, cos2, sin2, powers, SM, job.has_damping ? 1 : 0,
-            job.damping, rows, NB, (int*)dev->ev_off.p, (int*)dev->ev_k.p, (Real*)dev->ev_q.p);
+            job.damping, rows, NB, (int*)dev->ev_off.p, (int*)dev->ev_k.p, (Real*)dev->ev_q.p,
+            (double2*)dev->ev_unc.p);
         CUDA_OK(cudaGetLastError());
         ++launches;
     }
@@ -512,15 +576,8 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     A.ev_off = (const int*)dev->ev_off.p;
     A.ev_k = (const int*)dev->ev_k.p;
     A.ev_q = dev->ev_q.p;
+    A.ev_unc = (const double2*)dev->ev_unc.p;
     A.NB = NB;
-    double gc = 0.0, gs = 0.0;
-    for (int j = 0; j < n_phi; ++j) {
-        double wj = (j == 0 || j == n_phi - 1) ? 0.5 : 1.0;
-        gc += wj * job.cos2phi[j];
-        gs += wj * job.sin2phi[j];
-    }
-    A.G_cos = gc;
-    A.G_sin = gs;
     A.dt = job.dt;
     A.dphi = 2.0 * M_PI / (double)n_phi;
     A.dcos = 2.0 / (double)(n_cos - 1);
@@ -562,7 +619,7 @@ size_t factored_bytes_per_frame(const SpectrumJob& job) {
     const size_t rows = job.n_sel * job.n_cos;
     const size_t bpt = std::min<size_t>(32, kCols / (2 * job.n_sets));
     const size_t tiles = (job.n_sel + bpt - 1) / bpt;
-    return rows * ((NB + 1) * sizeof(int) + job.n_phi * (sizeof(int) + NQ * real)) +
+    return rows * ((NB + 1) * (sizeof(int) + sizeof(double2)) + job.n_phi * (sizeof(int) + NQ * real)) +
            tiles * 2 * job.n_sets * job.n_w * sizeof(double2);
 }
 
