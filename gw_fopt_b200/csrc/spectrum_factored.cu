@@ -46,13 +46,12 @@
 
 namespace bgw {
 
-constexpr int kKC = 16;          // time steps per chunk (GEMM k-tile, event bucket)
+constexpr int kKC = 16;          // time steps per GEMM k-tile
 constexpr int kWT = 64;          // frequencies per CTA
 constexpr int kRows = 2 * kWT;   // GEMM rows: (Re, Im) of each frequency
 constexpr int kCols = 64;        // GEMM columns per CTA
 constexpr int kThreads = 256;
 constexpr int kTM = 8, kTN = 4;  // register tile per thread
-constexpr int kMaxQ = 2 + 2 * 8; // q values per event: (P0 cos, P0 sin) + 2 per (set, term), <= 8 terms
 
 // ---------------------------------------------------------------------------
 __global__ void k_time_tables(const D4* __restrict__ bub, const uint32_t* __restrict__ sel, int n_sel,
@@ -74,111 +73,88 @@ __global__ void k_time_tables(const D4* __restrict__ bub, const uint32_t* __rest
 }
 
 // ---------------------------------------------------------------------------
-// One warp per row (frame, slot, i): events sorted by bucket, stable in j.
+// k_beta: one warp per row (frame, slot, i).  The row's collided patches
+// become events at the first step k_j with (t_k - t_a) >= tau_j (exact FP64
+// comparisons, GBF:405), counting-sorted (stable in j) into blocks of 32
+// steps.  Block b covers k = 32 b + lane: each lane gathers its step's event
+// weights, a warp inclusive scan gives the collided sums Pm(k) and a warp
+// exclusive suffix scan plus the backward block totals gives the uncollided
+// sums U(k) -- both are sums of the terms they stand for, never differences.
+// beta(k) = rf_i u_k cut_k [dt^3 U(k) + sum_m a_m dt^{3-p_m} e^{-dt/w} Pm(k)]
+// is written to beta[frame][i][col][k], col = slot*2S + 2s + g.
+struct BetaArgs {
+    const double* tau;     // (kn, n_sel, n_cos*n_phi)
+    const D4* bub;         // bubbles (frame 0; times are frame independent)
+    const uint32_t* sel;
+    int n_sel, n_cos, n_phi, n_t, S, M;
+    const double* t_arr;
+    const double* cutw;
+    const double* cos_t;
+    const double* cos2;
+    const double* sin2;
+    const double* powers;  // (S*M)
+    const double* coeffs;  // (S*M)
+    const double* D;       // (n_sel, n_t, 1+S*M)
+    int has_damp;
+    double damp;
+    double dphi, dcos, dt;
+    long n_rows;           // kn * n_sel * n_cos
+    int nblk;              // ceil(n_t / 32)
+    long cols_pad;         // columns per (frame, i), padded
+    int t_pad;             // row length of beta
+    int per_warp_bytes;
+};
+
 template <class Real>
-__global__ void __launch_bounds__(256)
-    k_events(const double* __restrict__ tau, const D4* __restrict__ bub, const uint32_t* __restrict__ sel,
-             int n_sel, int n_cos, int n_phi, const double* __restrict__ t_arr, int n_t,
-             const double* __restrict__ cos2, const double* __restrict__ sin2, const double* __restrict__ powers,
-             int SM, int has_damp, double damp, long n_rows, int NB, int* __restrict__ ev_off,
-             int* __restrict__ ev_k, Real* __restrict__ ev_q, double2* __restrict__ ev_unc) {
-    extern __shared__ int sm_ev[];
+__global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ beta) {
+    extern __shared__ __align__(16) unsigned char sm_b[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long row = (long)blockIdx.x * (blockDim.x >> 5) + warp;
-    const int per_warp = 2 * (NB + 1) + 4 * NB + 2;  // ints: hist, run, then 2*NB doubles (8-byte aligned)
-    int* hist = sm_ev + warp * per_warp;
-    int* run = hist + (NB + 1);
-    if (row >= n_rows) return;
-    const int slot = (int)((row / n_cos) % n_sel);
-    const double ta = bub[sel[slot]].t;
-    const double* trow = tau + (size_t)row * n_phi;
-    const int NQ = 2 + 2 * SM;
-    for (int b = lane; b <= NB; b += 32) hist[b] = 0;
-    __syncwarp();
-    auto bucket_of = [&](int j, int& kj) -> int {
-        kj = n_t;
-        if (j >= n_phi) return -1;
+    if (row >= A.n_rows) return;
+    const int SM = A.S * A.M, NQ = 2 + 2 * SM, NB = A.nblk;
+    unsigned char* base = sm_b + (size_t)warp * A.per_warp_bytes;
+    double* evq = reinterpret_cast<double*>(base);             // [n_phi][NQ]
+    double* btot = evq + (size_t)A.n_phi * NQ;                  // [NB][2] block totals of q0
+    double* uend = btot + 2 * NB;                               // [NB][2] uncollided after block
+    int* evk = reinterpret_cast<int*>(uend + 2 * NB);           // [n_phi]
+    int* boff = evk + A.n_phi;                                  // [NB+1]
+    int* brun = boff + NB + 1;                                  // [NB]
+    const int slot = (int)((row / A.n_cos) % A.n_sel);
+    const int i = (int)(row % A.n_cos);
+    const long frame = row / ((long)A.n_cos * A.n_sel);
+    const double ta = A.bub[A.sel[slot]].t;
+    const double* trow = A.tau + (size_t)row * A.n_phi;
+    const unsigned full = 0xffffffffu;
+    auto block_of = [&](int j, int& kj) -> int {
+        kj = A.n_t;
+        if (j >= A.n_phi) return -2;  // not a patch
         const double tj = trow[j];
-        if (!(tj > 0.0)) return -1;
-        int lo = 0, hi = n_t;  // first k with (t_k - t_a) >= tau_j (GBF:405)
+        if (!(tj > 0.0)) return -1;    // never collides
+        int lo = 0, hi = A.n_t;
         while (lo < hi) {
-            int mid = (lo + hi) >> 1;
-            if (t_arr[mid] - ta >= tj) hi = mid;
+            const int mid = (lo + hi) >> 1;
+            if (A.t_arr[mid] - ta >= tj) hi = mid;
             else lo = mid + 1;
         }
         kj = lo;
-        return lo < n_t ? lo / kKC : -1;
+        return lo < A.n_t ? lo >> 5 : -1;
     };
-    const unsigned full = 0xffffffffu;
-    for (int j0 = 0; j0 < n_phi; j0 += 32) {
-        int kj;
-        const int b = bucket_of(j0 + lane, kj);
-        const unsigned m = __match_any_sync(full, b);
-        if (b >= 0 && lane == __ffs(m) - 1) hist[b] += __popc(m);
-        __syncwarp();
-    }
-    if (lane == 0) {
-        int acc = 0;
-        for (int b = 0; b < NB; ++b) {
-            int c = hist[b];
-            hist[b] = acc;
-            run[b] = acc;
-            acc += c;
-        }
-        hist[NB] = acc;
-    }
-    __syncwarp();
-    int* off = ev_off + (size_t)row * (NB + 1);
-    for (int b = lane; b <= NB; b += 32) off[b] = hist[b];
-    const unsigned lt = (1u << lane) - 1u;
-    for (int j0 = 0; j0 < n_phi; j0 += 32) {
-        const int j = j0 + lane;
-        int kj;
-        const int b = bucket_of(j, kj);
-        const unsigned m = __match_any_sync(full, b);
-        int pos = 0;
-        if (b >= 0) pos = run[b] + __popc(m & lt);
-        __syncwarp();
-        if (b >= 0 && lane == __ffs(m) - 1) run[b] += __popc(m);
-        __syncwarp();
-        if (b >= 0) {
-            const size_t e = (size_t)row * n_phi + pos;
-            ev_k[e] = kj;
-            const double tj = trow[j];
-            const double wj = (j == 0 || j == n_phi - 1) ? 0.5 : 1.0;
-            const double qc = wj * cos2[j], qs = wj * sin2[j];
-            Real* q = ev_q + e * NQ;
-            q[0] = (Real)qc;
-            q[1] = (Real)qs;
-            const double ed = has_damp ? exp(tj / damp) : 1.0;
-            for (int t = 0; t < SM; ++t) {
-                const double f = pow(tj, powers[t]) * ed;
-                q[2 + 2 * t] = (Real)(qc * f);
-                q[3 + 2 * t] = (Real)(qs * f);
-            }
-        }
-    }
-    __syncwarp();
-    // Uncollided sums U[c] = sum of q over the patches not collided before
-    // bucket c: the never-colliding patches plus the events of buckets >= c,
-    // accumulated backwards (a sum of the remaining terms, never a difference
-    // of two large sums).  Per-bucket sums are formed in lane order.
-    double* bsum = reinterpret_cast<double*>(run + (NB + 1));  // [NB][2] after hist/run
     for (int b = lane; b < NB; b += 32) {
-        bsum[2 * b] = 0.0;
-        bsum[2 * b + 1] = 0.0;
+        boff[b] = 0;
+        btot[2 * b] = btot[2 * b + 1] = 0.0;
     }
     __syncwarp();
-    double nc = 0.0, ns = 0.0;  // never collided within the grid (lane 0 accumulates)
-    for (int j0 = 0; j0 < n_phi; j0 += 32) {
+    // pass 1: block counts, block totals of q0, never-collided sums (lane order)
+    double nc = 0.0, ns = 0.0;
+    for (int j0 = 0; j0 < A.n_phi; j0 += 32) {
         const int j = j0 + lane;
         int kj;
-        const int b = bucket_of(j, kj);
+        const int b = block_of(j, kj);
         double qc = 0.0, qs = 0.0;
-        if (j < n_phi) {
-            const double wj = (j == 0 || j == n_phi - 1) ? 0.5 : 1.0;
-            qc = wj * cos2[j];
-            qs = wj * sin2[j];
+        if (b >= -1) {
+            const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
+            qc = wj * A.cos2[j];
+            qs = wj * A.sin2[j];
         }
         const unsigned m = __match_any_sync(full, b);
         const bool leader = lane == __ffs(m) - 1;
@@ -186,30 +162,130 @@ __global__ void __launch_bounds__(256)
         for (int l = 0; l < 32; ++l) {
             const double vc = __shfl_sync(full, qc, l), vs = __shfl_sync(full, qs, l);
             const int bl = __shfl_sync(full, b, l);
-            const bool valid_l = j0 + l < n_phi;
-            if (leader && valid_l && bl == b) {
+            if (leader && bl == b) {
                 gc += vc;
                 gs += vs;
             }
-            if (lane == 0 && valid_l && bl < 0) {
+            if (lane == 0 && bl == -1) {
                 nc += vc;
                 ns += vs;
             }
         }
         if (leader && b >= 0) {
-            bsum[2 * b] += gc;
-            bsum[2 * b + 1] += gs;
+            boff[b] += __popc(m);
+            btot[2 * b] += gc;
+            btot[2 * b + 1] += gs;
         }
         __syncwarp();
     }
     if (lane == 0) {
-        double2* U = ev_unc + (size_t)row * (NB + 1);
-        double uc = nc, us = ns;
-        U[NB] = make_double2(uc, us);
-        for (int c = NB - 1; c >= 0; --c) {
-            uc += bsum[2 * c];
-            us += bsum[2 * c + 1];
-            U[c] = make_double2(uc, us);
+        int acc = 0;
+        for (int b = 0; b < NB; ++b) {
+            const int c = boff[b];
+            boff[b] = acc;
+            brun[b] = acc;
+            acc += c;
+        }
+        boff[NB] = acc;
+        double uc = nc, us = ns;  // uncollided after the last block: never-colliding patches
+        for (int b = NB - 1; b >= 0; --b) {
+            uend[2 * b] = uc;
+            uend[2 * b + 1] = us;
+            uc += btot[2 * b];
+            us += btot[2 * b + 1];
+        }
+    }
+    __syncwarp();
+    // pass 2: scatter events (stable in j within a block)
+    const unsigned lt = (1u << lane) - 1u;
+    for (int j0 = 0; j0 < A.n_phi; j0 += 32) {
+        const int j = j0 + lane;
+        int kj;
+        const int b = block_of(j, kj);
+        const unsigned m = __match_any_sync(full, b);
+        int pos = 0;
+        if (b >= 0) pos = brun[b] + __popc(m & lt);
+        __syncwarp();
+        if (b >= 0 && lane == __ffs(m) - 1) brun[b] += __popc(m);
+        __syncwarp();
+        if (b >= 0) {
+            evk[pos] = kj;
+            const double tj = trow[j];
+            const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
+            const double qc = wj * A.cos2[j], qs = wj * A.sin2[j];
+            double* q = evq + (size_t)pos * NQ;
+            q[0] = qc;
+            q[1] = qs;
+            const double ed = A.has_damp ? exp(tj / A.damp) : 1.0;
+            for (int t = 0; t < SM; ++t) {
+                const double f = pow(tj, A.powers[t]) * ed;
+                q[2 + 2 * t] = qc * f;
+                q[3 + 2 * t] = qs * f;
+            }
+        }
+    }
+    __syncwarp();
+    // pass 3: beta over the blocks of 32 steps
+    const double ci = A.cos_t[i];
+    const double vi = (i == 0 || i == A.n_cos - 1) ? 0.5 : 1.0;
+    const double rf = (0.5 * (1.0 - ci * ci) * A.dphi) * (A.dcos * vi) * A.dt * (1.0 / (6.0 * CUDART_PI));
+    Real* brow = beta + ((size_t)frame * A.n_cos + i) * A.cols_pad * A.t_pad + (size_t)slot * 2 * A.S * A.t_pad;
+    double pstart[16];
+#pragma unroll
+    for (int q = 0; q < 16; ++q) pstart[q] = 0.0;
+    for (int b = 0; b < NB; ++b) {
+        const int k = (b << 5) + lane;
+        double h[18];
+#pragma unroll
+        for (int q = 0; q < 18; ++q) h[q] = 0.0;
+        for (int e = boff[b]; e < boff[b + 1]; ++e) {
+            if (evk[e] != k) continue;
+#pragma unroll
+            for (int q = 0; q < 18; ++q)
+                if (q < NQ) h[q] += evq[(size_t)e * NQ + q];
+        }
+        // exclusive suffix over lanes of the uncollided weights
+        double uc = h[0], us = h[1];
+        for (int o = 1; o < 32; o <<= 1) {
+            const double tc = __shfl_down_sync(full, uc, o), ts = __shfl_down_sync(full, us, o);
+            if (lane + o < 32) {
+                uc += tc;
+                us += ts;
+            }
+        }
+        double xc = __shfl_down_sync(full, uc, 1), xs = __shfl_down_sync(full, us, 1);
+        if (lane == 31) xc = xs = 0.0;
+        const double Uc = uend[2 * b] + xc, Us = uend[2 * b + 1] + xs;
+        // inclusive prefix over lanes of the collided weights
+#pragma unroll
+        for (int q = 2; q < 18; ++q) {
+            if (q >= NQ) break;
+            double v = h[q];
+            for (int o = 1; o < 32; o <<= 1) {
+                const double t = __shfl_up_sync(full, v, o);
+                if (lane >= o) v += t;
+            }
+            h[q] = pstart[q - 2] + v;
+            pstart[q - 2] += __shfl_sync(full, v, 31);
+        }
+        if (k < A.n_t) {
+            const double* Drow = A.D + ((size_t)slot * A.n_t + k) * (1 + SM);
+            const double d3 = Drow[0];
+            const double wk = rf * A.cutw[k] * ((k == 0 || k == A.n_t - 1) ? 0.5 : 1.0);
+            for (int s = 0; s < A.S; ++s) {
+                double vc = d3 * Uc, vs = d3 * Us;
+                for (int m = 0; m < A.M; ++m) {
+                    const int t = s * A.M + m;
+                    const double f = A.coeffs[t] * Drow[1 + t];
+                    vc += f * h[2 + 2 * t];
+                    vs += f * h[3 + 2 * t];
+                }
+                const bool on = d3 != 0.0;
+                brow[(size_t)(2 * s) * A.t_pad + k] = on ? (Real)(wk * vc) : (Real)0;
+                brow[(size_t)(2 * s + 1) * A.t_pad + k] = on ? (Real)(wk * vs) : (Real)0;
+            }
+        } else if (k < A.t_pad) {
+            for (int c = 0; c < 2 * A.S; ++c) brow[(size_t)c * A.t_pad + k] = (Real)0;
         }
     }
 }
@@ -220,33 +296,24 @@ struct FactArgs {
     size_t n_tot;
     const uint32_t* sel;
     int n_sel;
-    int n_cos, n_phi, n_t, n_w;
-    int S, M;
-    const double* cos_t;
+    int n_cos, n_t, n_w;
+    int S;
     const double* t_arr;
-    const double* cutw;
     const double* w;
-    const double* coeffs;  // (S, M)
-    const double* D;       // (n_sel, n_t, 1+S*M)
+    const double* cos_t;
     const int* kfirst;     // (n_sel)
-    const int* ev_off;     // (rows, NB+1)
-    const int* ev_k;       // (rows, n_phi)
-    const void* ev_q;      // (rows, n_phi, NQ) Real
-    const double2* ev_unc; // (rows, NB+1): uncollided sums of q before bucket c
-    int NB;
-    double dt, dphi, dcos;
+    const void* beta;      // (kn, n_cos, cols_pad, t_pad) Real
+    long cols_pad;
+    int t_pad;
+    double dt;
     int bpt;               // bubbles per column tile
     int tiles_per_frame;
     double2* partial;      // (kn, tiles_per_frame, 2, S, W)
 };
 
-struct SmemF {
-    double anchor_re[kWT], anchor_im[kWT];
-};
-
 // sin/cos of an FP64 argument: FP64 kernel uses sincos; the mixed kernel
-// reduces the argument modulo 2 pi in FP64 (Cody-Waite, two constants) and
-// evaluates sincosf on the reduced FP32 argument.
+// reduces the argument modulo 2 pi in FP64 and evaluates sincosf on the
+// reduced FP32 argument.
 template <class Real>
 __device__ __forceinline__ void phase(double arg, double& s, double& c);
 
@@ -271,35 +338,32 @@ __device__ __forceinline__ void phase<float>(double arg, double& s, double& c) {
 }
 
 template <class Real>
-__global__ void __launch_bounds__(kThreads, 1) k_spec_factored(FactArgs A) {
+__global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
-    // shared-memory layout
-    Real* Msm = reinterpret_cast<Real*>(smem);                       // [kKC][kRows]
-    Real* Bsm = Msm + kKC * kRows;                                   // [kKC][kCols]
-    double* Pn_re = reinterpret_cast<double*>(Bsm + kKC * kCols);     // [kKC][kWT]
+    constexpr int BP = kKC + (sizeof(Real) == 4 ? 4 : 2);        // padded k-stride of the beta tile
+    Real* Msm = reinterpret_cast<Real*>(smem);                   // [kKC][kRows]
+    Real* Bsm = Msm + kKC * kRows;                               // [kCols][BP]
+    double* Pn_re = reinterpret_cast<double*>(Bsm + kCols * BP);   // [kKC][kWT]
     double* Pn_im = Pn_re + kKC * kWT;
-    double* E_re = Pn_im + kKC * kWT;                                // [kWT][bpt]
+    double* E_re = Pn_im + kKC * kWT;                            // [kWT][32]
     double* E_im = E_re + kWT * 32;
-    double2* Yt = reinterpret_cast<double2*>(E_im + kWT * 32);        // [kCols][kWT]
-    double2* Cacc = Yt + kCols * kWT;                                // [kWT][S][2]
-    double* Pst = reinterpret_cast<double*>(Cacc + kWT * A.S * 2);    // [bpt][NQ]
-    double* anc = Pst + 32 * kMaxQ;                                  // [2][kWT]
-    int* binfo = reinterpret_cast<int*>(anc + 2 * kWT);               // [bpt]: slot or -1
+    double2* Yt = reinterpret_cast<double2*>(E_im + kWT * 32);    // [kCols][kWT]
+    double2* Cacc = Yt + kCols * kWT;                            // [kWT][S][2]
+    double* anc = reinterpret_cast<double*>(Cacc + kWT * A.S * 2); // [2][kWT]
+    int* binfo = reinterpret_cast<int*>(anc + 2 * kWT);           // [32]: slot or -1
 
     const int tid = threadIdx.x;
     const int ty = tid / 16, tx = tid % 16;
     const int w0 = blockIdx.x * kWT;
     const int frame = blockIdx.y / A.tiles_per_frame;
     const int tile = blockIdx.y % A.tiles_per_frame;
-    const int NQ = 2 + 2 * A.S * A.M;
-    const int SM = A.S * A.M;
     const int cols_per_b = 2 * A.S;
     const D4* B = A.bub + (size_t)frame * A.n_tot;
-    const Real* evq = static_cast<const Real*>(A.ev_q);
+    const Real* beta = static_cast<const Real*>(A.beta);
 
-    if (tid < A.bpt) {
+    if (tid < 32) {
         const int slot = tile * A.bpt + tid;
-        binfo[tid] = slot < A.n_sel ? slot : -1;
+        binfo[tid] = (tid < A.bpt && slot < A.n_sel) ? slot : -1;
     }
     for (int q = tid; q < kWT * A.S * 2; q += kThreads) Cacc[q] = make_double2(0.0, 0.0);
     __syncthreads();
@@ -308,36 +372,32 @@ __global__ void __launch_bounds__(kThreads, 1) k_spec_factored(FactArgs A) {
         if (binfo[b] >= 0) kstart = min(kstart, A.kfirst[binfo[b]]);
     const int c_start = kstart / kKC;
     const int n_chunks = (A.n_t + kKC - 1) / kKC;
-    const double inv6pi = 1.0 / (6.0 * CUDART_PI);
+    const long col0 = (long)tile * A.bpt * cols_per_b;  // first column of this tile
 
     for (int i = 0; i < A.n_cos; ++i) {
         const double ci = A.cos_t[i];
         const double one_m_c = 1.0 - ci;
-        const double vi = (i == 0 || i == A.n_cos - 1) ? 0.5 : 1.0;
-        const double row_factor = (0.5 * (1.0 - ci * ci) * A.dphi) * (A.dcos * vi) * A.dt * inv6pi;
-        // within-chunk phase steps P_n(w) = e^{i w (1-c_i) n dt}, and epilogue phases
         for (int q = tid; q < kKC * kWT; q += kThreads) {
             const int n = q / kWT, wl = q % kWT;
             const int wi = w0 + wl;
-            double s = 0.0, c = 1.0;
-            if (wi < A.n_w) phase<Real>(A.w[wi] * one_m_c * (n * A.dt), s, c);
-            Pn_re[q] = c;
-            Pn_im[q] = s;
+            double sn = 0.0, cs = 1.0;
+            if (wi < A.n_w) phase<Real>(A.w[wi] * one_m_c * (n * A.dt), sn, cs);
+            Pn_re[q] = cs;
+            Pn_im[q] = sn;
         }
         for (int q = tid; q < kWT * A.bpt; q += kThreads) {
             const int wl = q / A.bpt, b = q % A.bpt;
             const int wi = w0 + wl;
-            double s = 0.0, c = 0.0;
+            double sn = 0.0, cs = 0.0;
             if (wi < A.n_w && binfo[b] >= 0) {
                 const D4 xa = B[A.sel[binfo[b]]];
-                phase<Real>(A.w[wi] * (xa.t * ci - xa.z), s, c);
+                phase<Real>(A.w[wi] * (xa.t * ci - xa.z), sn, cs);
             }
-            E_re[wl * 32 + b] = c;
-            E_im[wl * 32 + b] = s;
+            E_re[wl * 32 + b] = cs;
+            E_im[wl * 32 + b] = sn;
         }
-        for (int q = tid; q < 32 * kMaxQ; q += kThreads) Pst[q] = 0.0;  // layout [bubble][kMaxQ]
+        const Real* bi = beta + (((size_t)frame * A.n_cos + i) * A.cols_pad + col0) * A.t_pad;
         double acc[kTM][kTN];
-        Real cacc[kTM][kTN];
 #pragma unroll
         for (int r = 0; r < kTM; ++r)
 #pragma unroll
@@ -346,13 +406,18 @@ __global__ void __launch_bounds__(kThreads, 1) k_spec_factored(FactArgs A) {
 
         for (int ch = c_start; ch < n_chunks; ++ch) {
             const int k0 = ch * kKC;
-            // (1) anchors e^{i w (1-c_i) t_k0} and the M tile
             if (tid < kWT) {
                 const int wi = w0 + tid;
-                double s = 0.0, c = 0.0;
-                if (wi < A.n_w) phase<Real>(A.w[wi] * one_m_c * A.t_arr[k0], s, c);
-                anc[tid] = c;
-                anc[kWT + tid] = s;
+                double sn = 0.0, cs = 0.0;
+                if (wi < A.n_w) phase<Real>(A.w[wi] * one_m_c * A.t_arr[k0], sn, cs);
+                anc[tid] = cs;
+                anc[kWT + tid] = sn;
+            }
+            // beta tile [col][k0 .. k0+kKC): rows of t_pad contiguous values
+            for (int q = tid; q < kCols * kKC; q += kThreads) {
+                const int col = q / kKC, n = q % kKC;
+                const int k = k0 + n;
+                Bsm[col * BP + n] = k < A.t_pad ? __ldg(bi + (size_t)col * A.t_pad + k) : (Real)0;
             }
             __syncthreads();
             for (int q = tid; q < kKC * kWT; q += kThreads) {
@@ -363,67 +428,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_spec_factored(FactArgs A) {
                 Msm[n * kRows + 2 * wl] = valid ? (Real)(ar * pr - ai * pi) : (Real)0;
                 Msm[n * kRows + 2 * wl + 1] = valid ? (Real)(ar * pi + ai * pr) : (Real)0;
             }
-            // (2) the beta tile from running prefix sums and this bucket's events
-            for (int q = tid; q < kKC * kCols; q += kThreads) {
-                const int n = q / kCols, col = q % kCols;
-                const int k = k0 + n;
-                const int b = col / cols_per_b, sg = col % cols_per_b;
-                const int s = sg >> 1, g = sg & 1;
-                double beta = 0.0;
-                if (b < A.bpt && binfo[b] >= 0 && k < A.n_t) {
-                    const int slot = binfo[b];
-                    const double* Drow = A.D + ((size_t)slot * A.n_t + k) * (1 + SM);
-                    const double d3 = Drow[0];
-                    if (d3 != 0.0) {
-                        const long row = ((long)frame * A.n_sel + slot) * A.n_cos + i;
-                        const int* off = A.ev_off + (size_t)row * (A.NB + 1);
-                        const int e0 = off[ch], e1 = off[ch + 1];
-                        const int* ek = A.ev_k + (size_t)row * A.n_phi;
-                        const Real* eq = evq + (size_t)row * A.n_phi * NQ;
-                        // uncollided patches: those of later buckets plus this bucket's with k_e > k
-                        double unc = g ? A.ev_unc[(size_t)row * (A.NB + 1) + ch + 1].y
-                                       : A.ev_unc[(size_t)row * (A.NB + 1) + ch + 1].x;
-                        double pm[8];
-                        for (int m = 0; m < A.M; ++m) pm[m] = Pst[b * kMaxQ + 2 + 2 * (s * A.M + m) + g];
-                        for (int e = e0; e < e1; ++e) {
-                            if (ek[e] > k) {
-                                unc += (double)eq[(size_t)e * NQ + g];
-                            } else {
-                                for (int m = 0; m < A.M; ++m)
-                                    pm[m] += (double)eq[(size_t)e * NQ + 2 + 2 * (s * A.M + m) + g];
-                            }
-                        }
-                        double v = d3 * unc;
-                        for (int m = 0; m < A.M; ++m) v += A.coeffs[s * A.M + m] * Drow[1 + s * A.M + m] * pm[m];
-                        beta = row_factor * A.cutw[k] * ((k == 0 || k == A.n_t - 1) ? 0.5 : 1.0) * v;
-                    }
-                }
-                Bsm[n * kCols + col] = (Real)beta;
-            }
             __syncthreads();
-            // (3) fold this bucket into the running prefix sums
-            for (int q = tid; q < A.bpt * NQ; q += kThreads) {
-                const int b = q / NQ, qi = q % NQ;
-                if (binfo[b] < 0) continue;
-                const long row = ((long)frame * A.n_sel + binfo[b]) * A.n_cos + i;
-                const int* off = A.ev_off + (size_t)row * (A.NB + 1);
-                const Real* eq = evq + (size_t)row * A.n_phi * NQ;
-                double p = Pst[b * kMaxQ + qi];
-                for (int e = off[ch]; e < off[ch + 1]; ++e) p += (double)eq[(size_t)e * NQ + qi];
-                Pst[b * kMaxQ + qi] = p;
-            }
-            // (4) register-tiled GEMM over the chunk
+            Real cacc[kTM][kTN];
 #pragma unroll
             for (int r = 0; r < kTM; ++r)
 #pragma unroll
                 for (int u = 0; u < kTN; ++u) cacc[r][u] = (Real)0;
-#pragma unroll 4
+#pragma unroll
             for (int n = 0; n < kKC; ++n) {
                 Real a[kTM], bb[kTN];
 #pragma unroll
                 for (int r = 0; r < kTM; ++r) a[r] = Msm[n * kRows + ty * kTM + r];
 #pragma unroll
-                for (int u = 0; u < kTN; ++u) bb[u] = Bsm[n * kCols + tx * kTN + u];
+                for (int u = 0; u < kTN; ++u) bb[u] = Bsm[(tx * kTN + u) * BP + n];
 #pragma unroll
                 for (int r = 0; r < kTM; ++r)
 #pragma unroll
@@ -465,7 +482,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_spec_factored(FactArgs A) {
         }
         __syncthreads();
     }
-    // partial (frame, tile, g, s, w)
     for (int q = tid; q < kWT * A.S * 2; q += kThreads) {
         const int wl = q / (A.S * 2), sg = q % (A.S * 2);
         const int s = sg >> 1, g = sg & 1;
@@ -492,17 +508,35 @@ __global__ void k_reduce_tiles(const double2* __restrict__ partial, int tiles, s
 }
 
 // ---------------------------------------------------------------------------
-static size_t fact_smem_bytes(int real_size, int S) {
-    size_t b = (size_t)kKC * kRows * real_size + (size_t)kKC * kCols * real_size;
+template <class Real>
+static size_t gemm_smem_bytes(int S) {
+    constexpr int BP = kKC + (sizeof(Real) == 4 ? 4 : 2);
+    size_t b = (size_t)kKC * kRows * sizeof(Real) + (size_t)kCols * BP * sizeof(Real);
     b = (b + 15) & ~(size_t)15;
     b += 2 * (size_t)kKC * kWT * sizeof(double);
     b += 2 * (size_t)kWT * 32 * sizeof(double);
     b += (size_t)kCols * kWT * sizeof(double2);
     b += (size_t)kWT * S * 2 * sizeof(double2);
-    b += 32 * kMaxQ * sizeof(double);
     b += 2 * kWT * sizeof(double);
     b += 32 * sizeof(int);
     return b;
+}
+
+struct FactGeom {
+    int bpt, tiles_per_frame, t_pad, nblk;
+    long cols_pad;
+};
+
+static FactGeom fact_geom(const SpectrumJob& job, size_t real_size) {
+    FactGeom g;
+    const int S = (int)job.n_sets;
+    g.bpt = std::min(32, kCols / (2 * S));
+    g.tiles_per_frame = (int)((job.n_sel + g.bpt - 1) / g.bpt);
+    g.cols_pad = (long)g.tiles_per_frame * g.bpt * 2 * S;
+    const int align = real_size == 4 ? 4 : 2;
+    g.t_pad = (int)((job.n_t + align - 1) / align * align);
+    g.nblk = (int)((job.n_t + 31) / 32);
+    return g;
 }
 
 template <class Real>
@@ -513,21 +547,19 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     const int S = (int)job.n_sets, M = (int)job.n_terms, SM = S * M;
     const int n_t = (int)job.n_t, n_cos = (int)job.n_cos, n_phi = (int)job.n_phi, n_w = (int)job.n_w;
     const int n_sel = (int)job.n_sel;
-    if (M > 8 || 2 + 2 * SM > kMaxQ || 2 * S > kCols)
+    if (SM > 8 || 2 * S > kCols)
         throw Error{"the factored kernels support at most 8 (set, term) pairs; use the fp64_direct kernel"};
     if (job.has_damping) {
-        double max_tau_over = job.t_arr[job.n_t - 1] / job.damping;
-        if (!(std::fabs(max_tau_over) < 600.0))
+        const double span = job.t_arr[job.n_t - 1] - job.t_arr[0] + 4.0;
+        if (!(std::fabs(span / job.damping) < 600.0))
             throw Error{"damping width too small for the factored kernels (exp overflow); use fp64_direct"};
     }
-    const int NB = (n_t + kKC - 1) / kKC;
-    const int NQ = 2 + 2 * SM;
-    const long rows = (long)kn * n_sel * n_cos;
+    const FactGeom G = fact_geom(job, sizeof(Real));
     uint64_t launches = 0;
     // per-bubble time tables (frame independent)
     dev->fact_D.ensure((size_t)n_sel * n_t * (1 + SM) * sizeof(double));
     dev->fact_kfirst.ensure((size_t)n_sel * sizeof(int));
-    // bubble times are frame independent: frame 0 of bub_frames serves
+    if (n_sel > 65535) throw Error{"too many radiating bubbles for the time-table grid"};
     {
         dim3 g((unsigned)((n_t + 127) / 128), (unsigned)n_sel);
         k_time_tables<<<g, 128, 0, dev->stream>>>(bub_frames, sel, n_sel, t_arr, n_t, powers, SM,
@@ -536,21 +568,52 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         CUDA_OK(cudaGetLastError());
         ++launches;
     }
-    // events
-    dev->ev_off.ensure((size_t)rows * (NB + 1) * sizeof(int));
-    dev->ev_k.ensure((size_t)rows * n_phi * sizeof(int));
-    dev->ev_q.ensure((size_t)rows * n_phi * NQ * sizeof(Real));
-    dev->ev_unc.ensure((size_t)rows * (NB + 1) * sizeof(double2));
+    // beta
+    const size_t beta_elems = (size_t)kn * n_cos * G.cols_pad * G.t_pad;
+    dev->ev_q.ensure(beta_elems * sizeof(Real));
+    if ((long)n_sel * 2 * S != G.cols_pad) {
+        // padding columns of the last tile are read by the GEMM: keep them zero
+        CUDA_OK(cudaMemsetAsync(dev->ev_q.p, 0, beta_elems * sizeof(Real), dev->stream));
+    }
     {
-        const int warps = 8;
-        size_t smem = (size_t)warps * (2 * (NB + 1) + 4 * NB + 2) * sizeof(int);
-        if (smem > 200 * 1024) throw Error{"n_t too large for the event kernel"};
-        CUDA_OK(cudaFuncSetAttribute(k_events<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        unsigned blocks = (unsigned)((rows + warps - 1) / warps);
-        k_events<Real><<<blocks, warps * 32, smem, dev->stream>>>(
-            tau, bub_frames, sel, n_sel, n_cos, n_phi, t_arr, n_t, cos2, sin2, powers, SM, job.has_damping ? 1 : 0,
-            job.damping, rows, NB, (int*)dev->ev_off.p, (int*)dev->ev_k.p, (Real*)dev->ev_q.p,
-            (double2*)dev->ev_unc.p);
+        BetaArgs B;
+        B.tau = tau;
+        B.bub = bub_frames;
+        B.sel = sel;
+        B.n_sel = n_sel;
+        B.n_cos = n_cos;
+        B.n_phi = n_phi;
+        B.n_t = n_t;
+        B.S = S;
+        B.M = M;
+        B.t_arr = t_arr;
+        B.cutw = cutw;
+        B.cos_t = cos_t;
+        B.cos2 = cos2;
+        B.sin2 = sin2;
+        B.powers = powers;
+        B.coeffs = coeffs;
+        B.D = (const double*)dev->fact_D.p;
+        B.has_damp = job.has_damping ? 1 : 0;
+        B.damp = job.damping;
+        B.dphi = 2.0 * M_PI / (double)n_phi;
+        B.dcos = 2.0 / (double)(n_cos - 1);
+        B.dt = job.dt;
+        B.n_rows = (long)kn * n_sel * n_cos;
+        B.nblk = G.nblk;
+        B.cols_pad = G.cols_pad;
+        B.t_pad = G.t_pad;
+        const int NQ = 2 + 2 * SM;
+        size_t pw = (size_t)n_phi * NQ * sizeof(double) + 4 * (size_t)G.nblk * sizeof(double) +
+                    ((size_t)n_phi + 2 * G.nblk + 1) * sizeof(int);
+        pw = (pw + 15) & ~(size_t)15;
+        B.per_warp_bytes = (int)pw;
+        int warps = (int)std::min<size_t>(8, (200 * 1024) / pw);
+        if (warps < 1) throw Error{"n_phi too large for the beta kernel"};
+        const size_t smem = (size_t)warps * pw;
+        CUDA_OK(cudaFuncSetAttribute(k_beta<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const unsigned blocks = (unsigned)((B.n_rows + warps - 1) / warps);
+        k_beta<Real><<<blocks, warps * 32, smem, dev->stream>>>(B, (Real*)dev->ev_q.p);
         CUDA_OK(cudaGetLastError());
         ++launches;
     }
@@ -561,41 +624,32 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     A.sel = sel;
     A.n_sel = n_sel;
     A.n_cos = n_cos;
-    A.n_phi = n_phi;
     A.n_t = n_t;
     A.n_w = n_w;
     A.S = S;
-    A.M = M;
-    A.cos_t = cos_t;
     A.t_arr = t_arr;
-    A.cutw = cutw;
     A.w = w;
-    A.coeffs = coeffs;
-    A.D = (const double*)dev->fact_D.p;
+    A.cos_t = cos_t;
     A.kfirst = (const int*)dev->fact_kfirst.p;
-    A.ev_off = (const int*)dev->ev_off.p;
-    A.ev_k = (const int*)dev->ev_k.p;
-    A.ev_q = dev->ev_q.p;
-    A.ev_unc = (const double2*)dev->ev_unc.p;
-    A.NB = NB;
+    A.beta = dev->ev_q.p;
+    A.cols_pad = G.cols_pad;
+    A.t_pad = G.t_pad;
     A.dt = job.dt;
-    A.dphi = 2.0 * M_PI / (double)n_phi;
-    A.dcos = 2.0 / (double)(n_cos - 1);
-    A.bpt = std::min(32, kCols / (2 * S));
-    A.tiles_per_frame = (n_sel + A.bpt - 1) / A.bpt;
+    A.bpt = G.bpt;
+    A.tiles_per_frame = G.tiles_per_frame;
     const size_t per = (size_t)2 * S * n_w;
-    dev->fact_partial.ensure((size_t)kn * A.tiles_per_frame * per * sizeof(double2));
+    dev->fact_partial.ensure((size_t)kn * G.tiles_per_frame * per * sizeof(double2));
     A.partial = (double2*)dev->fact_partial.p;
-    const size_t smem = fact_smem_bytes((int)sizeof(Real), S);
-    CUDA_OK(cudaFuncSetAttribute(k_spec_factored<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const size_t gy = (size_t)kn * A.tiles_per_frame;
+    const size_t smem = gemm_smem_bytes<Real>(S);
+    CUDA_OK(cudaFuncSetAttribute(k_gemm<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    const size_t gy = (size_t)kn * G.tiles_per_frame;
     if (gy > 65535) throw Error{"too many column tiles in one k-hat chunk"};
     dim3 grid((unsigned)((n_w + kWT - 1) / kWT), (unsigned)gy);
-    k_spec_factored<Real><<<grid, kThreads, smem, dev->stream>>>(A);
+    k_gemm<Real><<<grid, kThreads, smem, dev->stream>>>(A);
     CUDA_OK(cudaGetLastError());
     ++launches;
     dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
-    k_reduce_tiles<<<gr, 256, 0, dev->stream>>>(A.partial, A.tiles_per_frame, per, (int)kn, out);
+    k_reduce_tiles<<<gr, 256, 0, dev->stream>>>(A.partial, G.tiles_per_frame, per, (int)kn, out);
     CUDA_OK(cudaGetLastError());
     ++launches;
     return launches;
@@ -613,14 +667,10 @@ uint64_t launch_factored(Device* dev, const SpectrumJob& job, const D4* bub_fram
 }
 
 size_t factored_bytes_per_frame(const SpectrumJob& job) {
-    const size_t NB = (job.n_t + kKC - 1) / kKC;
-    const size_t NQ = 2 + 2 * job.n_sets * job.n_terms;
     const size_t real = job.kernel == BGWX_KERNEL_MIXED ? sizeof(float) : sizeof(double);
-    const size_t rows = job.n_sel * job.n_cos;
-    const size_t bpt = std::min<size_t>(32, kCols / (2 * job.n_sets));
-    const size_t tiles = (job.n_sel + bpt - 1) / bpt;
-    return rows * ((NB + 1) * (sizeof(int) + sizeof(double2)) + job.n_phi * (sizeof(int) + NQ * real)) +
-           tiles * 2 * job.n_sets * job.n_w * sizeof(double2);
+    const FactGeom G = fact_geom(job, real);
+    return (size_t)job.n_cos * G.cols_pad * G.t_pad * real +
+           (size_t)G.tiles_per_frame * 2 * job.n_sets * job.n_w * sizeof(double2);
 }
 
 }  // namespace bgw
