@@ -46,7 +46,8 @@
 
 namespace bgw {
 
-constexpr int kKC = 16;          // time steps per GEMM k-tile
+constexpr int kKC = 32;          // time steps per GEMM k-tile
+constexpr int kFold = 8;         // mixed: FP32 partial sums are folded into FP64 every kFold steps
 constexpr int kWT = 64;          // frequencies per CTA
 constexpr int kRows = 2 * kWT;   // GEMM rows: (Re, Im) of each frequency
 constexpr int kCols = 64;        // GEMM columns per CTA
@@ -402,6 +403,19 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
         for (int r = 0; r < kTM; ++r)
 #pragma unroll
             for (int u = 0; u < kTN; ++u) acc[r][u] = 0.0;
+        // beta tile of the first chunk, prefetched into registers
+        constexpr int kPer = kCols * kKC / kThreads;
+        Real pre[kPer];
+        auto fetch = [&](int k0) {
+#pragma unroll
+            for (int v = 0; v < kPer; ++v) {
+                const int q = tid + v * kThreads;
+                const int col = q / kKC, n = q % kKC;
+                const int k = k0 + n;
+                pre[v] = k < A.t_pad ? __ldg(bi + (size_t)col * A.t_pad + k) : (Real)0;
+            }
+        };
+        if (c_start < n_chunks) fetch(c_start * kKC);
         __syncthreads();
 
         for (int ch = c_start; ch < n_chunks; ++ch) {
@@ -413,11 +427,10 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
                 anc[tid] = cs;
                 anc[kWT + tid] = sn;
             }
-            // beta tile [col][k0 .. k0+kKC): rows of t_pad contiguous values
-            for (int q = tid; q < kCols * kKC; q += kThreads) {
-                const int col = q / kKC, n = q % kKC;
-                const int k = k0 + n;
-                Bsm[col * BP + n] = k < A.t_pad ? __ldg(bi + (size_t)col * A.t_pad + k) : (Real)0;
+#pragma unroll
+            for (int v = 0; v < kPer; ++v) {
+                const int q = tid + v * kThreads;
+                Bsm[(q / kKC) * BP + (q % kKC)] = pre[v];
             }
             __syncthreads();
             for (int q = tid; q < kKC * kWT; q += kThreads) {
@@ -429,27 +442,46 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
                 Msm[n * kRows + 2 * wl + 1] = valid ? (Real)(ar * pi + ai * pr) : (Real)0;
             }
             __syncthreads();
-            Real cacc[kTM][kTN];
+            if (ch + 1 < n_chunks) fetch(k0 + kKC);  // overlaps the GEMM below
+            if constexpr (sizeof(Real) == 8) {
+#pragma unroll 8
+                for (int n = 0; n < kKC; ++n) {
+                    double a[kTM], bb[kTN];
 #pragma unroll
-            for (int r = 0; r < kTM; ++r)
+                    for (int r = 0; r < kTM; ++r) a[r] = Msm[n * kRows + ty * kTM + r];
 #pragma unroll
-                for (int u = 0; u < kTN; ++u) cacc[r][u] = (Real)0;
+                    for (int u = 0; u < kTN; ++u) bb[u] = Bsm[(tx * kTN + u) * BP + n];
 #pragma unroll
-            for (int n = 0; n < kKC; ++n) {
-                Real a[kTM], bb[kTN];
+                    for (int r = 0; r < kTM; ++r)
 #pragma unroll
-                for (int r = 0; r < kTM; ++r) a[r] = Msm[n * kRows + ty * kTM + r];
+                        for (int u = 0; u < kTN; ++u) acc[r][u] = fma(a[r], bb[u], acc[r][u]);
+                }
+            } else {
+#pragma unroll 1
+                for (int n0 = 0; n0 < kKC; n0 += kFold) {
+                    float cacc[kTM][kTN];
 #pragma unroll
-                for (int u = 0; u < kTN; ++u) bb[u] = Bsm[(tx * kTN + u) * BP + n];
+                    for (int r = 0; r < kTM; ++r)
 #pragma unroll
-                for (int r = 0; r < kTM; ++r)
+                        for (int u = 0; u < kTN; ++u) cacc[r][u] = 0.0f;
 #pragma unroll
-                    for (int u = 0; u < kTN; ++u) cacc[r][u] = fma(a[r], bb[u], cacc[r][u]);
+                    for (int n = n0; n < n0 + kFold; ++n) {
+                        float a[kTM], bb[kTN];
+#pragma unroll
+                        for (int r = 0; r < kTM; ++r) a[r] = (float)Msm[n * kRows + ty * kTM + r];
+#pragma unroll
+                        for (int u = 0; u < kTN; ++u) bb[u] = (float)Bsm[(tx * kTN + u) * BP + n];
+#pragma unroll
+                        for (int r = 0; r < kTM; ++r)
+#pragma unroll
+                            for (int u = 0; u < kTN; ++u) cacc[r][u] = fmaf(a[r], bb[u], cacc[r][u]);
+                    }
+#pragma unroll
+                    for (int r = 0; r < kTM; ++r)
+#pragma unroll
+                        for (int u = 0; u < kTN; ++u) acc[r][u] += (double)cacc[r][u];
+                }
             }
-#pragma unroll
-            for (int r = 0; r < kTM; ++r)
-#pragma unroll
-                for (int u = 0; u < kTN; ++u) acc[r][u] += (double)cacc[r][u];
             __syncthreads();
         }
         // epilogue: C_{s,g}(w) += sum_b E(w, b) Y(w, (b, s, g))
