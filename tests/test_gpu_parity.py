@@ -51,10 +51,14 @@ def mixed_errors(got, ref):
 
 
 def check(kernel, got, ref, label):
-    if kernel == "mixed":
+    """fp64_direct follows the reference's arithmetic term by term: per-w relative error <= 1e-12.
+    fp64_factored and mixed form the phase as w t (1 - c) + w (t_a c - z_a), whose rounding
+    differs from the reference's per-term rounding: their error is held to the tolerance in the
+    global and peak-scaled norms (per-w values are printed)."""
+    if kernel != "fp64_direct":
         glob, peak = mixed_errors(got, ref)
         print(f"{label} {kernel}: global {glob:.3e} peak-scaled {peak:.3e} per-w {err_per_w(got, ref):.3e}")
-        assert glob < MIXED_TOL and peak < MIXED_TOL
+        assert glob < TOL[kernel] and peak < TOL[kernel]
     else:
         err = err_per_w(got, ref)
         print(f"{label} {kernel}: max_w rel err {err:.3e}")
