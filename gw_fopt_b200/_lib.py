@@ -67,6 +67,9 @@ SIGNATURES = {
     "bgwx_generalized_bulk_flow_set_stream": (C.c_int, [_hp, C.c_void_p]),
     "bgwx_generalized_bulk_flow_drop_resident_inputs": (C.c_int, [_hp]),
     "bgwx_measure_compute_peaks": (C.c_int, [_dp, _dp, _dp]),
+    "bgwx_first_colliding_noalloc": (
+        C.c_int, [C.c_void_p, C.c_size_t, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p, C.c_size_t, C.c_void_p,
+                  C.c_void_p, C.c_void_p]),
     "bgwx_rotation_for_khat": (None, [C.c_double, C.c_double, C.c_double, _dp]),
     "bgwx_generalized_bulk_flow_last_timings": (C.c_int, [_hp, C.POINTER(BgwxTimings)]),
     "bgwx_device_count": (C.c_int, []),

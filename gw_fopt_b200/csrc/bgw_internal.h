@@ -91,6 +91,10 @@ void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_
 
 int device_count();
 
+// Thread-local message of bgw_last_error_message (capi.cpp).
+void set_last_error(std::string message);
+void clear_last_error();
+
 // Lattice geometry (lattice.cpp).
 void lattice_contains(BgwxLatticeKind kind, const double* params, const double* pts, size_t n, uint8_t* out);
 std::vector<double> lattice_exterior(BgwxLatticeKind kind, const double* params, BgwxBoundaryCondition bc,

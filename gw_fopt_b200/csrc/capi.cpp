@@ -41,14 +41,20 @@ struct bgw_generalized_bulk_flow {
 };
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
 
+namespace bgw {
 void set_last_error(std::string m) {
     for (auto& ch : m)
         if (ch == '\0') ch = ' ';
     g_last_error = std::move(m);
 }
+void clear_last_error() { g_last_error.clear(); }
+}  // namespace bgw
+
+namespace {
+using bgw::set_last_error;
 
 // rust/c-bubble-gw/src/lib.rs:119-134: Ok -> clear; Err -> CalculationError.
 template <class F>

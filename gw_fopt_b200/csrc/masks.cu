@@ -34,6 +34,7 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
+#include <cstdint>
 
 #include "bgw_internal.h"
 #include "device_common.cuh"
@@ -134,7 +135,8 @@ __device__ __forceinline__ void collider_bounds(const D4& d, double& key, double
 }
 
 __global__ void __launch_bounds__(kNbThreads)
-    k_neighbors(const D4* __restrict__ bub, size_t n_tot, const uint32_t* __restrict__ sel, NbList* __restrict__ out) {
+    k_neighbors(const D4* __restrict__ bub, size_t n_int, size_t n_tot, const uint32_t* __restrict__ sel,
+                NbList* __restrict__ out) {
     __shared__ unsigned hist[2048];
     __shared__ unsigned s_prefix, s_mask, s_need, s_count, s_nout;
     __shared__ double s_key[kList];
@@ -142,8 +144,12 @@ __global__ void __launch_bounds__(kNbThreads)
     __shared__ double s_r1[kNbThreads], s_r2[kNbThreads];
     const int slot = blockIdx.x;
     const uint32_t a = sel[slot];
-    const D4 xa = bub[a];
     NbList* L = out + slot;
+    if (a >= n_int) {  // not an interior bubble: marked, never dereferenced
+        if (threadIdx.x == 0) L->count = -1;
+        return;
+    }
+    const D4 xa = bub[a];
     const size_t n_c = n_tot - 1;  // colliders other than a
     const bool complete = n_c <= (size_t)kList;
     auto fbits = [&](size_t c) -> unsigned {
@@ -286,6 +292,14 @@ __global__ void __launch_bounds__(kMaskListThreads)
     const uint32_t a = sel[slot];
     const NbList* L = lists + slot;
     const int n = L->count;
+    if (a >= n_int || n < 0) {  // invalid radiating bubble: sentinel outputs
+        if (d < nd) {
+            const size_t o = ((size_t)k * n_sel + slot) * nd + d;
+            tau_out[o] = CUDART_NAN;
+            if (code_out) code_out[o] = INT32_MIN;
+        }
+        return;
+    }
     const int no = L->n_outliers;
     for (int q = threadIdx.x; q < n; q += kMaskListThreads) {
         const int c = L->idx[q];
@@ -418,6 +432,25 @@ __global__ void __launch_bounds__(kMaskListThreads)
 }
 
 // ------------------------------------------------------------------ host
+void launch_masks_with_lists(cudaStream_t stream, const D4* bub, size_t n_int, size_t n_tot, const uint32_t* sel,
+                             size_t n_sel, const D4* dirs, size_t nd, NbList* lists, double* tau, int32_t* codes,
+                             unsigned long long* counters) {
+    if (n_tot < 2) {
+        CUDA_OK(cudaMemsetAsync(tau, 0, n_sel * nd * sizeof(double), stream));
+        if (codes) CUDA_OK(cudaMemsetAsync(codes, 0xff, n_sel * nd * sizeof(int32_t), stream));
+        return;
+    }
+    if (n_sel > 0x7fffffffULL) throw Error{"too many radiating bubbles"};
+    k_neighbors<<<(unsigned)n_sel, kNbThreads, 0, stream>>>(bub, n_int, n_tot, sel, lists);
+    CUDA_OK(cudaGetLastError());
+    const unsigned n_dblocks = (unsigned)((nd + kMaskListThreads - 1) / kMaskListThreads);
+    const size_t gx = (size_t)n_dblocks * n_sel;
+    if (gx > 0x7fffffffULL) throw Error{"too many (bubble, patch) pairs for one launch"};
+    k_masks_list<<<dim3((unsigned)gx, 1), kMaskListThreads, 0, stream>>>(bub, n_int, n_tot, sel, n_sel, lists, dirs,
+                                                                        nd, n_dblocks, tau, codes, counters);
+    CUDA_OK(cudaGetLastError());
+}
+
 void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames, size_t n_int, size_t n_tot,
                           const uint32_t* sel, size_t n_sel, const D4* dirs, size_t nd, size_t kn, double* tau,
                           int32_t* codes, unsigned long long* counters, bool build_lists, uint64_t* launches) {
@@ -430,7 +463,8 @@ void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames
     dev->nblists.ensure(n_sel * sizeof(NbList));
     if (build_lists) {
         if (n_sel > 0x7fffffffULL) throw Error{"too many radiating bubbles"};
-        k_neighbors<<<(unsigned)n_sel, kNbThreads, 0, dev->stream>>>(bub_unrot, n_tot, sel, (NbList*)dev->nblists.p);
+        k_neighbors<<<(unsigned)n_sel, kNbThreads, 0, dev->stream>>>(bub_unrot, n_int, n_tot, sel,
+                                                                      (NbList*)dev->nblists.p);
         CUDA_OK(cudaGetLastError());
         if (launches) ++*launches;
     }

@@ -22,6 +22,12 @@ struct NbList {
     int n_outliers;      // -1: too many near-lightlike colliders, use the exhaustive scan
 };
 
+// Builds candidate lists into `lists` (n_sel entries) and runs the exact
+// search for one frame on `stream`; tau/codes: (n_sel, nd).  Allocates nothing.
+void launch_masks_with_lists(cudaStream_t stream, const D4* bub, size_t n_int, size_t n_tot, const uint32_t* sel,
+                             size_t n_sel, const D4* dirs, size_t nd, NbList* lists, double* tau, int32_t* codes,
+                             unsigned long long* counters);
+
 // Builds the lists (when build_lists) from the unrotated bubbles and runs the
 // list-based exact search for kn frames.  tau/codes: (kn, n_sel, nd).
 void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames, size_t n_int, size_t n_tot,

@@ -141,6 +141,31 @@ BgwStatus bgwx_generalized_bulk_flow_drop_resident_inputs(bgw_generalized_bulk_f
  * No counterpart in the reference. */
 BgwStatus bgwx_measure_compute_peaks(double *fp64_flops, double *fp32_flops, double *sfu_ops);
 
+/* First-collider codes and collision delays, as bgwx_generalized_bulk_flow_first_colliding
+ * returns them, for callers that cannot allocate device memory: frameworks that
+ * serve all device memory from their own pool and long-running services that
+ * must not allocate after start-up.  Everything is caller-owned device memory:
+ *   d_bubbles   (n_total, 4) rows (t, x, y, z), interior rows first;
+ *   d_selected  (n_selected) uint32 interior indices, n_selected <= 512 (an index
+ *               >= n_interior yields codes INT32_MIN and delays NaN for that row);
+ *   d_dirs      (n_dirs, 4) patch directions (1, s cos(phi), s sin(phi), c) with
+ *               c = -1 + i*(2/(n_cos-1)), s = |sqrt(1 - c*c)|, phi = j*(2 pi/(n_phi-1)),
+ *               row i*n_phi + j, sin/cos from the C library;
+ *   d_codes     (n_selected, n_dirs) int32 out: -1 None, i Interior(i), -(i+2) Exterior(i);
+ *   d_delta_tab (n_selected, n_dirs) f64 out.
+ * The work runs on `stream` (a cudaStream_t, NULL = legacy default stream) and
+ * is left in flight.  The library's only work array, the per-bubble candidate
+ * lists, is a fixed static device array of 512 entries (about 0.8 MB on every
+ * GPU that loads the library, until exit); more than 512 selected bubbles is
+ * rejected with an error.  The first call on each device looks up that array's
+ * device address, so make the first call before any stream capture.  All calls
+ * share the array: calls whose work overlaps on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller.
+ * No counterpart in the reference. */
+BgwStatus bgwx_first_colliding_noalloc(const double *d_bubbles, size_t n_interior, size_t n_total,
+                                       const uint32_t *d_selected, size_t n_selected, const double *d_dirs,
+                                       size_t n_dirs, int32_t *d_codes, double *d_delta_tab, void *stream);
+
 /* The rotation R(k) used above, row-major 3x3.  No counterpart in the reference. */
 void bgwx_rotation_for_khat(double kx, double ky, double kz, double *R);
 
