@@ -75,7 +75,7 @@ struct Device {
     std::vector<cudaEvent_t> chunk_ev;  // 3 per k-hat chunk
     DevBuf bub, bubrot, dirs, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, sel, rot;
     DevBuf tau, codes, partial, out, counters, nblists;
-    DevBuf fact_D, fact_kfirst, ev_off, ev_k, ev_q, ev_unc, fact_partial;  // factored-kernel work arrays
+    DevBuf fact_D, fact_kfirst, beta, fact_partial;  // factored-kernel work arrays
     ~Device();
 };
 

@@ -38,6 +38,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "bgw_internal.h"
@@ -47,12 +48,11 @@
 namespace bgw {
 
 constexpr int kKC = 32;          // time steps per GEMM k-tile
-constexpr int kFold = 8;         // mixed: FP32 partial sums are folded into FP64 every kFold steps
+constexpr int kFold = 16;        // mixed: FP32 partial sums are folded into FP64 every kFold steps
 constexpr int kWT = 64;          // frequencies per CTA
 constexpr int kRows = 2 * kWT;   // GEMM rows: (Re, Im) of each frequency
-constexpr int kCols = 64;        // GEMM columns per CTA
 constexpr int kThreads = 256;
-constexpr int kTM = 8, kTN = 4;  // register tile per thread
+constexpr int kTM = 8;           // register tile rows per thread (columns: TN = 8 FP32, 4 FP64)
 
 // ---------------------------------------------------------------------------
 __global__ void k_time_tables(const D4* __restrict__ bub, const uint32_t* __restrict__ sel, int n_sel,
@@ -101,7 +101,9 @@ struct BetaArgs {
     double dphi, dcos, dt;
     long n_rows;           // kn * n_sel * n_cos
     int nblk;              // ceil(n_t / 32)
-    long cols_pad;         // columns per (frame, i), padded
+    long cols_pad;         // columns per (frame, i): tiles_per_frame * tile_cols
+    int tile_cols;         // columns of one GEMM tile
+    int bpt;               // bubbles per tile
     int t_pad;             // row length of beta
     int per_warp_bytes;
 };
@@ -230,7 +232,8 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
     const double ci = A.cos_t[i];
     const double vi = (i == 0 || i == A.n_cos - 1) ? 0.5 : 1.0;
     const double rf = (0.5 * (1.0 - ci * ci) * A.dphi) * (A.dcos * vi) * A.dt * (1.0 / (6.0 * CUDART_PI));
-    Real* brow = beta + ((size_t)frame * A.n_cos + i) * A.cols_pad * A.t_pad + (size_t)slot * 2 * A.S * A.t_pad;
+    const long col = (long)(slot / A.bpt) * A.tile_cols + (long)(slot % A.bpt) * 2 * A.S;
+    Real* brow = beta + (((size_t)frame * A.n_cos + i) * A.cols_pad + col) * A.t_pad;
     double pstart[16];
 #pragma unroll
     for (int q = 0; q < 16; ++q) pstart[q] = 0.0;
@@ -338,42 +341,54 @@ __device__ __forceinline__ void phase<float>(double arg, double& s, double& c) {
     c = cf;
 }
 
-template <class Real>
+// One CTA per (64-frequency tile, column tile), looping over the rows i.
+// Thread (ty, tx) of 16 x 16 owns rows ty*8 .. ty*8+7 (frequencies ty*4 .. +3,
+// Re/Im interleaved) and columns tx*TN .. tx*TN+TN-1.
+template <class Real, int TN>
 __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
-    constexpr int BP = kKC + (sizeof(Real) == 4 ? 4 : 2);        // padded k-stride of the beta tile
-    Real* Msm = reinterpret_cast<Real*>(smem);                   // [kKC][kRows]
-    Real* Bsm = Msm + kKC * kRows;                               // [kCols][BP]
-    double* Pn_re = reinterpret_cast<double*>(Bsm + kCols * BP);   // [kKC][kWT]
+    constexpr int COLS = 16 * TN;                                  // 128 (FP32) or 64 (FP64)
+    constexpr int BS = COLS + 16 / (int)sizeof(Real);              // padded row of the beta tile
+    constexpr int VEC = 16 / (int)sizeof(Real);                    // elements per 16-byte load
+    constexpr int NPRE = COLS * kKC / VEC / kThreads;              // 16-byte loads per thread per tile
+    Real* Msm = reinterpret_cast<Real*>(smem);                     // [kKC][kRows]
+    Real* Bsm = Msm + kKC * kRows;                                 // [kKC][BS]
+    double* Pn_re = reinterpret_cast<double*>(Bsm + kKC * BS);      // [kKC][kWT]
     double* Pn_im = Pn_re + kKC * kWT;
-    double* E_re = Pn_im + kKC * kWT;                            // [kWT][32]
-    double* E_im = E_re + kWT * 32;
-    double2* Yt = reinterpret_cast<double2*>(E_im + kWT * 32);    // [kCols][kWT]
-    double2* Cacc = Yt + kCols * kWT;                            // [kWT][S][2]
-    double* anc = reinterpret_cast<double*>(Cacc + kWT * A.S * 2); // [2][kWT]
-    int* binfo = reinterpret_cast<int*>(anc + 2 * kWT);           // [32]: slot or -1
+    double* anc = Pn_im + kKC * kWT;                               // [2][kWT]
+    double2* red = reinterpret_cast<double2*>(anc + 2 * kWT);       // [kThreads][4][2S]
+    double2* Cacc = red + kThreads * 4 * 2 * A.S;                  // [kWT][2S]
+    int* binfo = reinterpret_cast<int*>(Cacc + kWT * 2 * A.S);      // [bpt]: slot or -1
+    double* bt = reinterpret_cast<double*>(binfo + 64);            // [bpt] t_a
+    double* bz = bt + 64;                                          // [bpt] z_a
 
     const int tid = threadIdx.x;
     const int ty = tid / 16, tx = tid % 16;
     const int w0 = blockIdx.x * kWT;
     const int frame = blockIdx.y / A.tiles_per_frame;
     const int tile = blockIdx.y % A.tiles_per_frame;
-    const int cols_per_b = 2 * A.S;
+    const int cpb = 2 * A.S;  // columns per bubble
     const D4* B = A.bub + (size_t)frame * A.n_tot;
     const Real* beta = static_cast<const Real*>(A.beta);
 
-    if (tid < 32) {
+    if (tid < 64) {
         const int slot = tile * A.bpt + tid;
-        binfo[tid] = (tid < A.bpt && slot < A.n_sel) ? slot : -1;
+        const bool ok = tid < A.bpt && slot < A.n_sel;
+        binfo[tid] = ok ? slot : -1;
+        if (ok) {
+            const D4 xa = B[A.sel[slot]];
+            bt[tid] = xa.t;
+            bz[tid] = xa.z;
+        }
     }
-    for (int q = tid; q < kWT * A.S * 2; q += kThreads) Cacc[q] = make_double2(0.0, 0.0);
+    for (int q = tid; q < kWT * cpb; q += kThreads) Cacc[q] = make_double2(0.0, 0.0);
     __syncthreads();
     int kstart = A.n_t;
     for (int b = 0; b < A.bpt; ++b)
         if (binfo[b] >= 0) kstart = min(kstart, A.kfirst[binfo[b]]);
     const int c_start = kstart / kKC;
     const int n_chunks = (A.n_t + kKC - 1) / kKC;
-    const long col0 = (long)tile * A.bpt * cols_per_b;  // first column of this tile
+    const long col0 = (long)tile * COLS;
 
     for (int i = 0; i < A.n_cos; ++i) {
         const double ci = A.cos_t[i];
@@ -386,35 +401,25 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
             Pn_re[q] = cs;
             Pn_im[q] = sn;
         }
-        for (int q = tid; q < kWT * A.bpt; q += kThreads) {
-            const int wl = q / A.bpt, b = q % A.bpt;
-            const int wi = w0 + wl;
-            double sn = 0.0, cs = 0.0;
-            if (wi < A.n_w && binfo[b] >= 0) {
-                const D4 xa = B[A.sel[binfo[b]]];
-                phase<Real>(A.w[wi] * (xa.t * ci - xa.z), sn, cs);
-            }
-            E_re[wl * 32 + b] = cs;
-            E_im[wl * 32 + b] = sn;
-        }
         const Real* bi = beta + (((size_t)frame * A.n_cos + i) * A.cols_pad + col0) * A.t_pad;
-        double acc[kTM][kTN];
+        // 16-byte loads of the beta tile: column q / (kKC/VEC), steps VEC*(q % (kKC/VEC)) ...
+        using Vec = typename std::conditional<sizeof(Real) == 4, float4, double2>::type;
+        Vec pre[NPRE];
+        auto fetch = [&](int k0) {
+#pragma unroll
+            for (int v = 0; v < NPRE; ++v) {
+                const int q = tid + v * kThreads;
+                const int col = q / (kKC / VEC), n = (q % (kKC / VEC)) * VEC;
+                const int k = k0 + n;  // t_pad is a multiple of VEC: a load is all in or all out
+                if (k < A.t_pad) pre[v] = __ldg(reinterpret_cast<const Vec*>(bi + (size_t)col * A.t_pad + k));
+                else pre[v] = Vec{};
+            }
+        };
+        double acc[kTM][TN];
 #pragma unroll
         for (int r = 0; r < kTM; ++r)
 #pragma unroll
-            for (int u = 0; u < kTN; ++u) acc[r][u] = 0.0;
-        // beta tile of the first chunk, prefetched into registers
-        constexpr int kPer = kCols * kKC / kThreads;
-        Real pre[kPer];
-        auto fetch = [&](int k0) {
-#pragma unroll
-            for (int v = 0; v < kPer; ++v) {
-                const int q = tid + v * kThreads;
-                const int col = q / kKC, n = q % kKC;
-                const int k = k0 + n;
-                pre[v] = k < A.t_pad ? __ldg(bi + (size_t)col * A.t_pad + k) : (Real)0;
-            }
-        };
+            for (int u = 0; u < TN; ++u) acc[r][u] = 0.0;
         if (c_start < n_chunks) fetch(c_start * kKC);
         __syncthreads();
 
@@ -428,9 +433,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
                 anc[kWT + tid] = sn;
             }
 #pragma unroll
-            for (int v = 0; v < kPer; ++v) {
+            for (int v = 0; v < NPRE; ++v) {
                 const int q = tid + v * kThreads;
-                Bsm[(q / kKC) * BP + (q % kKC)] = pre[v];
+                const int col = q / (kKC / VEC), n = (q % (kKC / VEC)) * VEC;
+                const Real* pv = reinterpret_cast<const Real*>(&pre[v]);
+#pragma unroll
+                for (int e = 0; e < VEC; ++e) Bsm[(n + e) * BS + col] = pv[e];
             }
             __syncthreads();
             for (int q = tid; q < kKC * kWT; q += kThreads) {
@@ -442,71 +450,99 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
                 Msm[n * kRows + 2 * wl + 1] = valid ? (Real)(ar * pi + ai * pr) : (Real)0;
             }
             __syncthreads();
-            if (ch + 1 < n_chunks) fetch(k0 + kKC);  // overlaps the GEMM below
+            if (ch + 1 < n_chunks) fetch(k0 + kKC);  // in flight during the GEMM below
             if constexpr (sizeof(Real) == 8) {
-#pragma unroll 8
+#pragma unroll 4
                 for (int n = 0; n < kKC; ++n) {
-                    double a[kTM], bb[kTN];
+                    double a[kTM], bb[TN];
+                    const double2* ap = reinterpret_cast<const double2*>(Msm + n * kRows + ty * kTM);
+                    const double2* bp = reinterpret_cast<const double2*>(Bsm + n * BS + tx * TN);
 #pragma unroll
-                    for (int r = 0; r < kTM; ++r) a[r] = Msm[n * kRows + ty * kTM + r];
+                    for (int r = 0; r < kTM / 2; ++r) {
+                        const double2 v = ap[r];
+                        a[2 * r] = v.x;
+                        a[2 * r + 1] = v.y;
+                    }
 #pragma unroll
-                    for (int u = 0; u < kTN; ++u) bb[u] = Bsm[(tx * kTN + u) * BP + n];
-#pragma unroll
-                    for (int r = 0; r < kTM; ++r)
-#pragma unroll
-                        for (int u = 0; u < kTN; ++u) acc[r][u] = fma(a[r], bb[u], acc[r][u]);
-                }
-            } else {
-#pragma unroll 1
-                for (int n0 = 0; n0 < kKC; n0 += kFold) {
-                    float cacc[kTM][kTN];
-#pragma unroll
-                    for (int r = 0; r < kTM; ++r)
-#pragma unroll
-                        for (int u = 0; u < kTN; ++u) cacc[r][u] = 0.0f;
-#pragma unroll
-                    for (int n = n0; n < n0 + kFold; ++n) {
-                        float a[kTM], bb[kTN];
-#pragma unroll
-                        for (int r = 0; r < kTM; ++r) a[r] = (float)Msm[n * kRows + ty * kTM + r];
-#pragma unroll
-                        for (int u = 0; u < kTN; ++u) bb[u] = (float)Bsm[(tx * kTN + u) * BP + n];
-#pragma unroll
-                        for (int r = 0; r < kTM; ++r)
-#pragma unroll
-                            for (int u = 0; u < kTN; ++u) cacc[r][u] = fmaf(a[r], bb[u], cacc[r][u]);
+                    for (int u = 0; u < TN / 2; ++u) {
+                        const double2 v = bp[u];
+                        bb[2 * u] = v.x;
+                        bb[2 * u + 1] = v.y;
                     }
 #pragma unroll
                     for (int r = 0; r < kTM; ++r)
 #pragma unroll
-                        for (int u = 0; u < kTN; ++u) acc[r][u] += (double)cacc[r][u];
+                        for (int u = 0; u < TN; ++u) acc[r][u] = fma(a[r], bb[u], acc[r][u]);
+                }
+            } else {
+#pragma unroll 1
+                for (int n0 = 0; n0 < kKC; n0 += kFold) {
+                    float cacc[kTM][TN];
+#pragma unroll
+                    for (int r = 0; r < kTM; ++r)
+#pragma unroll
+                        for (int u = 0; u < TN; ++u) cacc[r][u] = 0.0f;
+#pragma unroll
+                    for (int n = n0; n < n0 + kFold; ++n) {
+                        float a[kTM], bb[TN];
+                        const float4* ap = reinterpret_cast<const float4*>(Msm + n * kRows + ty * kTM);
+                        const float4* bp = reinterpret_cast<const float4*>(Bsm + n * BS + tx * TN);
+#pragma unroll
+                        for (int r = 0; r < kTM / 4; ++r) {
+                            const float4 v = ap[r];
+                            a[4 * r] = v.x;
+                            a[4 * r + 1] = v.y;
+                            a[4 * r + 2] = v.z;
+                            a[4 * r + 3] = v.w;
+                        }
+#pragma unroll
+                        for (int u = 0; u < TN / 4; ++u) {
+                            const float4 v = bp[u];
+                            bb[4 * u] = v.x;
+                            bb[4 * u + 1] = v.y;
+                            bb[4 * u + 2] = v.z;
+                            bb[4 * u + 3] = v.w;
+                        }
+#pragma unroll
+                        for (int r = 0; r < kTM; ++r)
+#pragma unroll
+                            for (int u = 0; u < TN; ++u) cacc[r][u] = fmaf(a[r], bb[u], cacc[r][u]);
+                    }
+#pragma unroll
+                    for (int r = 0; r < kTM; ++r)
+#pragma unroll
+                        for (int u = 0; u < TN; ++u) acc[r][u] += (double)cacc[r][u];
                 }
             }
             __syncthreads();
         }
-        // epilogue: C_{s,g}(w) += sum_b E(w, b) Y(w, (b, s, g))
+        // epilogue: per thread, C_{s,g}(w) partials of its columns in fixed order
+        double2* my = red + (size_t)tid * 4 * cpb;
+        for (int q = 0; q < 4 * cpb; ++q) my[q] = make_double2(0.0, 0.0);
 #pragma unroll
         for (int q = 0; q < kTM / 2; ++q) {
-            const int wl = (ty * kTM) / 2 + q;
+            const int wl = ty * (kTM / 2) + q;
+            const int wi = w0 + wl;
 #pragma unroll
-            for (int u = 0; u < kTN; ++u) {
-                const int col = tx * kTN + u;
-                const int b = col / cols_per_b;
-                double2 v = make_double2(0.0, 0.0);
-                if (b < A.bpt) {
-                    const double er = E_re[wl * 32 + b], ei = E_im[wl * 32 + b];
-                    const double yr = acc[2 * q][u], yi = acc[2 * q + 1][u];
-                    v = make_double2(er * yr - ei * yi, er * yi + ei * yr);
-                }
-                Yt[col * kWT + wl] = v;
+            for (int u = 0; u < TN; ++u) {
+                const int col = tx * TN + u;
+                const int b = col / cpb;
+                if (b >= A.bpt || binfo[b] < 0 || wi >= A.n_w) continue;
+                double sn, cs;
+                phase<Real>(A.w[wi] * (bt[b] * ci - bz[b]), sn, cs);
+                const double yr = acc[2 * q][u], yi = acc[2 * q + 1][u];
+                double2& d = my[q * cpb + (col % cpb)];
+                d.x += cs * yr - sn * yi;
+                d.y += cs * yi + sn * yr;
             }
         }
         __syncthreads();
-        for (int q = tid; q < kWT * A.S * 2; q += kThreads) {
-            const int wl = q / (A.S * 2), sg = q % (A.S * 2);
+        for (int q = tid; q < kWT * cpb; q += kThreads) {
+            const int wl = q / cpb, sg = q % cpb;
+            const int tyw = wl / (kTM / 2), qq = wl % (kTM / 2);
             double2 sum = Cacc[q];
-            for (int b = 0; b < A.bpt; ++b) {
-                const double2 v = Yt[(b * cols_per_b + sg) * kWT + wl];
+            for (int t = 0; t < 16; ++t) {
+                const double2 v = red[((size_t)(tyw * 16 + t) * 4 + qq) * cpb + sg];
                 sum.x += v.x;
                 sum.y += v.y;
             }
@@ -514,8 +550,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
         }
         __syncthreads();
     }
-    for (int q = tid; q < kWT * A.S * 2; q += kThreads) {
-        const int wl = q / (A.S * 2), sg = q % (A.S * 2);
+    for (int q = tid; q < kWT * cpb; q += kThreads) {
+        const int wl = q / cpb, sg = q % cpb;
         const int s = sg >> 1, g = sg & 1;
         const int wi = w0 + wl;
         if (wi >= A.n_w) continue;
@@ -540,31 +576,36 @@ __global__ void k_reduce_tiles(const double2* __restrict__ partial, int tiles, s
 }
 
 // ---------------------------------------------------------------------------
-template <class Real>
+template <class Real, int TN>
 static size_t gemm_smem_bytes(int S) {
-    constexpr int BP = kKC + (sizeof(Real) == 4 ? 4 : 2);
-    size_t b = (size_t)kKC * kRows * sizeof(Real) + (size_t)kCols * BP * sizeof(Real);
+    constexpr int COLS = 16 * TN;
+    constexpr int BS = COLS + 16 / (int)sizeof(Real);
+    size_t b = (size_t)kKC * kRows * sizeof(Real) + (size_t)kKC * BS * sizeof(Real);
     b = (b + 15) & ~(size_t)15;
-    b += 2 * (size_t)kKC * kWT * sizeof(double);
-    b += 2 * (size_t)kWT * 32 * sizeof(double);
-    b += (size_t)kCols * kWT * sizeof(double2);
-    b += (size_t)kWT * S * 2 * sizeof(double2);
-    b += 2 * kWT * sizeof(double);
-    b += 32 * sizeof(int);
+    b += 2 * (size_t)kKC * kWT * sizeof(double);   // step table
+    b += 2 * (size_t)kWT * sizeof(double);         // anchors
+    b += (size_t)kThreads * 4 * 2 * S * sizeof(double2);  // epilogue partials
+    b += (size_t)kWT * 2 * S * sizeof(double2);    // C accumulator
+    b += 64 * sizeof(int) + 2 * 64 * sizeof(double);
     return b;
 }
 
+template <class Real>
+constexpr int gemm_tn() { return sizeof(Real) == 4 ? 8 : 4; }
+
 struct FactGeom {
-    int bpt, tiles_per_frame, t_pad, nblk;
+    int bpt, tiles_per_frame, t_pad, nblk, tile_cols;
     long cols_pad;
 };
 
 static FactGeom fact_geom(const SpectrumJob& job, size_t real_size) {
     FactGeom g;
     const int S = (int)job.n_sets;
-    g.bpt = std::min(32, kCols / (2 * S));
+    const int cols = 16 * (real_size == 4 ? 8 : 4);
+    g.tile_cols = cols;
+    g.bpt = std::min(64, cols / (2 * S));
     g.tiles_per_frame = (int)((job.n_sel + g.bpt - 1) / g.bpt);
-    g.cols_pad = (long)g.tiles_per_frame * g.bpt * 2 * S;
+    g.cols_pad = (long)g.tiles_per_frame * cols;  // every tile is `cols` wide; unused columns stay zero
     const int align = real_size == 4 ? 4 : 2;
     g.t_pad = (int)((job.n_t + align - 1) / align * align);
     g.nblk = (int)((job.n_t + 31) / 32);
@@ -579,7 +620,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     const int S = (int)job.n_sets, M = (int)job.n_terms, SM = S * M;
     const int n_t = (int)job.n_t, n_cos = (int)job.n_cos, n_phi = (int)job.n_phi, n_w = (int)job.n_w;
     const int n_sel = (int)job.n_sel;
-    if (SM > 8 || 2 * S > kCols)
+    if (SM > 8 || 2 * S > 16 * gemm_tn<Real>())
         throw Error{"the factored kernels support at most 8 (set, term) pairs; use the fp64_direct kernel"};
     if (job.has_damping) {
         const double span = job.t_arr[job.n_t - 1] - job.t_arr[0] + 4.0;
@@ -602,10 +643,10 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     }
     // beta
     const size_t beta_elems = (size_t)kn * n_cos * G.cols_pad * G.t_pad;
-    dev->ev_q.ensure(beta_elems * sizeof(Real));
-    if ((long)n_sel * 2 * S != G.cols_pad) {
+    dev->beta.ensure(beta_elems * sizeof(Real));
+    if ((long)n_sel * 2 * S != G.cols_pad) {  // unused tile columns must read as zero
         // padding columns of the last tile are read by the GEMM: keep them zero
-        CUDA_OK(cudaMemsetAsync(dev->ev_q.p, 0, beta_elems * sizeof(Real), dev->stream));
+        CUDA_OK(cudaMemsetAsync(dev->beta.p, 0, beta_elems * sizeof(Real), dev->stream));
     }
     {
         BetaArgs B;
@@ -634,6 +675,8 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         B.n_rows = (long)kn * n_sel * n_cos;
         B.nblk = G.nblk;
         B.cols_pad = G.cols_pad;
+        B.tile_cols = G.tile_cols;
+        B.bpt = G.bpt;
         B.t_pad = G.t_pad;
         const int NQ = 2 + 2 * SM;
         size_t pw = (size_t)n_phi * NQ * sizeof(double) + 4 * (size_t)G.nblk * sizeof(double) +
@@ -645,7 +688,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         const size_t smem = (size_t)warps * pw;
         CUDA_OK(cudaFuncSetAttribute(k_beta<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const unsigned blocks = (unsigned)((B.n_rows + warps - 1) / warps);
-        k_beta<Real><<<blocks, warps * 32, smem, dev->stream>>>(B, (Real*)dev->ev_q.p);
+        k_beta<Real><<<blocks, warps * 32, smem, dev->stream>>>(B, (Real*)dev->beta.p);
         CUDA_OK(cudaGetLastError());
         ++launches;
     }
@@ -663,7 +706,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     A.w = w;
     A.cos_t = cos_t;
     A.kfirst = (const int*)dev->fact_kfirst.p;
-    A.beta = dev->ev_q.p;
+    A.beta = dev->beta.p;
     A.cols_pad = G.cols_pad;
     A.t_pad = G.t_pad;
     A.dt = job.dt;
@@ -672,12 +715,14 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     const size_t per = (size_t)2 * S * n_w;
     dev->fact_partial.ensure((size_t)kn * G.tiles_per_frame * per * sizeof(double2));
     A.partial = (double2*)dev->fact_partial.p;
-    const size_t smem = gemm_smem_bytes<Real>(S);
-    CUDA_OK(cudaFuncSetAttribute(k_gemm<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    constexpr int TN = gemm_tn<Real>();
+    const size_t smem = gemm_smem_bytes<Real, TN>(S);
+    if (smem > 227 * 1024) throw Error{"too many coefficient sets for the factored kernel's shared memory"};
+    CUDA_OK(cudaFuncSetAttribute(k_gemm<Real, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     const size_t gy = (size_t)kn * G.tiles_per_frame;
     if (gy > 65535) throw Error{"too many column tiles in one k-hat chunk"};
     dim3 grid((unsigned)((n_w + kWT - 1) / kWT), (unsigned)gy);
-    k_gemm<Real><<<grid, kThreads, smem, dev->stream>>>(A);
+    k_gemm<Real, TN><<<grid, kThreads, smem, dev->stream>>>(A);
     CUDA_OK(cudaGetLastError());
     ++launches;
     dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
