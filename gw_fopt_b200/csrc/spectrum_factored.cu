@@ -133,12 +133,12 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         if (j >= A.n_phi) return -2;  // not a patch
         const double tj = trow[j];
         if (!(tj > 0.0)) return -1;    // never collides
-        int lo = 0, hi = A.n_t;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            if (A.t_arr[mid] - ta >= tj) hi = mid;
-            else lo = mid + 1;
-        }
+        // first k with (t_k - t_a) >= tau_j: arithmetic estimate, then exact
+        // comparisons (the predicate is monotone in k) settle the boundary
+        const double est = ceil((ta + tj - A.t_arr[0]) / A.dt);
+        int lo = est < 0.0 ? 0 : (est > (double)A.n_t ? A.n_t : (int)est);
+        while (lo > 0 && A.t_arr[lo - 1] - ta >= tj) --lo;
+        while (lo < A.n_t && !(A.t_arr[lo] - ta >= tj)) ++lo;
         kj = lo;
         return lo < A.n_t ? lo >> 5 : -1;
     };
@@ -242,35 +242,44 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         double h[18];
 #pragma unroll
         for (int q = 0; q < 18; ++q) h[q] = 0.0;
+        const bool events = boff[b] != boff[b + 1];  // warp-uniform
         for (int e = boff[b]; e < boff[b + 1]; ++e) {
             if (evk[e] != k) continue;
 #pragma unroll
             for (int q = 0; q < 18; ++q)
                 if (q < NQ) h[q] += evq[(size_t)e * NQ + q];
         }
-        // exclusive suffix over lanes of the uncollided weights
-        double uc = h[0], us = h[1];
-        for (int o = 1; o < 32; o <<= 1) {
-            const double tc = __shfl_down_sync(full, uc, o), ts = __shfl_down_sync(full, us, o);
-            if (lane + o < 32) {
-                uc += tc;
-                us += ts;
-            }
-        }
-        double xc = __shfl_down_sync(full, uc, 1), xs = __shfl_down_sync(full, us, 1);
-        if (lane == 31) xc = xs = 0.0;
-        const double Uc = uend[2 * b] + xc, Us = uend[2 * b + 1] + xs;
-        // inclusive prefix over lanes of the collided weights
-#pragma unroll
-        for (int q = 2; q < 18; ++q) {
-            if (q >= NQ) break;
-            double v = h[q];
+        double Uc = uend[2 * b], Us = uend[2 * b + 1];
+        if (events) {
+            // exclusive suffix over lanes of the uncollided weights
+            double uc = h[0], us = h[1];
             for (int o = 1; o < 32; o <<= 1) {
-                const double t = __shfl_up_sync(full, v, o);
-                if (lane >= o) v += t;
+                const double tc = __shfl_down_sync(full, uc, o), ts = __shfl_down_sync(full, us, o);
+                if (lane + o < 32) {
+                    uc += tc;
+                    us += ts;
+                }
             }
-            h[q] = pstart[q - 2] + v;
-            pstart[q - 2] += __shfl_sync(full, v, 31);
+            double xc = __shfl_down_sync(full, uc, 1), xs = __shfl_down_sync(full, us, 1);
+            if (lane == 31) xc = xs = 0.0;
+            Uc += xc;
+            Us += xs;
+            // inclusive prefix over lanes of the collided weights
+#pragma unroll
+            for (int q = 2; q < 18; ++q) {
+                if (q >= NQ) break;
+                double v = h[q];
+                for (int o = 1; o < 32; o <<= 1) {
+                    const double t = __shfl_up_sync(full, v, o);
+                    if (lane >= o) v += t;
+                }
+                h[q] = pstart[q - 2] + v;
+                pstart[q - 2] += __shfl_sync(full, v, 31);
+            }
+        } else {
+#pragma unroll
+            for (int q = 2; q < 18; ++q)
+                if (q < NQ) h[q] = pstart[q - 2];
         }
         if (k < A.n_t) {
             const double* Drow = A.D + ((size_t)slot * A.n_t + k) * (1 + SM);
@@ -343,7 +352,14 @@ __device__ __forceinline__ void phase<float>(double arg, double& s, double& c) {
 
 // One CTA per (64-frequency tile, column tile), looping over the rows i.
 // Thread (ty, tx) of 16 x 16 owns rows ty*8 .. ty*8+7 (frequencies ty*4 .. +3,
-// Re/Im interleaved) and columns tx*TN .. tx*TN+TN-1.
+// Re/Im interleaved) and TN columns in two groups of TN/2: tx*TN/2 + u and
+// COLS/2 + tx*TN/2 + u, so that consecutive threads read consecutive 16-byte
+// words of a beta-tile row (no shared-memory bank conflicts).
+template <int TN, int COLS>
+__device__ __forceinline__ int thread_col(int tx, int u) {
+    return u < TN / 2 ? tx * (TN / 2) + u : COLS / 2 + tx * (TN / 2) + (u - TN / 2);
+}
+
 template <class Real, int TN>
 __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -456,7 +472,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
                 for (int n = 0; n < kKC; ++n) {
                     double a[kTM], bb[TN];
                     const double2* ap = reinterpret_cast<const double2*>(Msm + n * kRows + ty * kTM);
-                    const double2* bp = reinterpret_cast<const double2*>(Bsm + n * BS + tx * TN);
+                    const double2* bp0 = reinterpret_cast<const double2*>(Bsm + n * BS + tx * (TN / 2));
+                    const double2* bp1 = reinterpret_cast<const double2*>(Bsm + n * BS + COLS / 2 + tx * (TN / 2));
 #pragma unroll
                     for (int r = 0; r < kTM / 2; ++r) {
                         const double2 v = ap[r];
@@ -464,10 +481,12 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
                         a[2 * r + 1] = v.y;
                     }
 #pragma unroll
-                    for (int u = 0; u < TN / 2; ++u) {
-                        const double2 v = bp[u];
-                        bb[2 * u] = v.x;
-                        bb[2 * u + 1] = v.y;
+                    for (int u = 0; u < TN / 4; ++u) {
+                        const double2 v0 = bp0[u], v1 = bp1[u];
+                        bb[2 * u] = v0.x;
+                        bb[2 * u + 1] = v0.y;
+                        bb[TN / 2 + 2 * u] = v1.x;
+                        bb[TN / 2 + 2 * u + 1] = v1.y;
                     }
 #pragma unroll
                     for (int r = 0; r < kTM; ++r)
@@ -486,7 +505,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
                     for (int n = n0; n < n0 + kFold; ++n) {
                         float a[kTM], bb[TN];
                         const float4* ap = reinterpret_cast<const float4*>(Msm + n * kRows + ty * kTM);
-                        const float4* bp = reinterpret_cast<const float4*>(Bsm + n * BS + tx * TN);
+                        const float4 b0 = *reinterpret_cast<const float4*>(Bsm + n * BS + tx * (TN / 2));
+                        const float4 b1 = *reinterpret_cast<const float4*>(Bsm + n * BS + COLS / 2 + tx * (TN / 2));
 #pragma unroll
                         for (int r = 0; r < kTM / 4; ++r) {
                             const float4 v = ap[r];
@@ -495,14 +515,14 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
                             a[4 * r + 2] = v.z;
                             a[4 * r + 3] = v.w;
                         }
-#pragma unroll
-                        for (int u = 0; u < TN / 4; ++u) {
-                            const float4 v = bp[u];
-                            bb[4 * u] = v.x;
-                            bb[4 * u + 1] = v.y;
-                            bb[4 * u + 2] = v.z;
-                            bb[4 * u + 3] = v.w;
-                        }
+                        bb[0] = b0.x;
+                        bb[1] = b0.y;
+                        bb[2] = b0.z;
+                        bb[3] = b0.w;
+                        bb[4] = b1.x;
+                        bb[5] = b1.y;
+                        bb[6] = b1.z;
+                        bb[7] = b1.w;
 #pragma unroll
                         for (int r = 0; r < kTM; ++r)
 #pragma unroll
@@ -517,21 +537,21 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
             __syncthreads();
         }
         // epilogue: per thread, C_{s,g}(w) partials of its columns in fixed order
-        double2* my = red + (size_t)tid * 4 * cpb;
-        for (int q = 0; q < 4 * cpb; ++q) my[q] = make_double2(0.0, 0.0);
+        // partials in structure-of-arrays order red[(q*cpb + sg)*kThreads + tid]
+        for (int q = 0; q < 4 * cpb; ++q) red[(size_t)q * kThreads + tid] = make_double2(0.0, 0.0);
 #pragma unroll
         for (int q = 0; q < kTM / 2; ++q) {
             const int wl = ty * (kTM / 2) + q;
             const int wi = w0 + wl;
 #pragma unroll
             for (int u = 0; u < TN; ++u) {
-                const int col = tx * TN + u;
+                const int col = thread_col<TN, COLS>(tx, u);
                 const int b = col / cpb;
                 if (b >= A.bpt || binfo[b] < 0 || wi >= A.n_w) continue;
                 double sn, cs;
                 phase<Real>(A.w[wi] * (bt[b] * ci - bz[b]), sn, cs);
                 const double yr = acc[2 * q][u], yi = acc[2 * q + 1][u];
-                double2& d = my[q * cpb + (col % cpb)];
+                double2& d = red[(size_t)(q * cpb + (col % cpb)) * kThreads + tid];
                 d.x += cs * yr - sn * yi;
                 d.y += cs * yi + sn * yr;
             }
@@ -542,7 +562,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
             const int tyw = wl / (kTM / 2), qq = wl % (kTM / 2);
             double2 sum = Cacc[q];
             for (int t = 0; t < 16; ++t) {
-                const double2 v = red[((size_t)(tyw * 16 + t) * 4 + qq) * cpb + sg];
+                const double2 v = red[(size_t)(qq * cpb + sg) * kThreads + tyw * 16 + t];
                 sum.x += v.x;
                 sum.y += v.y;
             }
