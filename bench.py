@@ -45,8 +45,9 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--config", type=int, default=2)
-    ap.add_argument("--kernel", default="fp64_direct", choices=["fp64_direct", "fp64_factored", "mixed"])
+    ap.add_argument("--config", type=int, default=3)
+    ap.add_argument("--kernel", default="mixed", choices=["fp64_direct", "fp64_factored", "mixed"])
+    ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison measurements")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -134,6 +135,38 @@ def cpu_baseline(cfg, seconds: float, threads: int | None = None):
     return {"value": pte / dt, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{n_sel} radiating bubbles x 1 k-hat of {cfg.name} (all {cfg.interior.shape[0] + cfg.exterior.shape[0]}"
                       f" colliders), {dt:.1f} s", "seconds": dt}
+
+
+def compare_fp64(cfg, kernel, res, lib, L):
+    """FP64 kernels on stated subsets of the same workload (directions are independent, and a
+    subset of radiating bubbles with every collider present is an exact partial sum), plus the
+    error of this run's spectrum against fp64_factored on the same directions."""
+    from gw_fopt_b200 import workloads as W
+    out = {}
+    sub = min(16, cfg.khat.shape[0])
+    g = make_flow(cfg, "fp64_factored")
+    ref = g.compute_c_integral_khat(cfg.w, cfg.khat[:sub], t_begin=cfg.t_begin, t_end=cfg.t_end, n_t=cfg.n_t)
+    t = g.last_timings()
+    pte = sub * cfg.n * cfg.n_cos * cfg.n_phi * cfg.n_t
+    out["fp64_factored"] = {"value": pte / (t["total_ms"] * 1e-3), "unit": UNIT, "sample": f"{sub} of {cfg.khat.shape[0]} k-hat"}
+    if kernel == "mixed":
+        got = res[:sub]
+        d = (got - ref).reshape(-1, ref.shape[-1])
+        r = ref.reshape(-1, ref.shape[-1])
+        per_w = np.linalg.norm(d, axis=0) / np.linalg.norm(r, axis=0)
+        out["mixed_error_vs_fp64"] = {"global": float(np.linalg.norm(d) / np.linalg.norm(r)),
+                                      "peak_scaled": float(np.linalg.norm(d, axis=0).max() / np.linalg.norm(r, axis=0).max()),
+                                      "per_w_median": float(np.median(per_w)), "per_w_max": float(per_w.max()),
+                                      "sample": f"{sub} k-hat"}
+    gd = make_flow(cfg, "fp64_direct")
+    n_rad = min(cfg.n, 128)
+    sel = np.arange(n_rad)
+    gd.compute_c_integral_khat(cfg.w, cfg.khat[:1], t_begin=cfg.t_begin, t_end=cfg.t_end, n_t=cfg.n_t, selected_bubbles=sel)
+    t = gd.last_timings()
+    pte = n_rad * cfg.n_cos * cfg.n_phi * cfg.n_t
+    out["fp64_direct"] = {"value": pte / (t["total_ms"] * 1e-3), "unit": UNIT,
+                          "sample": f"{n_rad} radiating bubbles (all colliders) x 1 k-hat"}
+    return out
 
 
 def dist_env():
@@ -243,20 +276,22 @@ def run_b200(args):
                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e / args.steps}
         assert np.array_equal(host_out, res)
 
-    # roofline of the dominant kernel (counted-flop convention F = 6 PTE + 8 Phi + 20 Phi_t)
+    # roofline.  Counted work (declared convention) F = 6 PTE + 8 Phi + 20 Phi_t of the whole
+    # spectrum stage, over the spectrum kernels' time; the dominant kernel's own executed
+    # work (the time-phase GEMM: 2 * (2W) * n_t * columns * n_cos flops per frame) is reported
+    # beside it against the same FMA peak.
     p64, p32, psfu = C.c_double(), C.c_double(), C.c_double()
     L.check(lib.bgwx_measure_compute_peaks(C.byref(p64), C.byref(p32), C.byref(psfu)))
     peaks = {"fp64_tflops": p64.value / 1e12, "fp32_tflops": p32.value / 1e12, "sfu_tops": psfu.value / 1e12}
     spec_s = tm["spectrum_ms"] * 1e-3
-    masks_s = tm["masks_ms"] * 1e-3
-    dominant = "spectrum" if spec_s >= masks_s else "masks"
+    peak = (p32.value if args.kernel == "mixed" else p64.value) / 1e12
+    bound = "fp32" if args.kernel == "mixed" else "fp64"
     achieved = cfg.counted_flops / spec_s / 1e12 if spec_s > 0 else None
-    if args.kernel == "mixed":
-        peak = p32.value / 1e12
-        bound = "fp32"
-    else:
-        peak = p64.value / 1e12
-        bound = "fp64"
+    gemm = None
+    if args.kernel != "fp64_direct" and tm["gemm_ms"] > 0:
+        gemm_flops = 2.0 * (2 * Wn) * cfg.n_t * (cfg.n * 2 * S) * cfg.n_cos * K
+        gemm = {"kernel": "k_gemm", "ms_per_step": tm["gemm_ms"], "executed_tflops": gemm_flops / (tm["gemm_ms"] * 1e-3) / 1e12,
+                "frac_of_peak": gemm_flops / (tm["gemm_ms"] * 1e-3) / 1e12 / peak, "beta_ms_per_step": tm["beta_ms"]}
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
@@ -266,11 +301,16 @@ def run_b200(args):
             traffic = None
     roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "kernel": f"spectrum ({args.kernel})", "dominant_kernel": dominant,
-                "spectrum_ms": tm["spectrum_ms"], "masks_ms": tm["masks_ms"],
-                "peak_source": "measured on this GPU by bgwx_measure_compute_peaks (FMA chains); "
-                               "MEASURED_PEAKS.json has HBM/bf16 only", "peaks": peaks}
+                "kernel": f"spectrum stage ({args.kernel}): k_time_tables + k_beta + k_gemm + k_reduce_tiles"
+                          if args.kernel != "fp64_direct" else "k_spec_direct + k_reduce",
+                "work": "counted F = 6 PTE + 8 Phi + 20 Phi_t per step",
+                "spectrum_ms": tm["spectrum_ms"], "masks_ms": tm["masks_ms"], "dominant_gemm": gemm,
+                "peak_source": "measured on this GPU (bgwx_measure_compute_peaks: FMA chains, of measured); "
+                               "MEASURED_PEAKS.json holds HBM/bf16 only", "peaks": peaks}
 
+    compare = None
+    if not args.no_compare and world == 1:
+        compare = compare_fp64(cfg, args.kernel, res, lib, L)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if args.kernel != "mixed" else "f32+f64", "data": "synthetic",
@@ -278,7 +318,12 @@ def run_b200(args):
                        "n_cos": cfg.n_cos, "n_phi": cfg.n_phi, "n_t": cfg.n_t, "n_w": int(Wn),
                        "n_khat_per_gpu": int(K), "kernel": args.kernel, "pte_per_step": pte_total,
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"khat-shard x{world}"},
-            "roofline": roofline, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clocks}
+            "roofline": roofline, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
+            "compare": compare}
+    if compare:
+        for k in ("fp64_factored", "fp64_direct"):
+            if k in compare:
+                compare[f"{args.kernel}_over_{k}"] = value / compare[k]["value"]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, args.cpu_seconds)
     if rank == 0:

@@ -72,6 +72,8 @@ Device::~Device() {
         if (e) cudaEventDestroy(e);
     for (auto& e : chunk_ev)
         if (e) cudaEventDestroy(e);
+    for (auto& e : fact_ev)
+        if (e) cudaEventDestroy(e);
 }
 
 // ---------------------------------------------------------------------------
@@ -423,6 +425,11 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
         CUDA_OK(cudaEventCreate(&e));
         dev->chunk_ev.push_back(e);
     }
+    while (dev->fact_ev.size() < 3 * n_chunks) {
+        cudaEvent_t e;
+        CUDA_OK(cudaEventCreate(&e));
+        dev->fact_ev.push_back(e);
+    }
     if (rot) dev->bubrot.ensure(kc * job.n_tot * sizeof(D4));
     dev->counters.ensure(64);
     CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
@@ -493,7 +500,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             ++launches;
         } else {
             launches += launch_factored(dev, job, fb, sel, (const double*)dev->tau.p, cos_t, sin2, cos2, coeffs,
-                                        powers, t_arr, cutw, w, kn, final_out + k0 * per);
+                                        powers, t_arr, cutw, w, kn, final_out + k0 * per, &dev->fact_ev[3 * ci]);
         }
         CUDA_OK(cudaEventRecord(cev[2], dev->stream));
     }
@@ -508,16 +515,26 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     CUDA_OK(cudaStreamSynchronize(dev->stream));
     float total = 0, ms_masks = 0, ms_spec = 0;
     CUDA_OK(cudaEventElapsedTime(&total, dev->ev[4], dev->ev[5]));
+    float ms_beta = 0, ms_gemm = 0;
     for (size_t ci = 0; ci < n_chunks; ++ci) {
         float a = 0, b = 0;
         CUDA_OK(cudaEventElapsedTime(&a, dev->chunk_ev[3 * ci], dev->chunk_ev[3 * ci + 1]));
         CUDA_OK(cudaEventElapsedTime(&b, dev->chunk_ev[3 * ci + 1], dev->chunk_ev[3 * ci + 2]));
         ms_masks += a;
         ms_spec += b;
+        if (job.kernel != BGWX_KERNEL_FP64_DIRECT) {
+            float c = 0, d = 0;
+            CUDA_OK(cudaEventElapsedTime(&c, dev->fact_ev[3 * ci], dev->fact_ev[3 * ci + 1]));
+            CUDA_OK(cudaEventElapsedTime(&d, dev->fact_ev[3 * ci + 1], dev->fact_ev[3 * ci + 2]));
+            ms_beta += c;
+            ms_gemm += d;
+        }
     }
     if (tm) {
         tm->masks_ms += ms_masks;
         tm->spectrum_ms += ms_spec;
+        tm->beta_ms += ms_beta;
+        tm->gemm_ms += ms_gemm;
         tm->total_ms += total;
         tm->launches += launches;
         tm->directions += K * job.n_sel * nd;

@@ -636,7 +636,7 @@ template <class Real>
 static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_frames, const uint32_t* sel,
                              const double* tau, const double* cos_t, const double* sin2, const double* cos2,
                              const double* coeffs, const double* powers, const double* t_arr, const double* cutw,
-                             const double* w, size_t kn, double2* out) {
+                             const double* w, size_t kn, double2* out, cudaEvent_t* ev3) {
     const int S = (int)job.n_sets, M = (int)job.n_terms, SM = S * M;
     const int n_t = (int)job.n_t, n_cos = (int)job.n_cos, n_phi = (int)job.n_phi, n_w = (int)job.n_w;
     const int n_sel = (int)job.n_sel;
@@ -662,6 +662,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         ++launches;
     }
     // beta
+    CUDA_OK(cudaEventRecord(ev3[0], dev->stream));
     const size_t beta_elems = (size_t)kn * n_cos * G.cols_pad * G.t_pad;
     dev->beta.ensure(beta_elems * sizeof(Real));
     if ((long)n_sel * 2 * S != G.cols_pad) {  // unused tile columns must read as zero
@@ -713,6 +714,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         ++launches;
     }
     // GEMM + epilogue
+    CUDA_OK(cudaEventRecord(ev3[1], dev->stream));
     FactArgs A;
     A.bub = bub_frames;
     A.n_tot = job.n_tot;
@@ -745,6 +747,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     k_gemm<Real, TN><<<grid, kThreads, smem, dev->stream>>>(A);
     CUDA_OK(cudaGetLastError());
     ++launches;
+    CUDA_OK(cudaEventRecord(ev3[2], dev->stream));
     dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
     k_reduce_tiles<<<gr, 256, 0, dev->stream>>>(A.partial, G.tiles_per_frame, per, (int)kn, out);
     CUDA_OK(cudaGetLastError());
@@ -755,12 +758,12 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
 uint64_t launch_factored(Device* dev, const SpectrumJob& job, const D4* bub_frames, const uint32_t* sel,
                          const double* tau, const double* cos_t, const double* sin2, const double* cos2,
                          const double* coeffs, const double* powers, const double* t_arr, const double* cutw,
-                         const double* w, size_t kn, double2* out) {
+                         const double* w, size_t kn, double2* out, cudaEvent_t* ev3) {
     if (job.kernel == BGWX_KERNEL_MIXED)
         return launch_typed<float>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w,
-                                   kn, out);
+                                   kn, out, ev3);
     return launch_typed<double>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, kn,
-                                out);
+                                out, ev3);
 }
 
 size_t factored_bytes_per_frame(const SpectrumJob& job) {

@@ -55,6 +55,8 @@ typedef struct BgwxTimings {
     uint64_t launches;  /* kernels launched by the last call */
     uint64_t directions;/* patch directions searched by the mask kernel */
     uint64_t fallbacks; /* directions resolved by the exact slow path */
+    double beta_ms;     /* factored kernels: beta producer */
+    double gemm_ms;     /* factored kernels: time-phase GEMM and epilogue */
 } BgwxTimings;
 
 #ifdef __cplusplus
