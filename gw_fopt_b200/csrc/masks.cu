@@ -53,6 +53,16 @@ __device__ __forceinline__ bool check_pt(const D4& dba, double nb, const D4& dca
     return mdot(cv, x) > 0.0;
 }
 
+// check(b, c) with both Minkowski norms precomputed (same values as check_pt).
+__device__ __forceinline__ bool check_pre(const D4& dba, double nb, const D4& dca, double nc, const D4& x) {
+    D4 cv;
+    cv.t = dsub(dmul(dba.t, nc), dmul(dca.t, nb));
+    cv.x = dsub(dmul(dba.x, nc), dmul(dca.x, nb));
+    cv.y = dsub(dmul(dba.y, nc), dmul(dca.y, nb));
+    cv.z = dsub(dmul(dba.z, nc), dmul(dca.z, nb));
+    return mdot(cv, x) > 0.0;
+}
+
 // Exhaustive decision for one direction (global memory): argmin, check it
 // against everything, then the failures; the reference loop if more than
 // kMaxFail failures.
@@ -280,10 +290,14 @@ __global__ void __launch_bounds__(kMaskListThreads)
                  size_t n_sel, const NbList* __restrict__ lists, const D4* __restrict__ dirs, size_t nd,
                  unsigned n_dblocks, double* __restrict__ tau_out, int32_t* __restrict__ code_out,
                  unsigned long long* __restrict__ counters) {
+    // per listed collider: Delta = x_c - x_a and its Minkowski norm, computed once
+    // per block with the reference's operations (direction independent)
     __shared__ D4 s_pos[kList];
+    __shared__ double s_nrm[kList];
     __shared__ double s_key[kList];
     __shared__ int s_idx[kList];
     __shared__ D4 s_opos[kMaxOutliers];
+    __shared__ double s_onrm[kMaxOutliers];
     __shared__ int s_oidx[kMaxOutliers];
     const int k = blockIdx.y;
     const size_t slot = blockIdx.x / n_dblocks;
@@ -301,19 +315,23 @@ __global__ void __launch_bounds__(kMaskListThreads)
         return;
     }
     const int no = L->n_outliers;
+    const D4 xa = B[a];
     for (int q = threadIdx.x; q < n; q += kMaskListThreads) {
         const int c = L->idx[q];
         s_idx[q] = c;
         s_key[q] = L->key[q];
-        s_pos[q] = B[c];
+        const D4 dc = dsub4(B[c], xa);
+        s_pos[q] = dc;
+        s_nrm[q] = mdot(dc, dc);
     }
     for (int q = threadIdx.x; q < no; q += kMaskListThreads) {
         s_oidx[q] = L->outlier[q];
-        s_opos[q] = B[L->outlier[q]];
+        const D4 dc = dsub4(B[L->outlier[q]], xa);
+        s_opos[q] = dc;
+        s_onrm[q] = mdot(dc, dc);
     }
     __syncthreads();
     if (d >= nd) return;
-    const D4 xa = B[a];
     const D4 x = dirs[d];
     const double kmax = L->kmax, rho1 = L->rho1, rho2 = L->rho2;
     const double u64 = 64.0 * 1.1102230246251565e-16;
@@ -327,7 +345,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
             if (s_key[e] > theta) break;
             const int ce = s_idx[e];
             if (ce == c) continue;
-            if (!check_pt(dc, nc, dsub4(s_pos[e], xa), x)) {
+            if (!check_pre(dc, nc, s_pos[e], s_nrm[e], x)) {
                 ok = false;
                 if (fails) {
                     if (nfail < kMaxFail) fails[nfail] = e;
@@ -343,7 +361,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
             bool in_list = false;  // already checked above when listed with key <= theta
             for (int q = 0; q < n && s_key[q] <= theta; ++q) in_list |= (s_idx[q] == ce);
             if (in_list) continue;
-            if (!check_pt(dc, nc, dsub4(s_opos[e], xa), x)) {
+            if (!check_pre(dc, nc, s_opos[e], s_onrm[e], x)) {
                 ok = false;
                 if (!fails) return false;
                 nfail = kMaxFail + 1;  // outliers are resolved by the exhaustive path
@@ -367,21 +385,24 @@ __global__ void __launch_bounds__(kMaskListThreads)
                 ended = false;
                 break;
             }
-            const D4 dba = dsub4(s_pos[e], xa);
-            const double dot = mdot(dba, x);
+            const double dot = mdot(s_pos[e], x);
             if (dot > 1e-10) {
-                const double tau = __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
-                if (tau > 0.0 && tau < best) {
-                    best = tau;
-                    bi = e;
+                // cheap filter before the exact quotient: tau < best needs nrm < 2 dot best
+                const double nrm = s_nrm[e];
+                if (nrm > 0.0 && nrm < dmul(dmul(2.0, dot), best) * (1.0 + 1e-12)) {
+                    const double tau = __ddiv_rn(nrm, dmul(2.0, dot));
+                    if (tau > 0.0 && tau < best) {
+                        best = tau;
+                        bi = e;
+                    }
                 }
             }
         }
         if (ended && !(kmax > best * (1.0 + 1e-12))) full = !(bi < 0 && kmax == CUDART_INF);
         if (!full && bi >= 0) {
             // 2. verify the argmin
-            const D4 dm = dsub4(s_pos[bi], xa);
-            const double nm = mdot(dm, dm), dotm = mdot(dm, x);
+            const D4 dm = s_pos[bi];
+            const double nm = s_nrm[bi], dotm = mdot(dm, x);
             const double th = theta_of(dm, best, dotm);
             if (!(th < kmax)) {
                 full = true;
@@ -396,10 +417,10 @@ __global__ void __launch_bounds__(kMaskListThreads)
                     // 3. the passer, if any, is among the failures
                     for (int f = 0; f < nfail && result < 0 && !full; ++f) {
                         const int e = fails[f];
-                        const D4 dc = dsub4(s_pos[e], xa);
+                        const D4 dc = s_pos[e];
                         const double dot = mdot(dc, x);
                         if (!(dot > 1e-10)) continue;
-                        const double nc = mdot(dc, dc);
+                        const double nc = s_nrm[e];
                         const double tau = __ddiv_rn(nc, dmul(2.0, dot));
                         if (!(tau > 0.0)) continue;
                         const double thf = theta_of(dc, tau, dot);

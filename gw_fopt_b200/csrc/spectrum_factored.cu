@@ -108,13 +108,14 @@ struct BetaArgs {
     int per_warp_bytes;
 };
 
-template <class Real>
+template <class Real, int SMC>
 __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ beta) {
     extern __shared__ __align__(16) unsigned char sm_b[];
+    constexpr int NQ = 2 + 2 * SMC;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long row = (long)blockIdx.x * (blockDim.x >> 5) + warp;
     if (row >= A.n_rows) return;
-    const int SM = A.S * A.M, NQ = 2 + 2 * SM, NB = A.nblk;
+    const int NB = A.nblk;
     unsigned char* base = sm_b + (size_t)warp * A.per_warp_bytes;
     double* evq = reinterpret_cast<double*>(base);             // [n_phi][NQ]
     double* btot = evq + (size_t)A.n_phi * NQ;                  // [NB][2] block totals of q0
@@ -142,44 +143,26 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         kj = lo;
         return lo < A.n_t ? lo >> 5 : -1;
     };
-    for (int b = lane; b < NB; b += 32) {
-        boff[b] = 0;
-        btot[2 * b] = btot[2 * b + 1] = 0.0;
-    }
+    for (int b = lane; b < NB; b += 32) boff[b] = 0;
     __syncwarp();
-    // pass 1: block counts, block totals of q0, never-collided sums (lane order)
+    // pass 1: events per block; never-colliding weights (lane sums, fixed-order reduction)
     double nc = 0.0, ns = 0.0;
     for (int j0 = 0; j0 < A.n_phi; j0 += 32) {
         const int j = j0 + lane;
         int kj;
         const int b = block_of(j, kj);
-        double qc = 0.0, qs = 0.0;
-        if (b >= -1) {
+        if (b == -1) {
             const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
-            qc = wj * A.cos2[j];
-            qs = wj * A.sin2[j];
+            nc += wj * A.cos2[j];
+            ns += wj * A.sin2[j];
         }
         const unsigned m = __match_any_sync(full, b);
-        const bool leader = lane == __ffs(m) - 1;
-        double gc = 0.0, gs = 0.0;
-        for (int l = 0; l < 32; ++l) {
-            const double vc = __shfl_sync(full, qc, l), vs = __shfl_sync(full, qs, l);
-            const int bl = __shfl_sync(full, b, l);
-            if (leader && bl == b) {
-                gc += vc;
-                gs += vs;
-            }
-            if (lane == 0 && bl == -1) {
-                nc += vc;
-                ns += vs;
-            }
-        }
-        if (leader && b >= 0) {
-            boff[b] += __popc(m);
-            btot[2 * b] += gc;
-            btot[2 * b + 1] += gs;
-        }
+        if (b >= 0 && lane == __ffs(m) - 1) boff[b] += __popc(m);
         __syncwarp();
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        nc += __shfl_down_sync(full, nc, o);
+        ns += __shfl_down_sync(full, ns, o);
     }
     if (lane == 0) {
         int acc = 0;
@@ -190,13 +173,6 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             acc += c;
         }
         boff[NB] = acc;
-        double uc = nc, us = ns;  // uncollided after the last block: never-colliding patches
-        for (int b = NB - 1; b >= 0; --b) {
-            uend[2 * b] = uc;
-            uend[2 * b + 1] = us;
-            uc += btot[2 * b];
-            us += btot[2 * b + 1];
-        }
     }
     __syncwarp();
     // pass 2: scatter events (stable in j within a block)
@@ -220,7 +196,8 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             q[0] = qc;
             q[1] = qs;
             const double ed = A.has_damp ? exp(tj / A.damp) : 1.0;
-            for (int t = 0; t < SM; ++t) {
+#pragma unroll
+            for (int t = 0; t < SMC; ++t) {
                 const double f = pow(tj, A.powers[t]) * ed;
                 q[2 + 2 * t] = qc * f;
                 q[3 + 2 * t] = qs * f;
@@ -228,29 +205,51 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         }
     }
     __syncwarp();
-    // pass 3: beta over the blocks of 32 steps
+    // block totals of the uncollided weights (each in event order), then the
+    // uncollided sums after each block, accumulated backwards
+    for (int b = lane; b < NB; b += 32) {
+        double c = 0.0, d = 0.0;
+        for (int e = boff[b]; e < boff[b + 1]; ++e) {
+            c += evq[(size_t)e * NQ];
+            d += evq[(size_t)e * NQ + 1];
+        }
+        btot[2 * b] = c;
+        btot[2 * b + 1] = d;
+    }
+    __syncwarp();
+    if (lane == 0) {
+        double uc = nc, us = ns;
+        for (int b = NB - 1; b >= 0; --b) {
+            uend[2 * b] = uc;
+            uend[2 * b + 1] = us;
+            uc += btot[2 * b];
+            us += btot[2 * b + 1];
+        }
+    }
+    __syncwarp();
+    // pass 3: beta over the blocks of 32 steps (lane = step within the block)
     const double ci = A.cos_t[i];
     const double vi = (i == 0 || i == A.n_cos - 1) ? 0.5 : 1.0;
     const double rf = (0.5 * (1.0 - ci * ci) * A.dphi) * (A.dcos * vi) * A.dt * (1.0 / (6.0 * CUDART_PI));
     const long col = (long)(slot / A.bpt) * A.tile_cols + (long)(slot % A.bpt) * 2 * A.S;
     Real* brow = beta + (((size_t)frame * A.n_cos + i) * A.cols_pad + col) * A.t_pad;
-    double pstart[16];
+    const double* Dslot = A.D + (size_t)slot * A.n_t * (1 + SMC);
+    double pstart[2 * SMC];
 #pragma unroll
-    for (int q = 0; q < 16; ++q) pstart[q] = 0.0;
+    for (int q = 0; q < 2 * SMC; ++q) pstart[q] = 0.0;
     for (int b = 0; b < NB; ++b) {
         const int k = (b << 5) + lane;
-        double h[18];
-#pragma unroll
-        for (int q = 0; q < 18; ++q) h[q] = 0.0;
-        const bool events = boff[b] != boff[b + 1];  // warp-uniform
-        for (int e = boff[b]; e < boff[b + 1]; ++e) {
-            if (evk[e] != k) continue;
-#pragma unroll
-            for (int q = 0; q < 18; ++q)
-                if (q < NQ) h[q] += evq[(size_t)e * NQ + q];
-        }
         double Uc = uend[2 * b], Us = uend[2 * b + 1];
-        if (events) {
+        double P[2 * SMC];
+        if (boff[b] != boff[b + 1]) {  // warp-uniform: this block has events
+            double h[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) h[q] = 0.0;
+            for (int e = boff[b]; e < boff[b + 1]; ++e) {
+                if (evk[e] != k) continue;
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) h[q] += evq[(size_t)e * NQ + q];
+            }
             // exclusive suffix over lanes of the uncollided weights
             double uc = h[0], us = h[1];
             for (int o = 1; o < 32; o <<= 1) {
@@ -266,32 +265,31 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             Us += xs;
             // inclusive prefix over lanes of the collided weights
 #pragma unroll
-            for (int q = 2; q < 18; ++q) {
-                if (q >= NQ) break;
-                double v = h[q];
+            for (int q = 0; q < 2 * SMC; ++q) {
+                double v = h[2 + q];
                 for (int o = 1; o < 32; o <<= 1) {
                     const double t = __shfl_up_sync(full, v, o);
                     if (lane >= o) v += t;
                 }
-                h[q] = pstart[q - 2] + v;
-                pstart[q - 2] += __shfl_sync(full, v, 31);
+                P[q] = pstart[q] + v;
+                pstart[q] += __shfl_sync(full, v, 31);
             }
         } else {
 #pragma unroll
-            for (int q = 2; q < 18; ++q)
-                if (q < NQ) h[q] = pstart[q - 2];
+            for (int q = 0; q < 2 * SMC; ++q) P[q] = pstart[q];
         }
         if (k < A.n_t) {
-            const double* Drow = A.D + ((size_t)slot * A.n_t + k) * (1 + SM);
+            const double* Drow = Dslot + (size_t)k * (1 + SMC);
             const double d3 = Drow[0];
             const double wk = rf * A.cutw[k] * ((k == 0 || k == A.n_t - 1) ? 0.5 : 1.0);
             for (int s = 0; s < A.S; ++s) {
                 double vc = d3 * Uc, vs = d3 * Us;
-                for (int m = 0; m < A.M; ++m) {
-                    const int t = s * A.M + m;
+#pragma unroll
+                for (int t = 0; t < SMC; ++t) {
+                    if (t / A.M != s) continue;
                     const double f = A.coeffs[t] * Drow[1 + t];
-                    vc += f * h[2 + 2 * t];
-                    vs += f * h[3 + 2 * t];
+                    vc += f * P[2 * t];
+                    vs += f * P[2 * t + 1];
                 }
                 const bool on = d3 != 0.0;
                 brow[(size_t)(2 * s) * A.t_pad + k] = on ? (Real)(wk * vc) : (Real)0;
@@ -300,6 +298,29 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         } else if (k < A.t_pad) {
             for (int c = 0; c < 2 * A.S; ++c) brow[(size_t)c * A.t_pad + k] = (Real)0;
         }
+    }
+}
+
+template <class Real, int SMC>
+static void launch_beta_smc(const BetaArgs& B, Real* out, size_t smem, unsigned blocks, int threads,
+                            cudaStream_t st) {
+    CUDA_OK(cudaFuncSetAttribute(k_beta<Real, SMC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_beta<Real, SMC><<<blocks, threads, smem, st>>>(B, out);
+}
+
+template <class Real>
+static void launch_beta(int SM, const BetaArgs& B, Real* out, size_t smem, unsigned blocks, int threads,
+                        cudaStream_t st) {
+    switch (SM) {
+        case 1: launch_beta_smc<Real, 1>(B, out, smem, blocks, threads, st); break;
+        case 2: launch_beta_smc<Real, 2>(B, out, smem, blocks, threads, st); break;
+        case 3: launch_beta_smc<Real, 3>(B, out, smem, blocks, threads, st); break;
+        case 4: launch_beta_smc<Real, 4>(B, out, smem, blocks, threads, st); break;
+        case 5: launch_beta_smc<Real, 5>(B, out, smem, blocks, threads, st); break;
+        case 6: launch_beta_smc<Real, 6>(B, out, smem, blocks, threads, st); break;
+        case 7: launch_beta_smc<Real, 7>(B, out, smem, blocks, threads, st); break;
+        case 8: launch_beta_smc<Real, 8>(B, out, smem, blocks, threads, st); break;
+        default: throw Error{"at most 8 (set, term) pairs in the factored kernels"};
     }
 }
 
@@ -707,9 +728,8 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         int warps = (int)std::min<size_t>(8, (200 * 1024) / pw);
         if (warps < 1) throw Error{"n_phi too large for the beta kernel"};
         const size_t smem = (size_t)warps * pw;
-        CUDA_OK(cudaFuncSetAttribute(k_beta<Real>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
         const unsigned blocks = (unsigned)((B.n_rows + warps - 1) / warps);
-        k_beta<Real><<<blocks, warps * 32, smem, dev->stream>>>(B, (Real*)dev->beta.p);
+        launch_beta<Real>(SM, B, (Real*)dev->beta.p, smem, blocks, warps * 32, dev->stream);
         CUDA_OK(cudaGetLastError());
         ++launches;
     }
