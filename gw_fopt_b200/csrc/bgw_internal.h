@@ -79,6 +79,12 @@ void device_destroy(Device*);
 // Throws Error.
 void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_device, BgwxTimings* timings);
 
+// Runs one job per realization back to back on the handle's stream (largest
+// first, so the grow-only work arrays are sized once) into one device array
+// and copies it out once; out: (R, n_k, 2, n_sets, n_w) complex as
+// interleaved doubles.  Jobs with no radiating bubble yield zeros.
+void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out, BgwxTimings* timings);
+
 // Uses `stream` (a cudaStream_t) for all later work; nullptr = own stream.
 void device_set_stream(Device* dev, void* stream);
 

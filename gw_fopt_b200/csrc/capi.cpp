@@ -145,6 +145,49 @@ Cutoff make_cutoff(const BgwTimeCutoffConfig& c) {
     return k;
 }
 
+// The parts of a spectrum job that come from the handle's settings and the
+// call's grids (everything except the bubbles and the radiating selection).
+bgw::SpectrumJob settings_job(const bgw_generalized_bulk_flow* h, const std::vector<double>& t_arr,
+                              const std::vector<double>& cw, const double* w, size_t n_w, const double* rot,
+                              size_t n_k) {
+    bgw::SpectrumJob job;
+    job.n_cos = h->n_cos;
+    job.n_phi = h->n_phi;
+    job.cos_thetax = h->cos_thetax.data();
+    job.dirs = h->dirs.data();
+    job.sin2phi = h->sin2phi.data();
+    job.cos2phi = h->cos2phi.data();
+    job.n_sets = h->n_sets;
+    job.n_terms = h->n_terms;
+    job.coeffs = h->coeffs.data();
+    job.powers = h->powers.data();
+    job.has_damping = h->has_damping;
+    job.damping = h->damping;
+    job.n_t = t_arr.size();
+    job.t_arr = t_arr.data();
+    job.cutoff = cw.data();
+    job.dt = t_arr[1] - t_arr[0];
+    job.n_w = n_w;
+    job.w = w;
+    job.rot = rot;
+    job.n_k = n_k;
+    job.kernel = h->kernel;
+    return job;
+}
+
+// Rotations R(k) of the (n_khat, 3) unit rows.
+std::vector<double> khat_rotations(const double* khat, size_t n_khat) {
+    const double* k = slice(khat, checked_mul(n_khat, 3, "khat"), "khat");
+    std::vector<double> rot(9 * n_khat);
+    for (size_t q = 0; q < n_khat; ++q) {
+        double kx = k[3 * q], ky = k[3 * q + 1], kz = k[3 * q + 2];
+        double n2 = kx * kx + ky * ky + kz * kz;
+        if (!(std::fabs(n2 - 1.0) <= 1e-9)) throw Error{"khat rows must be unit vectors"};
+        bgw::rotation_for_khat(kx, ky, kz, &rot[9 * q]);
+    }
+    return rot;
+}
+
 // Shared body of compute_c_integral (generalized_bulk_flow.rs:928-984) for
 // n_k frames; rot == nullptr means the unrotated frame.
 void compute_common(bgw_generalized_bulk_flow* h, const double* w_arr, size_t n_w, bool has_t_begin, double t_begin,
@@ -185,33 +228,12 @@ void compute_common(bgw_generalized_bulk_flow* h, const double* w_arr, size_t n_
             std::vector<double> t_arr = bgw::linspace(tb, t_end, n_t);
             std::vector<double> cw(n_t);
             for (size_t k = 0; k < n_t; ++k) cw[k] = cut.eval(t_arr[k]);
-            bgw::SpectrumJob job;
+            bgw::SpectrumJob job = settings_job(h, t_arr, cw, w, n_w, rot, n_k);
             job.bubbles = h->bubbles.data();
             job.n_int = h->n_int;
             job.n_tot = h->n_int + h->n_ext;
-            job.n_cos = h->n_cos;
-            job.n_phi = h->n_phi;
-            job.cos_thetax = h->cos_thetax.data();
-            job.dirs = h->dirs.data();
-            job.sin2phi = h->sin2phi.data();
-            job.cos2phi = h->cos2phi.data();
-            job.n_sets = S;
-            job.n_terms = h->n_terms;
-            job.coeffs = h->coeffs.data();
-            job.powers = h->powers.data();
-            job.has_damping = h->has_damping;
-            job.damping = h->damping;
-            job.n_t = n_t;
-            job.t_arr = t_arr.data();
-            job.cutoff = cw.data();
-            job.dt = t_arr[1] - t_arr[0];
-            job.n_w = n_w;
-            job.w = w;
             job.sel = ids.data();
             job.n_sel = ids.size();
-            job.rot = rot;
-            job.n_k = n_k;
-            job.kernel = h->kernel;
             if (out_device) {
                 bgw::run_spectrum(device(h), job, static_cast<double*>(out_device), true, &h->timings);
                 device_written = true;
@@ -351,14 +373,7 @@ BgwStatus bgwx_generalized_bulk_flow_compute_c_integral_khat(bgw_generalized_bul
                                                              size_t out_len) {
     return run_ffi([&] {
         auto* h = handle(bulk_flow);
-        const double* k = slice(khat, checked_mul(n_khat, 3, "khat"), "khat");
-        std::vector<double> rot(9 * n_khat);
-        for (size_t q = 0; q < n_khat; ++q) {
-            double kx = k[3 * q], ky = k[3 * q + 1], kz = k[3 * q + 2];
-            double n2 = kx * kx + ky * ky + kz * kz;
-            if (!(std::fabs(n2 - 1.0) <= 1e-9)) throw Error{"khat rows must be unit vectors"};
-            bgw::rotation_for_khat(kx, ky, kz, &rot[9 * q]);
-        }
+        std::vector<double> rot = khat_rotations(khat, n_khat);
         if (n_khat == 0) {
             if (out_len != 0)
                 throw Error{"out_len=" + std::to_string(out_len) + " does not match expected length 0"};
@@ -376,17 +391,73 @@ BgwStatus bgwx_generalized_bulk_flow_compute_c_integral_khat_device(
     return run_ffi([&] {
         auto* h = handle(bulk_flow);
         if (!out_device) throw Error{"out_device must not be null"};
-        const double* k = slice(khat, checked_mul(n_khat, 3, "khat"), "khat");
         if (n_khat == 0) throw Error{"khat must hold at least one direction"};
-        std::vector<double> rot(9 * n_khat);
-        for (size_t q = 0; q < n_khat; ++q) {
-            double kx = k[3 * q], ky = k[3 * q + 1], kz = k[3 * q + 2];
-            double n2 = kx * kx + ky * ky + kz * kz;
-            if (!(std::fabs(n2 - 1.0) <= 1e-9)) throw Error{"khat rows must be unit vectors"};
-            bgw::rotation_for_khat(kx, ky, kz, &rot[9 * q]);
-        }
+        std::vector<double> rot = khat_rotations(khat, n_khat);
         compute_common(h, w_arr, n_w, has_t_begin, t_begin, t_end, n_t, selected_bubbles, n_selected_bubbles,
                        selected_bubbles != nullptr, time_cutoff, rot.data(), n_khat, nullptr, out_len, out_device);
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_compute_ensemble_khat(
+    bgw_generalized_bulk_flow* bulk_flow, const double* interior, const size_t* interior_offsets,
+    const double* exterior, const size_t* exterior_offsets, size_t n_realizations, bool validate,
+    const double* w_arr, size_t n_w, bool has_t_begin, double t_begin, double t_end, size_t n_t,
+    const double* khat, size_t n_khat, BgwTimeCutoffConfig time_cutoff, BgwComplex64* out, size_t out_len) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        const size_t R = n_realizations;
+        const size_t S = h->n_sets;
+        const size_t per_r = checked_mul(checked_mul(checked_mul(n_khat, 2, "out"), S, "out"), n_w, "out");
+        const size_t expected = checked_mul(R, per_r, "out");
+        if (out_len != expected)
+            throw Error{"out_len=" + std::to_string(out_len) + " does not match expected length " +
+                        std::to_string(expected)};
+        if (expected == 0) return;
+        const size_t* io = slice(interior_offsets, R + 1, "interior_offsets");
+        const size_t* eo = slice(exterior_offsets, R + 1, "exterior_offsets");
+        if (io[0] != 0 || eo[0] != 0) throw Error{"offsets must start at 0"};
+        for (size_t r = 0; r < R; ++r)
+            if (io[r + 1] < io[r] || eo[r + 1] < eo[r]) throw Error{"offsets must be non-decreasing"};
+        const double* pi = slice(interior, checked_mul(io[R], 4, "interior bubbles"), "interior");
+        const double* pe = slice(exterior, checked_mul(eo[R], 4, "exterior bubbles"), "exterior");
+        if (n_t < 2) throw Error{"Invalid resolution: n_t must be >= 2 for integration"};
+        const double tb = has_t_begin ? t_begin : 0.0;
+        if (tb > t_end)
+            throw Error{"Invalid time range: t_begin=" + bgw::rust_f64(tb) + " > t_end=" + bgw::rust_f64(t_end)};
+        require_resolution(h);
+        std::vector<double> rot = khat_rotations(khat, n_khat);
+        const double* w = slice(w_arr, n_w, "w_arr");
+        Cutoff cut = make_cutoff(time_cutoff);
+        std::vector<double> t_arr = bgw::linspace(tb, t_end, n_t);
+        std::vector<double> cw(n_t);
+        for (size_t k = 0; k < n_t; ++k) cw[k] = cut.eval(t_arr[k]);
+        // per realization: interior rows then exterior rows, as a handle holds them
+        std::vector<std::vector<double>> bubbles(R);
+        std::vector<std::vector<uint32_t>> ids(R);
+        std::vector<bgw::SpectrumJob> jobs(R);
+        for (size_t r = 0; r < R; ++r) {
+            const size_t ni = io[r + 1] - io[r], ne = eo[r + 1] - eo[r];
+            const double* ri = pi ? pi + 4 * io[r] : nullptr;
+            const double* re = pe ? pe + 4 * eo[r] : nullptr;
+            if (validate) bgw::check_causality(ri, ni, re, ne);
+            if (ni > 0xffffffffULL) throw Error{"too many interior bubbles in one realization"};
+            bubbles[r].resize(4 * (ni + ne));
+            if (ni) std::memcpy(bubbles[r].data(), ri, 4 * ni * sizeof(double));
+            if (ne) std::memcpy(bubbles[r].data() + 4 * ni, re, 4 * ne * sizeof(double));
+            ids[r].resize(ni);
+            for (size_t a = 0; a < ni; ++a) ids[r][a] = (uint32_t)a;
+            jobs[r] = settings_job(h, t_arr, cw, w, n_w, rot.data(), n_khat);
+            jobs[r].bubbles = bubbles[r].data();
+            jobs[r].n_int = ni;
+            jobs[r].n_tot = ni + ne;
+            jobs[r].sel = ids[r].data();
+            jobs[r].n_sel = ni;
+        }
+        h->timings = BgwxTimings{};
+        std::vector<double> result(2 * expected, 0.0);
+        bgw::run_ensemble(device(h), jobs, result.data(), &h->timings);
+        BgwComplex64* o = const_cast<BgwComplex64*>(slice(out, out_len, "out"));
+        for (size_t q = 0; q < expected; ++q) o[q] = BgwComplex64{result[2 * q], result[2 * q + 1]};
     });
 }
 

@@ -77,6 +77,7 @@ struct Device {
     DevBuf bub, bubrot, dirs, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, sel, rot;
     DevBuf tau, codes, partial, out, counters, nblists;
     DevBuf fact_D, fact_kfirst, beta, fact_partial;  // factored-kernel work arrays
+    DevBuf ens_out;                                  // batched ensemble: all realizations' spectra
     ~Device();
 };
 

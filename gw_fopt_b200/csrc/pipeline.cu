@@ -543,4 +543,37 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     }
 }
 
+void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out, BgwxTimings* tm) {
+    CUDA_OK(cudaSetDevice(dev->id));
+    const size_t R = jobs.size();
+    if (R == 0) return;
+    const size_t per_r = jobs[0].n_k * 2 * jobs[0].n_sets * jobs[0].n_w;  // complex values per realization
+    dev->ens_out.ensure(R * per_r * sizeof(double2));
+    double2* eo = (double2*)dev->ens_out.p;
+    CUDA_OK(cudaMemsetAsync(eo, 0, R * per_r * sizeof(double2), dev->stream));
+    std::vector<size_t> order(R);
+    for (size_t r = 0; r < R; ++r) order[r] = r;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
+        return jobs[a].n_sel * jobs[a].n_tot > jobs[b].n_sel * jobs[b].n_tot;
+    });
+    BgwxTimings local{};
+    CUDA_OK(cudaEventRecord(dev->ev[6], dev->stream));
+    for (size_t r : order) {
+        if (jobs[r].n_sel == 0) continue;
+        run_spectrum(dev, jobs[r], reinterpret_cast<double*>(eo + r * per_r), true, &local);
+    }
+    CUDA_OK(cudaEventRecord(dev->ev[7], dev->stream));
+    CUDA_OK(cudaMemcpyAsync(out, eo, R * per_r * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
+    CUDA_OK(cudaStreamSynchronize(dev->stream));
+    float total = 0;
+    CUDA_OK(cudaEventElapsedTime(&total, dev->ev[6], dev->ev[7]));
+    if (tm) {
+        tm->total_ms += total;
+        tm->launches += local.launches;
+        tm->h2d_bytes += local.h2d_bytes;
+        tm->d2h_bytes += (double)(R * per_r * sizeof(double2));
+        for (const auto& j : jobs) tm->directions += j.n_k * j.n_sel * j.n_cos * j.n_phi;
+    }
+}
+
 }  // namespace bgw

@@ -1,10 +1,14 @@
 """One spectrum call of a synthetic workload, for profiling (ncu) and timing.
 
     python -m gw_fopt_b200.profile_case --config 3 --kernel mixed --khat 1 --bubbles 512 [--reps 1]
+    python -m gw_fopt_b200.profile_case --config 4 --kernel mixed --khat 64 --realizations 256 [--compare 4]
 
 --bubbles restricts the radiating bubbles to the first B (all colliders stay
 present), which keeps a profiler capture small while the per-bubble work and
-the collision geometry are those of the full configuration.
+the collision geometry are those of the full configuration.  Config 4 is the
+batched ensemble; --realizations takes the first R of its 256 realizations and
+--compare C also runs the first C realizations with the FP64 factored kernel
+and reports the mixed kernel's error against it.
 """
 from __future__ import annotations
 
@@ -25,7 +29,11 @@ def main():
     ap.add_argument("--khat", type=int, default=1)
     ap.add_argument("--bubbles", type=int, default=0)
     ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--realizations", type=int, default=256)
+    ap.add_argument("--compare", type=int, default=0)
     a = ap.parse_args()
+    if a.config == 4:
+        return run_ensemble(a)
     c = W.config(a.config, k_subset=a.khat)
     g = mb.GeneralizedBulkFlow(mb.LatticeBubbles(mb.EmptyLattice(), c.interior, c.exterior))
     g.set_resolution(c.n_cos, c.n_phi)
@@ -44,6 +52,51 @@ def main():
                           "radiating": int(n_rad), "wall_s": wall, "masks_ms": t["masks_ms"],
                           "spectrum_ms": t["spectrum_ms"], "total_ms": t["total_ms"], "fallbacks": t["fallbacks"],
                           "pte_per_s": pte / (t["total_ms"] * 1e-3), "checksum": float(np.abs(out).sum())}))
+
+
+def run_ensemble(a):
+    from .ensemble import BulkFlowEnsemble
+    t0 = time.perf_counter()
+    c = W.ensemble_config(k_subset=a.khat)
+    c.realizations = c.realizations[:a.realizations]
+    gen_s = time.perf_counter() - t0
+
+    def make(kernel, reals):
+        e = BulkFlowEnsemble(reals, validate=False)
+        e.set_resolution(c.n_cos, c.n_phi)
+        e.set_gradient_scaling_params(c.coefficients.tolist(), c.powers.tolist())
+        e.set_kernel(kernel)
+        return e
+
+    ens = make(a.kernel, c.realizations)
+    pte = c.pte
+    for r in range(a.reps):
+        t0 = time.perf_counter()
+        out = ens.compute_c_integral_khat(c.w, c.khat, t_begin=c.t_begin, t_end=c.t_end, n_t=c.n_t)
+        wall = time.perf_counter() - t0
+        t = ens.last_timings()
+        rec = {"rep": r, "config": c.name, "kernel": a.kernel, "realizations": len(c.realizations),
+               "khat": int(c.khat.shape[0]), "bubbles": c.n_total, "generate_s": gen_s, "wall_s": wall,
+               "total_ms": t["total_ms"], "launches": t["launches"], "pte": pte,
+               "pte_per_s": pte / (t["total_ms"] * 1e-3), "checksum": float(np.abs(out).sum())}
+        if a.compare and r == 0:
+            n = min(a.compare, len(c.realizations))
+            ref = make("fp64_factored", c.realizations[:n]).compute_c_integral_khat(
+                c.w, c.khat, t_begin=c.t_begin, t_end=c.t_end, n_t=c.n_t)
+            errs = []
+            for q in range(n):
+                g = out[q].reshape(-1, c.w.size)
+                f = ref[q].reshape(-1, c.w.size)
+                num = np.linalg.norm(g - f, axis=0)
+                errs.append((float(np.linalg.norm(g - f) / np.linalg.norm(f)),
+                             float(num.max() / np.linalg.norm(f, axis=0).max())))
+            rec["compare_realizations"] = n
+            rec["err_global_max"] = max(e[0] for e in errs)
+            rec["err_peak_scaled_max"] = max(e[1] for e in errs)
+            pm = np.mean(np.abs(out[:n]) ** 2, axis=0)
+            pr = np.mean(np.abs(ref) ** 2, axis=0)
+            rec["err_mean_power"] = float(np.linalg.norm(pm - pr) / np.linalg.norm(pr))
+        print(json.dumps(rec))
 
 
 if __name__ == "__main__":

@@ -74,6 +74,7 @@ def exponential_nucleation(n: int, beta: float, L: float = 1.0, seed: int = 2, g
     rng = np.random.default_rng(seed)
     V = L ** 3
     g0 = gamma_scale * n * beta / V  # Gamma0 V / beta = n * gamma_scale
+    block = 256
     while True:
         pos = np.empty((n, 3))
         tn = np.empty(n)
@@ -81,21 +82,52 @@ def exponential_nucleation(n: int, beta: float, L: float = 1.0, seed: int = 2, g
         t = 0.0
         rejections = 0
         while k < n and rejections < max_rejections:
-            # next arrival of a Poisson process with rate g0 V e^{beta t}
-            u = rng.random()
-            t = math.log(math.exp(beta * t) - beta * math.log(u) / (g0 * V)) / beta
-            x = rng.uniform(0.0, L, 3)
+            # A block of candidates, drawn from the stream in the order of one
+            # candidate at a time (u, then the three coordinates).  The arrival
+            # times do not depend on acceptance, so the block is tested against
+            # the bubbles accepted before it at once, and candidate by candidate
+            # against those accepted inside it: the outcome is that of testing
+            # one candidate at a time.
+            state = rng.bit_generator.state
+            r = rng.random((block, 4))
+            tc = np.empty(block)
+            for q in range(block):
+                # next arrival of a Poisson process with rate g0 V e^{beta t}
+                t = math.log(math.exp(beta * t) - beta * math.log(r[q, 0]) / (g0 * V)) / beta
+                tc[q] = t
+            xc = 0.0 + (L - 0.0) * r[:, 1:4]
             if k:
-                d = np.abs(pos[:k] - x)
+                d = np.abs(xc[:, None, :] - pos[None, :k, :])
                 d = np.minimum(d, L - d)  # minimum image = nearest periodic copy
-                r2 = np.einsum("ij,ij->i", d, d)
-                rad = t - tn[:k]
-                if np.any(r2 < rad * rad):
+                r2 = np.einsum("bij,bij->bi", d, d)
+                rad = tc[:, None] - tn[None, :k]
+                hit = np.any(r2 < rad * rad, axis=1)
+            else:
+                hit = np.zeros(block, dtype=bool)
+            k0 = k
+            used = 0
+            for q in range(block):
+                if k >= n or rejections >= max_rejections:
+                    break
+                used += 1
+                x = xc[q]
+                if hit[q]:
                     rejections += 1
                     continue
-            pos[k] = x
-            tn[k] = t
-            k += 1
+                if k > k0:
+                    d = np.abs(pos[k0:k] - x)
+                    d = np.minimum(d, L - d)
+                    r2 = np.einsum("ij,ij->i", d, d)
+                    rad = tc[q] - tn[k0:k]
+                    if np.any(r2 < rad * rad):
+                        rejections += 1
+                        continue
+                pos[k] = x
+                tn[k] = tc[q]
+                k += 1
+            if used < block:  # leave the stream where a one-at-a-time draw would have left it
+                rng.bit_generator.state = state
+                rng.random((used, 4))
         if k == n:
             break
         g0 *= 2.0
@@ -180,10 +212,61 @@ def config(idx: int, k_subset: int | None = None) -> SpectrumConfig:
 
 
 def ensemble(n_real: int = 256, seed: int = 4, n_min: int = 50, n_max: int = 800, beta_lo: float = 5.0,
-             beta_hi: float = 15.0):
-    """Realizations for the batched ensemble: N_r ~ U{n_min..n_max}, beta_r ~ U[beta_lo, beta_hi]."""
+             beta_hi: float = 15.0, max_rejections: int = 20000):
+    """Realizations for the batched ensemble: N_r ~ U{n_min..n_max}, beta_r ~ U[beta_lo, beta_hi].
+
+    At small beta L a box holds few bubbles before the false vacuum runs out, so
+    placing hundreds needs a larger rate prefactor; the lower rejection limit
+    makes the sampler move on to the doubled prefactor sooner."""
     rng = np.random.default_rng(seed)
     ns = rng.integers(n_min, n_max + 1, n_real)
     betas = rng.uniform(beta_lo, beta_hi, n_real)
     seeds = rng.integers(0, 2 ** 31 - 1, n_real)
-    return [exponential_nucleation(int(n), float(bt), seed=int(s)) for n, bt, s in zip(ns, betas, seeds)]
+    return [exponential_nucleation(int(n), float(bt), seed=int(s), max_rejections=max_rejections)
+            for n, bt, s in zip(ns, betas, seeds)]
+
+
+@dataclass
+class EnsembleConfig:
+    """The batched-ensemble workload: realizations plus the grids they share."""
+    name: str
+    realizations: list
+    n_cos: int
+    n_phi: int
+    n_t: int
+    t_begin: float
+    t_end: float
+    w: np.ndarray
+    khat: np.ndarray
+    coefficients: np.ndarray = field(default_factory=lambda: np.array([[1.0]]))
+    powers: np.ndarray = field(default_factory=lambda: np.array([[5.0]]))
+
+    @property
+    def n_total(self) -> int:
+        return int(sum(r[0].shape[0] for r in self.realizations))
+
+    @property
+    def pte(self) -> int:
+        return self.khat.shape[0] * self.n_total * self.n_cos * self.n_phi * self.n_t
+
+    @property
+    def phase_terms(self) -> int:
+        return self.khat.shape[0] * self.n_total * self.n_cos * self.n_t * self.w.size
+
+    @property
+    def phase_terms_t(self) -> int:
+        return self.khat.shape[0] * self.n_total * self.n_t * self.w.size
+
+    @property
+    def counted_flops(self) -> float:
+        return 6.0 * self.pte + 8.0 * self.phase_terms + 20.0 * self.phase_terms_t
+
+
+def ensemble_config(n_real: int = 256, k_subset: int | None = None) -> EnsembleConfig:
+    """Batched ensemble: 256 realizations, N_r ~ U{50..800}, beta_r L ~ U[5, 15] (seed 4), periodic;
+    96x96 patches, 384 time steps on [0, 1.5], 128 w geomspace [1, 3000], 64 Fibonacci k-hat."""
+    c = EnsembleConfig(f"ensemble-{n_real}r-96x96-T384-W128-K64", ensemble(n_real), 96, 96, 384, 0.0, 1.5,
+                       np.geomspace(1.0, 3000.0, 128), fibonacci_khat(64))
+    if k_subset is not None:
+        c.khat = c.khat[:k_subset]
+    return c

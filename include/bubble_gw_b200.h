@@ -128,6 +128,28 @@ BgwStatus bgwx_generalized_bulk_flow_compute_c_integral_khat_device(
     double t_end, size_t n_t, const double *khat, size_t n_khat, const size_t *selected_bubbles,
     size_t n_selected_bubbles, BgwTimeCutoffConfig time_cutoff, void *out_device, size_t out_len);
 
+/* Batched ensemble: the spectra of R independent nucleation realizations in
+ * one call, each along the same K directions k-hat.  Realization r's bubbles
+ * are rows interior_offsets[r] .. interior_offsets[r+1]-1 of `interior` and
+ * rows exterior_offsets[r] .. exterior_offsets[r+1]-1 of `exterior` (both
+ * (n, 4) row-major (t, x, y, z); offsets have R+1 non-decreasing entries
+ * starting at 0).  Every interior bubble of a realization radiates.  The
+ * resolution, gradient scaling parameters and kernel come from `bulk_flow`
+ * (its own bubbles are not used).  With `validate` each realization passes
+ * the causality check of bgw_generalized_bulk_flow_empty_lattice_new.
+ * out: (R, K, 2, n_sets, n_w); out_len = R*K*2*n_sets*n_w.  Block r equals
+ * bgwx_generalized_bulk_flow_compute_c_integral_khat on a handle holding
+ * realization r, bit for bit.  Replaces a caller's loop that builds one
+ * GeneralizedBulkFlow per realization and calls compute_c_integral on each
+ * (generalized_bulk_flow.rs:928-984, used as in
+ * docs/examples/generalized_bulkflow.py:679-703).  No counterpart in the
+ * reference's C ABI. */
+BgwStatus bgwx_generalized_bulk_flow_compute_ensemble_khat(
+    bgw_generalized_bulk_flow *bulk_flow, const double *interior, const size_t *interior_offsets,
+    const double *exterior, const size_t *exterior_offsets, size_t n_realizations, bool validate,
+    const double *w_arr, size_t n_w, bool has_t_begin, double t_begin, double t_end, size_t n_t,
+    const double *khat, size_t n_khat, BgwTimeCutoffConfig time_cutoff, BgwComplex64 *out, size_t out_len);
+
 /* Runs this handle's device work on `stream` (a cudaStream_t created by the
  * caller; NULL selects the handle's own non-blocking stream, so the legacy
  * default stream cannot be chosen).  No counterpart in the reference. */
