@@ -85,6 +85,13 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
 // interleaved doubles.  Jobs with no radiating bubble yield zeros.
 void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out, BgwxTimings* timings);
 
+// Vector-Jacobian product of the spectrum: gbar (n_k, 2, n_sets, n_w)
+// complex cotangents dL/dRe C + i dL/dIm C (interleaved doubles) ->
+// g_par (coefficients then powers, 2 n_sets n_terms) and g_bub ((n_tot, 4),
+// gradients with respect to every bubble row, exterior rows included).
+void run_adjoint(Device* dev, const SpectrumJob& job, const double* gbar, double* g_par, double* g_bub,
+                 BgwxTimings* timings);
+
 // Uses `stream` (a cudaStream_t) for all later work; nullptr = own stream.
 void device_set_stream(Device* dev, void* stream);
 

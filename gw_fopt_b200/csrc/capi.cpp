@@ -4,6 +4,7 @@
 // fallback: without a usable CUDA device the compute calls fail with
 // BGW_STATUS_CALCULATION_ERROR.
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <exception>
@@ -458,6 +459,80 @@ BgwStatus bgwx_generalized_bulk_flow_compute_ensemble_khat(
         bgw::run_ensemble(device(h), jobs, result.data(), &h->timings);
         BgwComplex64* o = const_cast<BgwComplex64*>(slice(out, out_len, "out"));
         for (size_t q = 0; q < expected; ++q) o[q] = BgwComplex64{result[2 * q], result[2 * q + 1]};
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_spectrum_vjp(bgw_generalized_bulk_flow* bulk_flow, const double* w_arr,
+                                                  size_t n_w, bool has_t_begin, double t_begin, double t_end,
+                                                  size_t n_t, const double* khat, size_t n_khat,
+                                                  BgwTimeCutoffConfig time_cutoff, const BgwComplex64* grad_out,
+                                                  size_t grad_len, double* grad_coefficients, double* grad_powers,
+                                                  double* grad_bubbles) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        const size_t S = h->n_sets, M = h->n_terms, SM = S * M;
+        const size_t K = n_khat ? n_khat : 1;
+        const size_t expected = checked_mul(checked_mul(checked_mul(K, 2, "grad_out"), S, "grad_out"), n_w,
+                                            "grad_out");
+        if (grad_len != expected)
+            throw Error{"grad_len=" + std::to_string(grad_len) + " does not match expected length " +
+                        std::to_string(expected)};
+        const size_t n_tot = h->n_int + h->n_ext;
+        double* gc = const_cast<double*>(slice<double>(grad_coefficients, SM, "grad_coefficients"));
+        double* gp = const_cast<double*>(slice<double>(grad_powers, SM, "grad_powers"));
+        double* gb = const_cast<double*>(slice<double>(grad_bubbles, checked_mul(n_tot, 4, "grad_bubbles"),
+                                                       "grad_bubbles"));
+        if (SM) std::fill(gc, gc + SM, 0.0), std::fill(gp, gp + SM, 0.0);
+        if (n_tot) std::fill(gb, gb + 4 * n_tot, 0.0);
+        if (n_t < 2) throw Error{"Invalid resolution: n_t must be >= 2 for integration"};
+        const double tb = has_t_begin ? t_begin : 0.0;
+        if (tb > t_end)
+            throw Error{"Invalid time range: t_begin=" + bgw::rust_f64(tb) + " > t_end=" + bgw::rust_f64(t_end)};
+        require_resolution(h);
+        if (expected == 0 || h->n_int == 0) return;
+        const BgwComplex64* g = slice(grad_out, grad_len, "grad_out");
+        std::vector<double> rot = khat_rotations(khat, n_khat);
+        const double* w = slice(w_arr, n_w, "w_arr");
+        Cutoff cut = make_cutoff(time_cutoff);
+        std::vector<double> t_arr = bgw::linspace(tb, t_end, n_t);
+        std::vector<double> cw(n_t);
+        for (size_t k = 0; k < n_t; ++k) cw[k] = cut.eval(t_arr[k]);
+        std::vector<uint32_t> ids(h->n_int);
+        for (size_t a = 0; a < h->n_int; ++a) ids[a] = (uint32_t)a;
+        bgw::SpectrumJob job = settings_job(h, t_arr, cw, w, n_w, n_khat ? rot.data() : nullptr, K);
+        job.bubbles = h->bubbles.data();
+        job.n_int = h->n_int;
+        job.n_tot = n_tot;
+        job.sel = ids.data();
+        job.n_sel = ids.size();
+        std::vector<double> gbar(2 * expected);
+        for (size_t q = 0; q < expected; ++q) {
+            gbar[2 * q] = g[q].re;
+            gbar[2 * q + 1] = g[q].im;
+        }
+        std::vector<double> gpar(2 * SM);
+        h->timings = BgwxTimings{};
+        bgw::run_adjoint(device(h), job, gbar.data(), gpar.data(), gb, &h->timings);
+        for (size_t q = 0; q < SM; ++q) {
+            gc[q] = gpar[q];
+            gp[q] = gpar[SM + q];
+        }
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_set_bubbles(bgw_generalized_bulk_flow* bulk_flow, const double* interior,
+                                                 size_t n_interior, const double* exterior, size_t n_exterior) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        size_t li = checked_mul(n_interior, 4, "interior bubbles");
+        size_t le = checked_mul(n_exterior, 4, "exterior bubbles");
+        const double* pi = slice(interior, li, "bubbles_interior");
+        const double* pe = slice(exterior, le, "bubbles_exterior");
+        h->bubbles.resize(li + le);
+        if (li) std::memcpy(h->bubbles.data(), pi, li * sizeof(double));
+        if (le) std::memcpy(h->bubbles.data() + li, pe, le * sizeof(double));
+        h->n_int = n_interior;
+        h->n_ext = n_exterior;
     });
 }
 

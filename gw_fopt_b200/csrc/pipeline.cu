@@ -23,6 +23,7 @@
 #include "device_common.cuh"
 #include "masks.cuh"
 #include "spectrum_factored.cuh"
+#include "adjoint.cuh"
 
 namespace bgw {
 
@@ -573,6 +574,81 @@ void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out
         tm->h2d_bytes += local.h2d_bytes;
         tm->d2h_bytes += (double)(R * per_r * sizeof(double2));
         for (const auto& j : jobs) tm->directions += j.n_k * j.n_sel * j.n_cos * j.n_phi;
+    }
+}
+
+void run_adjoint(Device* dev, const SpectrumJob& job, const double* gbar, double* g_par, double* g_bub,
+                 BgwxTimings* tm) {
+    CUDA_OK(cudaSetDevice(dev->id));
+    const size_t nd = job.n_cos * job.n_phi;
+    const size_t S = job.n_sets, W = job.n_w, K = job.n_k;
+    const size_t per = 2 * S * W;
+    const size_t SM = S * job.n_terms;
+    if (job.n_t > (size_t)0x7fffffff || W > (size_t)0x7fffffff) throw Error{"n_t or n_w too large"};
+    D4* bub = reinterpret_cast<D4*>(upload(dev, dev->bub, job.bubbles, 4 * job.n_tot, tm));
+    D4* dirs = reinterpret_cast<D4*>(upload(dev, dev->dirs, job.dirs, 4 * nd, tm));
+    double* cos_t = upload(dev, dev->cos_t, job.cos_thetax, job.n_cos, tm);
+    double* sin2 = upload(dev, dev->sin2, job.sin2phi, job.n_phi, tm);
+    double* cos2 = upload(dev, dev->cos2, job.cos2phi, job.n_phi, tm);
+    double* coeffs = upload(dev, dev->coeffs, job.coeffs, SM, tm);
+    double* powers = upload(dev, dev->powers, job.powers, SM, tm);
+    double* t_arr = upload(dev, dev->t_arr, job.t_arr, job.n_t, tm);
+    double* cutw = upload(dev, dev->cutw, job.cutoff, job.n_t, tm);
+    double* w = upload(dev, dev->w, job.w, W, tm);
+    uint32_t* sel = upload(dev, dev->sel, job.sel, job.n_sel, tm);
+    double* rot = job.rot ? upload(dev, dev->rot, job.rot, 9 * K, tm) : nullptr;
+    double2* gb = reinterpret_cast<double2*>(upload(dev, dev->adj_gbar, gbar, 2 * K * per, tm));
+
+    const size_t per_k = adjoint_bytes_per_frame(job);
+    size_t kc = std::max<size_t>(1, std::min(K, mask_budget_bytes() / std::max<size_t>(per_k, 1)));
+    kc = std::min<size_t>(kc, 65535);
+    const size_t rows = job.n_sel * job.n_cos;
+    dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
+    dev->codes.ensure(kc * job.n_sel * nd * sizeof(int32_t));
+    dev->adj_scratch.ensure(kc * (2 * rows * job.n_t * 2 * S + job.n_sel * nd + rows * (2 + 2 * SM)) *
+                            sizeof(double));
+    AdjointScratch sc;
+    sc.bbar = (double*)dev->adj_scratch.p;
+    sc.imq = sc.bbar + kc * rows * job.n_t * 2 * S;
+    sc.taubar = sc.imq + kc * rows * job.n_t * 2 * S;
+    sc.rowpart = sc.taubar + kc * job.n_sel * nd;
+    dev->adj_grad.ensure((4 * job.n_tot + 2 * SM) * sizeof(double));
+    double* d_gbub = (double*)dev->adj_grad.p;
+    double* d_gpar = d_gbub + 4 * job.n_tot;
+    CUDA_OK(cudaMemsetAsync(d_gbub, 0, (4 * job.n_tot + 2 * SM) * sizeof(double), dev->stream));
+    if (rot) dev->bubrot.ensure(kc * job.n_tot * sizeof(D4));
+    dev->counters.ensure(64);
+    CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
+
+    uint64_t launches = 0;
+    CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
+    for (size_t k0 = 0; k0 < K; k0 += kc) {
+        const size_t kn = std::min(kc, K - k0);
+        const D4* fb = bub;
+        if (rot) {
+            dim3 g((unsigned)((job.n_tot + 255) / 256), (unsigned)kn);
+            k_rotate<<<g, 256, 0, dev->stream>>>(bub, rot + 9 * k0, job.n_tot, (D4*)dev->bubrot.p);
+            CUDA_OK(cudaGetLastError());
+            ++launches;
+            fb = (const D4*)dev->bubrot.p;
+        }
+        launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, kn, (double*)dev->tau.p,
+                             (int32_t*)dev->codes.p, (unsigned long long*)dev->counters.p, k0 == 0, &launches);
+        launches += launch_adjoint_chunk(dev, job, fb, sel, (const double*)dev->tau.p, (const int32_t*)dev->codes.p,
+                                         dirs, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w,
+                                         rot ? rot + 9 * k0 : nullptr, gb + k0 * per, kn, sc, d_gbub, d_gpar);
+    }
+    CUDA_OK(cudaEventRecord(dev->ev[5], dev->stream));
+    CUDA_OK(cudaMemcpyAsync(g_bub, d_gbub, 4 * job.n_tot * sizeof(double), cudaMemcpyDeviceToHost, dev->stream));
+    CUDA_OK(cudaMemcpyAsync(g_par, d_gpar, 2 * SM * sizeof(double), cudaMemcpyDeviceToHost, dev->stream));
+    CUDA_OK(cudaStreamSynchronize(dev->stream));
+    float total = 0;
+    CUDA_OK(cudaEventElapsedTime(&total, dev->ev[4], dev->ev[5]));
+    if (tm) {
+        tm->total_ms += total;
+        tm->launches += launches;
+        tm->directions += K * job.n_sel * nd;
+        tm->d2h_bytes += (double)((4 * job.n_tot + 2 * SM) * sizeof(double));
     }
 }
 

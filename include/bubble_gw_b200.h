@@ -150,6 +150,31 @@ BgwStatus bgwx_generalized_bulk_flow_compute_ensemble_khat(
     const double *w_arr, size_t n_w, bool has_t_begin, double t_begin, double t_end, size_t n_t,
     const double *khat, size_t n_khat, BgwTimeCutoffConfig time_cutoff, BgwComplex64 *out, size_t out_len);
 
+/* Adjoint (vector-Jacobian product) of the spectrum of every interior bubble
+ * along K directions k-hat (n_khat = 0: the unrotated frame, K = 1).
+ * grad_out: (K, 2, n_sets, n_w) cotangents dL/dRe C + i dL/dIm C of a real
+ * loss L, grad_len = K*2*n_sets*n_w.  Writes dL/d(coefficients) and
+ * dL/d(powers) ((n_sets, n_terms) each) and dL/d(bubbles) ((n_interior +
+ * n_exterior, 4), columns (t, x, y, z); a caller whose exterior rows are
+ * images of interior rows adds each image row's gradient to its source row).
+ * FP64 throughout; the first-collider search is recomputed, phases are
+ * recomputed rather than stored.  Collision status and first-collider identity
+ * are piecewise constant in the inputs and carry no gradient.  Differentiates
+ * generalized_bulk_flow.rs:481-873 and the delays of :421-471.  No counterpart
+ * in the reference. */
+BgwStatus bgwx_generalized_bulk_flow_spectrum_vjp(bgw_generalized_bulk_flow *bulk_flow, const double *w_arr,
+                                                  size_t n_w, bool has_t_begin, double t_begin, double t_end,
+                                                  size_t n_t, const double *khat, size_t n_khat,
+                                                  BgwTimeCutoffConfig time_cutoff, const BgwComplex64 *grad_out,
+                                                  size_t grad_len, double *grad_coefficients, double *grad_powers,
+                                                  double *grad_bubbles);
+
+/* Replaces the handle's bubbles (no causality check, as
+ * bgwx_generalized_bulk_flow_new_unchecked), keeping its settings and device
+ * state: fitting loops move bubbles between calls.  No counterpart. */
+BgwStatus bgwx_generalized_bulk_flow_set_bubbles(bgw_generalized_bulk_flow *bulk_flow, const double *interior,
+                                                 size_t n_interior, const double *exterior, size_t n_exterior);
+
 /* Runs this handle's device work on `stream` (a cudaStream_t created by the
  * caller; NULL selects the handle's own non-blocking stream, so the legacy
  * default stream cannot be chosen).  No counterpart in the reference. */

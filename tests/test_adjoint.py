@@ -1,0 +1,143 @@
+"""Adjoint of the spectrum (config-5 path): gradients with respect to the scaling
+coefficients, their powers and the bubbles' nucleation events.
+
+CPU: the oracle's FP64 adjoint (oracle/adjoint.py) against central finite
+differences (h = 1e-6) of the oracle's forward spectrum, and the fit
+parametrisation.  GPU: the library's adjoint kernels against the oracle's
+adjoint, and the torch.autograd path against central finite differences of
+the library's FP64 forward (agreement 1e-5).
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import adjoint as OA
+from oracle import oracle as O
+from gw_fopt_b200 import workloads as W
+
+H = 1e-6
+FD_TOL = 1e-5
+
+
+def small_case(seed=3, n=4):
+    inter, ext = W.uniform_config(n, 1.0, 0.2, seed=seed)
+    return dict(inter=inter, ext=ext, n_cos=8, n_phi=9, n_t=24, w=np.geomspace(1, 60, 5), kh=W.fibonacci_khat(2))
+
+
+def oracle_loss(c, inter, co, po, G, damping):
+    ext = W.periodic_images(inter, 1.0)
+    C = O.compute_c_integral_khat(inter, ext, c["kh"], c["n_cos"], c["n_phi"], c["w"], 0.0, 1.5, c["n_t"],
+                                  coefficients=co, powers=po, damping=damping)
+    return float(np.real(np.sum(np.conj(G) * C)))
+
+
+@pytest.mark.parametrize("damping", [None, 0.8])
+def test_oracle_adjoint_vs_finite_differences(damping):
+    c = small_case()
+    rng = np.random.default_rng(0)
+    co = np.array([[0.7, 0.3]])
+    po = np.array([[5.0, 3.5]])
+    G = rng.normal(size=(2, 2, 1, 5)) + 1j * rng.normal(size=(2, 2, 1, 5))
+    gc, gp, gb = OA.spectrum_vjp(c["inter"], c["ext"], c["kh"], c["n_cos"], c["n_phi"], c["w"], 0.0, 1.5,
+                                 c["n_t"], G, co, po, damping=damping)
+    n = c["inter"].shape[0]
+    gi = gb[:n] + gb[n:].reshape(n, 6, 4).sum(1)
+    for name, arr, an in [("co", co, gc), ("po", po, gp)]:
+        for idx in [(0, 0), (0, 1)]:
+            p, m = arr.copy(), arr.copy()
+            p[idx] += H
+            m[idx] -= H
+            args_p = (p, po) if name == "co" else (co, p)
+            args_m = (m, po) if name == "co" else (co, m)
+            fd = (oracle_loss(c, c["inter"], *args_p, G, damping) - oracle_loss(c, c["inter"], *args_m, G, damping)) / (2 * H)
+            assert abs(fd - an[idx]) <= FD_TOL * abs(fd), (name, idx, fd, an[idx])
+    for a in range(n):
+        for q in range(4):
+            p, m = c["inter"].copy(), c["inter"].copy()
+            p[a, q] += H
+            m[a, q] -= H
+            fd = (oracle_loss(c, p, co, po, G, damping) - oracle_loss(c, m, co, po, G, damping)) / (2 * H)
+            assert abs(fd - gi[a, q]) <= FD_TOL * max(abs(fd), 1e-3 * np.abs(gi).max()), (a, q, fd, gi[a, q])
+
+
+def test_fit_parametrisation_and_loss():
+    from gw_fopt_b200.autograd import SurfaceTensionFit, log_power_residual
+    fit = SurfaceTensionFit(xi=1.5, alpha=0.8, gamma=0.5, delta=0.2)
+    co, po = fit()
+    assert torch.allclose(co, torch.tensor([[0.8, 0.2]], dtype=torch.float64))
+    assert torch.allclose(po, torch.tensor([[5.0, 4.5]], dtype=torch.float64))
+    c = torch.randn(2, 2, 1, 3, 2, dtype=torch.float64, requires_grad=True)
+    tgt = torch.rand(2, 1, 3, dtype=torch.float64) + 0.5
+    loss = log_power_residual(c, tgt)
+    loss.backward()
+    assert c.grad is not None and torch.isfinite(c.grad).all()
+
+
+def _library_model(c, kernel="fp64_factored", damping=None):
+    from gw_fopt_b200.autograd import BulkFlowSpectrum
+    return BulkFlowSpectrum(n_cos=c["n_cos"], n_phi=c["n_phi"], w=c["w"], khat=c["kh"], t_end=1.5, n_t=c["n_t"],
+                            box=1.0, damping=damping, kernel=kernel)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sets", [((0.7, 0.3), (5.0, 3.5)), ((1.0,), (5.0,))])
+@pytest.mark.parametrize("damping", [None, 0.8])
+def test_library_adjoint_vs_oracle(gpu_available, sets, damping):
+    c = small_case(seed=5, n=6)
+    c["n_cos"], c["n_phi"], c["n_t"] = 10, 12, 40
+    co = np.array([sets[0]])
+    po = np.array([sets[1]])
+    if len(sets[0]) == 1:  # two coefficient sets of one term each
+        co = np.array([[1.0], [0.4]])
+        po = np.array([[5.0], [2.5]])
+    S = co.shape[0]
+    rng = np.random.default_rng(1)
+    G = rng.normal(size=(2, 2, S, 5)) + 1j * rng.normal(size=(2, 2, S, 5))
+    m = _library_model(c, damping=damping)
+    gc, gp, gx = m.vjp(co, po, c["inter"], G)
+    oc, op, ob = OA.spectrum_vjp(c["inter"], c["ext"], c["kh"], c["n_cos"], c["n_phi"], c["w"], 0.0, 1.5,
+                                 c["n_t"], G, co, po, damping=damping)
+    n = c["inter"].shape[0]
+    ox = ob[:n] + ob[n:].reshape(n, 6, 4).sum(1)
+    for got, ref in [(gc, oc), (gp, op), (gx, ox)]:
+        assert np.allclose(got, ref, rtol=1e-9, atol=1e-12 * np.abs(ref).max()), (got, ref)
+
+
+@pytest.mark.gpu
+def test_autograd_vs_finite_differences(gpu_available):
+    from gw_fopt_b200.autograd import SurfaceTensionFit, log_power_residual
+    c = small_case(seed=7, n=8)
+    c["n_cos"], c["n_phi"], c["n_t"] = 16, 16, 64
+    c["w"] = np.geomspace(1.0, 200.0, 12)
+    c["kh"] = W.fibonacci_khat(3)
+    m = _library_model(c)
+    fit = SurfaceTensionFit(xi=1.5, alpha=0.9, gamma=0.3, delta=0.1)
+    x = torch.tensor(c["inter"], dtype=torch.float64, requires_grad=True)
+    with torch.no_grad():
+        co_t, po_t = SurfaceTensionFit(xi=2.0, alpha=1.0, gamma=0.0, delta=0.0)()
+        target = (m(co_t, po_t, x) ** 2).sum(-1).sum(1) * 1.1
+    co, po = fit()
+    loss = log_power_residual(m(co, po, x), target)
+    loss.backward()
+
+    def f(xi=1.5, alpha=0.9, gamma=0.3, delta=0.1, xx=None):
+        with torch.no_grad():
+            cc, pp = SurfaceTensionFit(xi, alpha, gamma, delta)()
+            return float(log_power_residual(m(cc, pp, x if xx is None else xx), target))
+
+    base = dict(xi=1.5, alpha=0.9, gamma=0.3, delta=0.1)
+    for name in base:
+        p, q = dict(base), dict(base)
+        p[name] += H
+        q[name] -= H
+        fd = (f(**p) - f(**q)) / (2 * H)
+        an = float(getattr(fit, name).grad)
+        assert abs(fd - an) <= FD_TOL * abs(fd), (name, fd, an)
+    gx = x.grad.numpy()
+    scale = np.abs(gx).max()
+    for a, q in [(0, 0), (1, 1), (2, 2), (3, 3), (5, 0), (7, 3)]:
+        xp, xm = x.detach().clone(), x.detach().clone()
+        xp[a, q] += H
+        xm[a, q] -= H
+        fd = (f(xx=xp) - f(xx=xm)) / (2 * H)
+        assert abs(fd - gx[a, q]) <= FD_TOL * max(abs(fd), 1e-2 * scale), (a, q, fd, gx[a, q])
