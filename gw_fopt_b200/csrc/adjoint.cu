@@ -23,9 +23,11 @@
 // identity are piecewise constant in the inputs and carry no gradient.
 //
 // Kernels:
-//   k_adj_phase   per (frame, bubble, row, step): Re P and Im Q (one FP64 sincos per w)
+//   k_adj_mtab    the time-phase table M_i(w, k), once per call
+//   k_adj_pq      per (frame, row): Re P and Im Q as two real products of depth W
 //   k_adj_rows    one warp per (frame, bubble, row): the patch sums above, dL/dtau per patch
-//   k_adj_geom    per (frame, bubble, patch): dL/dtau -> both bubbles of the collision (atomics)
+//   k_adj_geom    per (frame, bubble, patch): dL/dtau -> both bubbles of the collision (one atomic
+//                 per run of equal bubbles in a warp)
 //   k_adj_bubble  per (frame, bubble): the row partials of t_a and z_a (atomics)
 //   k_adj_params  per parameter: fixed-order sum of the row partials
 
@@ -41,7 +43,6 @@
 namespace bgw {
 
 constexpr int kAdjThreads = 256;
-constexpr int kMaxJPerLane = 8;  // n_phi <= 256
 
 struct AdjArgs {
     const D4* bub;        // rotated bubbles of the chunk's frames, (kn, n_tot)
@@ -72,52 +73,134 @@ struct AdjArgs {
 };
 
 // ---------------------------------------------------------------------------
+// The phase factorises as e^{i phi} = M_i(w, k) E_{a,i}(w) with
+// M_i = e^{i w t_k (1 - c_i)} (frame and bubble independent) and
+// E_{a,i} = e^{i w (t_a c_i - z_a)}, so for each row i
+//   P_{a,gs}(k) = sum_w H_{a,gs}(w) M_i(w, k),   H = conj(G_gs(w)) E_{a,i}(w),
+//   Re P = sum_w (Hr Mr - Hi Mi),   Im Q = sum_w w (Hr Mi + Hi Mr):
+// two real products of depth W per (frame, row), computed by k_adj_pq.
+__global__ void k_adj_mtab(const double* __restrict__ cos_t, const double* __restrict__ t_arr,
+                           const double* __restrict__ w, int n_cos, int n_w, int n_t, double2* __restrict__ mt) {
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (size_t)n_cos * n_w * n_t) return;
+    const int k = (int)(q % n_t);
+    const int wi = (int)((q / n_t) % n_w);
+    const int i = (int)(q / ((size_t)n_t * n_w));
+    double sn, cs;
+    sincos(w[wi] * (t_arr[k] * (1.0 - cos_t[i])), &sn, &cs);
+    mt[q] = make_double2(cs, sn);
+}
+
+constexpr int kPqRows = 64;   // (bubble, set, g) rows per tile
+constexpr int kPqCols = 64;   // time steps per tile
+constexpr int kPqW = 16;      // frequencies per shared-memory stage
+
+// One CTA per (row tile x step tile, cos-theta row i, frame).  Thread
+// (ty, tx) of 16 x 16 owns rows ty + 16 u and steps tx + 16 v (u, v < 4).
 template <int S>
-__global__ void __launch_bounds__(kAdjThreads) k_adj_phase(AdjArgs A) {
-    extern __shared__ __align__(16) unsigned char sm_raw[];
+__global__ void __launch_bounds__(kAdjThreads) k_adj_pq(AdjArgs A, const double2* __restrict__ mt, int row_tiles) {
     constexpr int S2 = 2 * S;
+    __shared__ double2 Hs[kPqW][kPqRows];
+    __shared__ double2 Ms[kPqW][kPqCols];
+    __shared__ double ws[kPqW];
+    const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
+    const int rt = blockIdx.x % row_tiles, kt = blockIdx.x / row_tiles;
+    const int i = blockIdx.y, f = blockIdx.z;
     const int W = A.n_w;
-    double2* G = reinterpret_cast<double2*>(sm_raw);  // [S2][W]
-    double* ws = reinterpret_cast<double*>(G + S2 * W);
-    const int i = blockIdx.x, slot = blockIdx.y, f = blockIdx.z;
-    for (int q = threadIdx.x; q < S2 * W; q += blockDim.x) G[q] = A.gbar[(size_t)f * S2 * W + q];
-    for (int q = threadIdx.x; q < W; q += blockDim.x) ws[q] = A.w[q];
-    __syncthreads();
-    const D4 xa = A.bub[(size_t)f * A.n_tot + A.sel[slot]];
+    const int n_rows = A.n_sel * S2;
+    const int r0 = rt * kPqRows, k0 = kt * kPqCols;
     const double ci = A.cos_t[i];
-    const size_t row = ((size_t)f * A.n_sel + slot) * A.n_cos + i;
-    for (int k = threadIdx.x; k < A.n_t; k += blockDim.x) {
-        const double tk = A.t_arr[k];
-        const double dtk = tk - xa.t;
-        const size_t o = (row * A.n_t + k) * S2;
-        double P[S2], Q[S2];
+    double P[4][4], Q[4][4];
 #pragma unroll
-        for (int g = 0; g < S2; ++g) P[g] = Q[g] = 0.0;
-        if (dtk > 0.0) {
-            const double theta = (tk - xa.z) - dtk * ci;
-            for (int q = 0; q < W; ++q) {
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+        for (int v = 0; v < 4; ++v) P[u][v] = Q[u][v] = 0.0;
+    for (int w0 = 0; w0 < W; w0 += kPqW) {
+        __syncthreads();
+        // H tile: row r = slot * S2 + gs
+        for (int q = tid; q < kPqW * kPqRows; q += blockDim.x) {
+            const int wl = q / kPqRows, rl = q % kPqRows;
+            const int wi = w0 + wl, r = r0 + rl;
+            double2 h = make_double2(0.0, 0.0);
+            if (wi < W && r < n_rows) {
+                const int slot = r / S2, gs = r % S2;
+                const D4 xa = A.bub[(size_t)f * A.n_tot + A.sel[slot]];
                 double sn, cs;
-                sincos(ws[q] * theta, &sn, &cs);
-#pragma unroll
-                for (int g = 0; g < S2; ++g) {
-                    const double2 gv = G[g * W + q];
-                    P[g] += gv.x * cs + gv.y * sn;
-                    Q[g] += ws[q] * (gv.x * sn - gv.y * cs);
-                }
+                sincos(A.w[wi] * (xa.t * ci - xa.z), &sn, &cs);
+                const double2 g = A.gbar[((size_t)f * S2 + gs) * W + wi];
+                // conj(g) * (cs + i sn)
+                h = make_double2(g.x * cs + g.y * sn, g.x * sn - g.y * cs);
             }
+            Hs[wl][rl] = h;
         }
+        for (int q = tid; q < kPqW * kPqCols; q += blockDim.x) {
+            const int wl = q / kPqCols, kl = q % kPqCols;
+            const int wi = w0 + wl, k = k0 + kl;
+            Ms[wl][kl] = (wi < W && k < A.n_t) ? mt[((size_t)i * W + wi) * A.n_t + k] : make_double2(0.0, 0.0);
+        }
+        if (tid < kPqW) ws[tid] = w0 + tid < W ? A.w[w0 + tid] : 0.0;
+        __syncthreads();
+#pragma unroll 4
+        for (int wl = 0; wl < kPqW; ++wl) {
+            double2 h[4], m[4];
 #pragma unroll
-        for (int g = 0; g < S2; ++g) {
-            A.s.bbar[o + g] = P[g];
-            A.s.imq[o + g] = Q[g];
+            for (int u = 0; u < 4; ++u) h[u] = Hs[wl][ty + 16 * u];
+#pragma unroll
+            for (int v = 0; v < 4; ++v) m[v] = Ms[wl][tx + 16 * v];
+            const double om = ws[wl];
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+                for (int v = 0; v < 4; ++v) {
+                    P[u][v] = fma(h[u].x, m[v].x, fma(-h[u].y, m[v].y, P[u][v]));
+                    Q[u][v] = fma(om, fma(h[u].x, m[v].y, h[u].y * m[v].x), Q[u][v]);
+                }
+        }
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int r = r0 + ty + 16 * u;
+        if (r >= n_rows) continue;
+        const int slot = r / S2, gs = r % S2;
+        const size_t row = ((size_t)f * A.n_sel + slot) * A.n_cos + i;
+#pragma unroll
+        for (int v = 0; v < 4; ++v) {
+            const int k = k0 + tx + 16 * v;
+            if (k >= A.n_t) continue;
+            const size_t o = (row * A.n_t + k) * S2 + gs;
+            A.s.bbar[o] = P[u][v];
+            A.s.imq[o] = Q[u][v];
         }
     }
 }
 
 // ---------------------------------------------------------------------------
-template <int S, int SMC>
-__global__ void __launch_bounds__(kAdjThreads) k_adj_rows(AdjArgs A) {
+// Per (bubble, step) factors of the collided scaling, frame independent:
+// with r = tau/dt, a r^p D = a (tau^p e^{tau/w}) (dt^{-p} e^{-dt/w}), so the
+// patch factor tau^p e^{tau/w} is formed once per patch and the step factor
+// once per (bubble, step).  Row layout: dt^2, dt^3, ln dt, 1/dt, then
+// dt^{-p_q} e^{-dt/w} for every (set, term) q; zeros where dt <= 0.
+__global__ void k_adj_ttab(const D4* __restrict__ bub, const uint32_t* __restrict__ sel, int n_sel,
+                           const double* __restrict__ t_arr, int n_t, const double* __restrict__ powers, int SM,
+                           int has_damp, double damp, double* __restrict__ tt) {
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (size_t)n_sel * n_t) return;
+    const int slot = (int)(q / n_t), k = (int)(q % n_t);
+    const double dtk = t_arr[k] - bub[sel[slot]].t;
+    double* row = tt + q * (4 + SM);
+    const bool on = dtk > 0.0;
+    row[0] = on ? dtk * dtk : 0.0;
+    row[1] = on ? dtk * dtk * dtk : 0.0;
+    row[2] = on ? log(dtk) : 0.0;
+    row[3] = on ? 1.0 / dtk : 0.0;
+    const double e = has_damp ? exp(-dtk / damp) : 1.0;
+    for (int m = 0; m < SM; ++m) row[4 + m] = on ? exp(-powers[m] * log(dtk)) * e : 0.0;
+}
+
+template <int S, int SMC, int JPL>
+__global__ void __launch_bounds__(kAdjThreads) k_adj_rows(AdjArgs A, const double* __restrict__ tt) {
     constexpr int S2 = 2 * S;
+    constexpr int TW = 4 + SMC;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const long row = (long)blockIdx.x * (blockDim.x >> 5) + warp;
     const long R = (long)A.n_sel * A.n_cos;  // rows per frame
@@ -127,40 +210,59 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_rows(AdjArgs A) {
     const int i = (int)(row % A.n_cos);
     const int M = A.M;
     const int nd = A.n_cos * A.n_phi;
-    const D4 xa = A.bub[(size_t)f * A.n_tot + A.sel[slot]];
+    const double ta = A.bub[(size_t)f * A.n_tot + A.sel[slot]].t;
     const double ci = A.cos_t[i];
     const double vi = (i == 0 || i == A.n_cos - 1) ? 0.5 : 1.0;
     const double rowc = 0.5 * (1.0 - ci * ci) * A.dphi * A.dcos * vi * A.dt / (6.0 * M_PI);
     const double invw = A.has_damp ? 1.0 / A.damp : 0.0;
 
-    double tau_j[kMaxJPerLane], q0[kMaxJPerLane], q1[kMaxJPerLane], tbar[kMaxJPerLane];
-#pragma unroll
-    for (int jj = 0; jj < kMaxJPerLane; ++jj) {
-        const int j = lane + 32 * jj;
-        const bool ok = j < A.n_phi;
-        const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
-        tau_j[jj] = ok ? A.tau[((size_t)f * A.n_sel + slot) * nd + (size_t)i * A.n_phi + j] : 0.0;
-        q0[jj] = ok ? wj * A.cos2[j] : 0.0;
-        q1[jj] = ok ? wj * A.sin2[j] : 0.0;
-        tbar[jj] = 0.0;
-    }
     double a_c[SMC], p_c[SMC];
 #pragma unroll
     for (int q = 0; q < SMC; ++q) {
         a_c[q] = A.coeffs[q];
         p_c[q] = A.powers[q];
     }
+    // per-patch factors of this lane's patches j = lane + 32 jj
+    double tau_j[JPL], q0[JPL], q1[JPL], tbar[JPL], lt[JPL], al[JPL][SMC], c2[JPL][SMC];
+#pragma unroll
+    for (int jj = 0; jj < JPL; ++jj) {
+        const int j = lane + 32 * jj;
+        const bool ok = j < A.n_phi;
+        const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
+        const double tj = ok ? A.tau[((size_t)f * A.n_sel + slot) * nd + (size_t)i * A.n_phi + j] : 0.0;
+        tau_j[jj] = tj;
+        q0[jj] = ok ? wj * A.cos2[j] : 0.0;
+        q1[jj] = ok ? wj * A.sin2[j] : 0.0;
+        tbar[jj] = 0.0;
+        const bool pos = tj > 0.0;
+        lt[jj] = pos ? log(tj) : 0.0;
+        const double et = (pos && A.has_damp) ? exp(tj * invw) : 1.0;
+#pragma unroll
+        for (int q = 0; q < SMC; ++q) {
+            al[jj][q] = pos ? exp(p_c[q] * lt[jj]) * et : 0.0;
+            c2[jj][q] = pos ? p_c[q] / tj + invw : 0.0;
+        }
+    }
     double acc_t = 0.0, acc_z = 0.0, abar[SMC], pbar[SMC];
 #pragma unroll
     for (int q = 0; q < SMC; ++q) abar[q] = pbar[q] = 0.0;
 
     const size_t base = ((size_t)f * A.n_sel + slot) * A.n_cos + i;
+    const double* trow = tt + (size_t)slot * A.n_t * TW;
     for (int k = 0; k < A.n_t; ++k) {
-        const double dtk = A.t_arr[k] - xa.t;
+        const double dtk = A.t_arr[k] - ta;
         if (!(dtk > 0.0)) continue;
+        const double* tk = trow + (size_t)k * TW;
+        const double d2 = tk[0], d3 = tk[1], ld = tk[2], invd = tk[3];
+        double be[SMC], c1[SMC];
+#pragma unroll
+        for (int q = 0; q < SMC; ++q) {
+            be[q] = tk[4 + q];
+            c1[q] = -p_c[q] * invd - invw;
+        }
         const double uk = (k == 0 || k == A.n_t - 1) ? 0.5 : 1.0;
         const double pre = rowc * uk * A.cutw[k];
-        const double d2 = dtk * dtk, d3 = d2 * dtk;
+        const double pd3 = pre * d3;
         const size_t o = (base * A.n_t + k) * S2;
         double bb[S2], iq[S2];
 #pragma unroll
@@ -169,8 +271,7 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_rows(AdjArgs A) {
             iq[g] = A.s.imq[o + g];
         }
 #pragma unroll
-        for (int jj = 0; jj < kMaxJPerLane; ++jj) {
-            if (lane + 32 * jj >= A.n_phi) break;
+        for (int jj = 0; jj < JPL; ++jj) {
             double Bs[S], Is[S];
 #pragma unroll
             for (int s = 0; s < S; ++s) {
@@ -178,24 +279,22 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_rows(AdjArgs A) {
                 Is[s] = iq[s] * q0[jj] + iq[S + s] * q1[jj];
             }
             const double tj = tau_j[jj];
+            // the reference's status test (generalized_bulk_flow.rs:405)
             if (tj > 0.0 && dtk >= tj) {
-                const double r = tj / dtk;
-                const double lr = log(r);
-                const double D = A.has_damp ? exp(-(dtk - tj) * invw) : 1.0;
                 double fs[S], dfdt[S], dfdtau[S];
 #pragma unroll
                 for (int s = 0; s < S; ++s) fs[s] = dfdt[s] = dfdtau[s] = 0.0;
 #pragma unroll
                 for (int q = 0; q < SMC; ++q) {
                     const int s = q / M;
-                    const double rpD = exp(p_c[q] * lr) * D;
+                    const double rpD = al[jj][q] * be[q];
                     const double e = a_c[q] * rpD;
                     fs[s] += e;
-                    dfdt[s] += e * (-p_c[q] / dtk - invw);
-                    dfdtau[s] += e * (p_c[q] / tj + invw);
-                    const double wgt = pre * d3 * Bs[s] * rpD;
+                    dfdt[s] += e * c1[q];
+                    dfdtau[s] += e * c2[jj][q];
+                    const double wgt = pd3 * Bs[s] * rpD;
                     abar[q] += wgt;
-                    pbar[q] += wgt * a_c[q] * lr;
+                    pbar[q] += wgt * a_c[q] * (lt[jj] - ld);
                 }
                 double st = 0.0, sz = 0.0, sx = 0.0;
 #pragma unroll
@@ -204,9 +303,9 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_rows(AdjArgs A) {
                     sz += Is[s] * fs[s];
                     sx += Bs[s] * dfdtau[s];
                 }
-                acc_t += pre * (-st - ci * d3 * sz);
-                acc_z += pre * d3 * sz;
-                tbar[jj] += pre * d3 * sx;
+                acc_t -= pre * st + ci * pd3 * sz;
+                acc_z += pd3 * sz;
+                tbar[jj] += pd3 * sx;
             } else {
                 double sb = 0.0, sz = 0.0;
 #pragma unroll
@@ -214,13 +313,13 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_rows(AdjArgs A) {
                     sb += Bs[s];
                     sz += Is[s];
                 }
-                acc_t += pre * (-3.0 * d2 * sb - ci * d3 * sz);
-                acc_z += pre * d3 * sz;
+                acc_t -= 3.0 * pre * d2 * sb + ci * pd3 * sz;
+                acc_z += pd3 * sz;
             }
         }
     }
 #pragma unroll
-    for (int jj = 0; jj < kMaxJPerLane; ++jj) {
+    for (int jj = 0; jj < JPL; ++jj) {
         const int j = lane + 32 * jj;
         if (j < A.n_phi) A.s.taubar[((size_t)f * A.n_sel + slot) * nd + (size_t)i * A.n_phi + j] = tbar[jj];
     }
@@ -248,51 +347,87 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_rows(AdjArgs A) {
 }
 
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void add_rotated_back(double* g, const double* R, double gt, double gx, double gy,
-                                                 double gz, double sign) {
+__device__ __forceinline__ void rotate_back(const double* R, double& gx, double& gy, double& gz) {
     // X' = R X  =>  dL/dX = R^T dL/dX'
-    double ux = gx, uy = gy, uz = gz;
-    if (R) {
-        ux = R[0] * gx + R[3] * gy + R[6] * gz;
-        uy = R[1] * gx + R[4] * gy + R[7] * gz;
-        uz = R[2] * gx + R[5] * gy + R[8] * gz;
+    if (!R) return;
+    const double ux = R[0] * gx + R[3] * gy + R[6] * gz;
+    const double uy = R[1] * gx + R[4] * gy + R[7] * gz;
+    const double uz = R[2] * gx + R[5] * gy + R[8] * gz;
+    gx = ux;
+    gy = uy;
+    gz = uz;
+}
+
+// Adds each lane's 4-vector to g_bub[key] (key < 0: nothing) with one atomic
+// per run of equal keys in consecutive lanes: neighbouring patches mostly share
+// their radiating bubble and their first collider.  Call with the full warp.
+__device__ __forceinline__ void warp_runs_add(double* g_bub, long key, double v0, double v1, double v2, double v3) {
+    const int lane = threadIdx.x & 31;
+    const long prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const bool head = lane == 0 || prev != key;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const int run = __popc(heads & (0xffffffffu >> (31 - lane)));  // runs started at or before this lane
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int r_up = __shfl_up_sync(0xffffffffu, run, off);
+        const double u0 = __shfl_up_sync(0xffffffffu, v0, off);
+        const double u1 = __shfl_up_sync(0xffffffffu, v1, off);
+        const double u2 = __shfl_up_sync(0xffffffffu, v2, off);
+        const double u3 = __shfl_up_sync(0xffffffffu, v3, off);
+        if (lane >= off && r_up == run) {
+            v0 += u0;
+            v1 += u1;
+            v2 += u2;
+            v3 += u3;
+        }
     }
-    atomicAdd(g + 0, sign * gt);
-    atomicAdd(g + 1, sign * ux);
-    atomicAdd(g + 2, sign * uy);
-    atomicAdd(g + 3, sign * uz);
+    const int r_dn = __shfl_down_sync(0xffffffffu, run, 1);
+    const bool tail = lane == 31 || r_dn != run;
+    if (tail && key >= 0) {
+        double* g = g_bub + 4 * key;
+        atomicAdd(g + 0, v0);
+        atomicAdd(g + 1, v1);
+        atomicAdd(g + 2, v2);
+        atomicAdd(g + 3, v3);
+    }
 }
 
 __global__ void k_adj_geom(AdjArgs A) {
     const int nd = A.n_cos * A.n_phi;
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     const int f = blockIdx.y;
-    if (q >= (size_t)A.n_sel * nd) return;
-    const int slot = (int)(q / nd), d = (int)(q % nd);
-    const size_t o = ((size_t)f * A.n_sel + slot) * nd + d;
-    const double tb = A.s.taubar[o];
-    if (tb == 0.0) return;
-    const int32_t code = A.codes[o];
-    const double tau = A.tau[o];
-    if (code == -1 || !(tau > 0.0)) return;
-    const size_t b = code >= 0 ? (size_t)code : (size_t)A.n_int + (size_t)(-(code + 2));
-    const uint32_t a = A.sel[slot];
-    const D4 xa = A.bub[(size_t)f * A.n_tot + a];
-    const D4 xb = A.bub[(size_t)f * A.n_tot + b];
-    const D4 n = A.dirs[d];
-    const double Dt = xb.t - xa.t, Dx = xb.x - xa.x, Dy = xb.y - xa.y, Dz = xb.z - xa.z;
-    const double dot = -Dt + Dx * n.x + Dy * n.y + Dz * n.z;
-    if (fabs(dot) < 1e-10) return;
-    const double D2 = -Dt * Dt + Dx * Dx + Dy * Dy + Dz * Dz;
-    const double inv = 1.0 / dot;
-    const double h = 0.5 * D2 * inv * inv;
-    const double gt = tb * (-Dt * inv + h);
-    const double gx = tb * (Dx * inv - h * n.x);
-    const double gy = tb * (Dy * inv - h * n.y);
-    const double gz = tb * (Dz * inv - h * n.z);
-    const double* R = A.rot ? A.rot + 9 * f : nullptr;
-    add_rotated_back(A.g_bub + 4 * b, R, gt, gx, gy, gz, 1.0);
-    add_rotated_back(A.g_bub + 4 * (size_t)a, R, gt, gx, gy, gz, -1.0);
+    long ka = -1, kb = -1;
+    double gt = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    if (q < (size_t)A.n_sel * nd) {
+        const int slot = (int)(q / nd), d = (int)(q % nd);
+        const size_t o = ((size_t)f * A.n_sel + slot) * nd + d;
+        const double tb = A.s.taubar[o];
+        const int32_t code = A.codes[o];
+        const double tau = A.tau[o];
+        if (tb != 0.0 && code != -1 && tau > 0.0) {
+            const size_t b = code >= 0 ? (size_t)code : (size_t)A.n_int + (size_t)(-(code + 2));
+            const uint32_t a = A.sel[slot];
+            const D4 xa = A.bub[(size_t)f * A.n_tot + a];
+            const D4 xb = A.bub[(size_t)f * A.n_tot + b];
+            const D4 n = A.dirs[d];
+            const double Dt = xb.t - xa.t, Dx = xb.x - xa.x, Dy = xb.y - xa.y, Dz = xb.z - xa.z;
+            const double dot = -Dt + Dx * n.x + Dy * n.y + Dz * n.z;
+            if (fabs(dot) >= 1e-10) {
+                const double D2 = -Dt * Dt + Dx * Dx + Dy * Dy + Dz * Dz;
+                const double inv = 1.0 / dot;
+                const double h = 0.5 * D2 * inv * inv;
+                gt = tb * (-Dt * inv + h);
+                gx = tb * (Dx * inv - h * n.x);
+                gy = tb * (Dy * inv - h * n.y);
+                gz = tb * (Dz * inv - h * n.z);
+                rotate_back(A.rot ? A.rot + 9 * f : nullptr, gx, gy, gz);
+                ka = (long)a;
+                kb = (long)b;
+            }
+        }
+    }
+    warp_runs_add(A.g_bub, kb, gt, gx, gy, gz);
+    warp_runs_add(A.g_bub, ka, -gt, -gx, -gy, -gz);
 }
 
 template <int SMC>
@@ -306,9 +441,14 @@ __global__ void k_adj_bubble(AdjArgs A) {
         st += rp[0];
         sz += rp[1];
     }
-    const double* R = A.rot ? A.rot + 9 * f : nullptr;
     // z' = R[2,:] . x  =>  dL/dx += dL/dz' R[2,:]
-    add_rotated_back(A.g_bub + 4 * (size_t)A.sel[slot], R, st, 0.0, 0.0, sz, 1.0);
+    double gx = 0.0, gy = 0.0, gz = sz;
+    rotate_back(A.rot ? A.rot + 9 * f : nullptr, gx, gy, gz);
+    double* g = A.g_bub + 4 * (size_t)A.sel[slot];
+    atomicAdd(g + 0, st);
+    atomicAdd(g + 1, gx);
+    atomicAdd(g + 2, gy);
+    atomicAdd(g + 3, gz);
 }
 
 template <int SMC>
@@ -327,22 +467,30 @@ __global__ void k_adj_params(AdjArgs A, long n_rows) {
 }
 
 // ---------------------------------------------------------------------------
+template <int S, int SMC, int JPL>
+static void launch_rows(const AdjArgs& A, long rows, cudaStream_t st, const double* tt) {
+    const int warps = kAdjThreads / 32;
+    k_adj_rows<S, SMC, JPL><<<(unsigned)((rows + warps - 1) / warps), kAdjThreads, 0, st>>>(A, tt);
+}
+
 template <int S, int SMC>
-static uint64_t launch_typed(const AdjArgs& A, size_t kn, cudaStream_t st) {
+static uint64_t launch_typed(const AdjArgs& A, size_t kn, cudaStream_t st, const double2* mt, const double* tt) {
     uint64_t launches = 0;
     {
-        const size_t smem = (size_t)2 * S * A.n_w * sizeof(double2) + (size_t)A.n_w * sizeof(double);
-        if (smem > 200 * 1024) throw Error{"too many frequencies for the adjoint's shared memory"};
-        CUDA_OK(cudaFuncSetAttribute(k_adj_phase<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        dim3 g((unsigned)A.n_cos, (unsigned)A.n_sel, (unsigned)kn);
-        k_adj_phase<S><<<g, kAdjThreads, smem, st>>>(A);
+        const int row_tiles = (A.n_sel * 2 * S + kPqRows - 1) / kPqRows;
+        const int col_tiles = (A.n_t + kPqCols - 1) / kPqCols;
+        if ((long)row_tiles * col_tiles > 0x7fffffffL) throw Error{"adjoint grid too large"};
+        dim3 g((unsigned)(row_tiles * col_tiles), (unsigned)A.n_cos, (unsigned)kn);
+        k_adj_pq<S><<<g, kAdjThreads, 0, st>>>(A, mt, row_tiles);
         CUDA_OK(cudaGetLastError());
         ++launches;
     }
     {
         const long rows = (long)kn * A.n_sel * A.n_cos;
-        const int warps = kAdjThreads / 32;
-        k_adj_rows<S, SMC><<<(unsigned)((rows + warps - 1) / warps), kAdjThreads, 0, st>>>(A);
+        if (A.n_phi <= 32) launch_rows<S, SMC, 1>(A, rows, st, tt);
+        else if (A.n_phi <= 64) launch_rows<S, SMC, 2>(A, rows, st, tt);
+        else if (A.n_phi <= 128) launch_rows<S, SMC, 4>(A, rows, st, tt);
+        else launch_rows<S, SMC, 8>(A, rows, st, tt);
         CUDA_OK(cudaGetLastError());
         ++launches;
         const size_t per = (size_t)A.n_sel * A.n_cos * A.n_phi;
@@ -362,16 +510,36 @@ static uint64_t launch_typed(const AdjArgs& A, size_t kn, cudaStream_t st) {
 }
 
 template <int S, int M>
-static uint64_t dispatch_m(const AdjArgs& A, size_t kn, cudaStream_t st) {
-    return launch_typed<S, S * M>(A, kn, st);
+static uint64_t dispatch_m(const AdjArgs& A, size_t kn, cudaStream_t st, const double2* mt, const double* tt) {
+    return launch_typed<S, S * M>(A, kn, st, mt, tt);
+}
+
+uint64_t launch_adjoint_tables(Device* dev, const SpectrumJob& job, const D4* bub, const uint32_t* sel,
+                               const double* cos_t, const double* t_arr, const double* w, const double* powers,
+                               double2* mt, double* tt) {
+    if (job.has_damping) {
+        const double span = job.t_arr[job.n_t - 1] - job.t_arr[0] + 4.0;
+        if (!(std::fabs(span / job.damping) < 600.0))
+            throw Error{"damping width too small for the adjoint (exp overflow)"};
+    }
+    const size_t n = job.n_cos * job.n_w * job.n_t;
+    k_adj_mtab<<<(unsigned)((n + 255) / 256), 256, 0, dev->stream>>>(cos_t, t_arr, w, (int)job.n_cos,
+                                                                       (int)job.n_w, (int)job.n_t, mt);
+    CUDA_OK(cudaGetLastError());
+    const size_t nt = job.n_sel * job.n_t;
+    k_adj_ttab<<<(unsigned)((nt + 255) / 256), 256, 0, dev->stream>>>(
+        bub, sel, (int)job.n_sel, t_arr, (int)job.n_t, powers, (int)(job.n_sets * job.n_terms),
+        job.has_damping ? 1 : 0, job.damping, tt);
+    CUDA_OK(cudaGetLastError());
+    return 2;
 }
 
 uint64_t launch_adjoint_chunk(Device* dev, const SpectrumJob& job, const D4* bub_frames, const uint32_t* sel,
                               const double* tau, const int32_t* codes, const D4* dirs, const double* cos_t,
                               const double* sin2, const double* cos2, const double* coeffs, const double* powers,
                               const double* t_arr, const double* cutw, const double* w, const double* rot,
-                              const double2* gbar, size_t kn, const AdjointScratch& s, double* g_bub,
-                              double* g_par) {
+                              const double2* gbar, size_t kn, const AdjointScratch& s, const double2* mt,
+                              const double* tt, double* g_bub, double* g_par) {
     AdjArgs A;
     A.bub = bub_frames;
     A.n_tot = job.n_tot;
@@ -406,7 +574,7 @@ uint64_t launch_adjoint_chunk(Device* dev, const SpectrumJob& job, const D4* bub
     A.s = s;
     A.g_bub = g_bub;
     A.g_par = g_par;
-    if (job.n_phi > 32 * kMaxJPerLane) throw Error{"the adjoint supports n_phi <= 256"};
+    if (job.n_phi > 256) throw Error{"the adjoint supports n_phi <= 256"};
     if (kn > 65535 || job.n_sel > 65535 || job.n_cos > 65535) throw Error{"adjoint grid too large"};
     const cudaStream_t st = dev->stream;
     const int S = A.S, M = A.M;
@@ -414,25 +582,25 @@ uint64_t launch_adjoint_chunk(Device* dev, const SpectrumJob& job, const D4* bub
     switch (S) {
         case 1:
             switch (M) {
-                case 1: return dispatch_m<1, 1>(A, kn, st);
-                case 2: return dispatch_m<1, 2>(A, kn, st);
-                case 3: return dispatch_m<1, 3>(A, kn, st);
-                case 4: return dispatch_m<1, 4>(A, kn, st);
+                case 1: return dispatch_m<1, 1>(A, kn, st, mt, tt);
+                case 2: return dispatch_m<1, 2>(A, kn, st, mt, tt);
+                case 3: return dispatch_m<1, 3>(A, kn, st, mt, tt);
+                case 4: return dispatch_m<1, 4>(A, kn, st, mt, tt);
                 default: break;
             }
             break;
         case 2:
             switch (M) {
-                case 1: return dispatch_m<2, 1>(A, kn, st);
-                case 2: return dispatch_m<2, 2>(A, kn, st);
+                case 1: return dispatch_m<2, 1>(A, kn, st, mt, tt);
+                case 2: return dispatch_m<2, 2>(A, kn, st, mt, tt);
                 default: break;
             }
             break;
         case 3:
-            if (M == 1) return dispatch_m<3, 1>(A, kn, st);
+            if (M == 1) return dispatch_m<3, 1>(A, kn, st, mt, tt);
             break;
         case 4:
-            if (M == 1) return dispatch_m<4, 1>(A, kn, st);
+            if (M == 1) return dispatch_m<4, 1>(A, kn, st, mt, tt);
             break;
         default: break;
     }

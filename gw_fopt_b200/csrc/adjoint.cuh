@@ -21,8 +21,14 @@ uint64_t launch_adjoint_chunk(Device* dev, const SpectrumJob& job, const D4* bub
                               const double* tau, const int32_t* codes, const D4* dirs, const double* cos_t,
                               const double* sin2, const double* cos2, const double* coeffs, const double* powers,
                               const double* t_arr, const double* cutw, const double* w, const double* rot,
-                              const double2* gbar, size_t kn, const AdjointScratch& s, double* g_bub,
-                              double* g_par);
+                              const double2* gbar, size_t kn, const AdjointScratch& s, const double2* mt,
+                              const double* tt, double* g_bub, double* g_par);
+
+// Frame-independent tables: mt (n_cos, n_w, n_t) time phases e^{i w t_k (1 - c_i)};
+// tt (n_sel, n_t, 4 + S M) per (bubble, step) factors of the collided scaling.
+uint64_t launch_adjoint_tables(Device* dev, const SpectrumJob& job, const D4* bub, const uint32_t* sel,
+                               const double* cos_t, const double* t_arr, const double* w, const double* powers,
+                               double2* mt, double* tt);
 
 size_t adjoint_bytes_per_frame(const SpectrumJob& job);
 

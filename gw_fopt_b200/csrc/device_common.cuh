@@ -78,7 +78,7 @@ struct Device {
     DevBuf tau, codes, partial, out, counters, nblists;
     DevBuf fact_D, fact_kfirst, beta, fact_partial;  // factored-kernel work arrays
     DevBuf ens_out;                                  // batched ensemble: all realizations' spectra
-    DevBuf adj_gbar, adj_scratch, adj_grad;          // adjoint: cotangents, work arrays, gradients
+    DevBuf adj_gbar, adj_scratch, adj_grad, adj_mtab; // adjoint: cotangents, work arrays, gradients, phases
     ~Device();
 };
 

@@ -622,6 +622,11 @@ void run_adjoint(Device* dev, const SpectrumJob& job, const double* gbar, double
 
     uint64_t launches = 0;
     CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
+    const size_t mt_bytes = (job.n_cos * W * job.n_t * sizeof(double2) + 255) & ~(size_t)255;
+    dev->adj_mtab.ensure(mt_bytes + job.n_sel * job.n_t * (4 + SM) * sizeof(double));
+    double2* mt = (double2*)dev->adj_mtab.p;
+    double* tt = (double*)((unsigned char*)dev->adj_mtab.p + mt_bytes);
+    launches += launch_adjoint_tables(dev, job, bub, sel, cos_t, t_arr, w, powers, mt, tt);
     for (size_t k0 = 0; k0 < K; k0 += kc) {
         const size_t kn = std::min(kc, K - k0);
         const D4* fb = bub;
@@ -636,7 +641,8 @@ void run_adjoint(Device* dev, const SpectrumJob& job, const double* gbar, double
                              (int32_t*)dev->codes.p, (unsigned long long*)dev->counters.p, k0 == 0, &launches);
         launches += launch_adjoint_chunk(dev, job, fb, sel, (const double*)dev->tau.p, (const int32_t*)dev->codes.p,
                                          dirs, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w,
-                                         rot ? rot + 9 * k0 : nullptr, gb + k0 * per, kn, sc, d_gbub, d_gpar);
+                                         rot ? rot + 9 * k0 : nullptr, gb + k0 * per, kn, sc, mt, tt, d_gbub,
+                                         d_gpar);
     }
     CUDA_OK(cudaEventRecord(dev->ev[5], dev->stream));
     CUDA_OK(cudaMemcpyAsync(g_bub, d_gbub, 4 * job.n_tot * sizeof(double), cudaMemcpyDeviceToHost, dev->stream));

@@ -19,6 +19,19 @@ H = 1e-6
 FD_TOL = 1e-5
 
 
+def central_fd(fun, h=H):
+    """Central difference at h, and whether it is free of a kink within 2h.
+
+    The spectrum is piecewise smooth: a patch's collision status flips where
+    dt_k crosses its delay tau, and the first collider changes where two
+    bubbles' walls arrive together.  Across such a point the derivative jumps;
+    a central difference that straddles one measures an average slope.  A
+    difference at h that disagrees with the one at 2h marks such a point."""
+    d1 = (fun(h) - fun(-h)) / (2 * h)
+    d2 = (fun(2 * h) - fun(-2 * h)) / (4 * h)
+    return d1, abs(d1 - d2) <= 1e-6 * max(abs(d1), abs(d2), 1e-300)
+
+
 def small_case(seed=3, n=4):
     inter, ext = W.uniform_config(n, 1.0, 0.2, seed=seed)
     return dict(inter=inter, ext=ext, n_cos=8, n_phi=9, n_t=24, w=np.geomspace(1, 60, 5), kh=W.fibonacci_khat(2))
@@ -51,13 +64,19 @@ def test_oracle_adjoint_vs_finite_differences(damping):
             args_m = (m, po) if name == "co" else (co, m)
             fd = (oracle_loss(c, c["inter"], *args_p, G, damping) - oracle_loss(c, c["inter"], *args_m, G, damping)) / (2 * H)
             assert abs(fd - an[idx]) <= FD_TOL * abs(fd), (name, idx, fd, an[idx])
+    checked = 0
     for a in range(n):
         for q in range(4):
-            p, m = c["inter"].copy(), c["inter"].copy()
-            p[a, q] += H
-            m[a, q] -= H
-            fd = (oracle_loss(c, p, co, po, G, damping) - oracle_loss(c, m, co, po, G, damping)) / (2 * H)
+            def fun(h, a=a, q=q):
+                x = c["inter"].copy()
+                x[a, q] += h
+                return oracle_loss(c, x, co, po, G, damping)
+            fd, smooth = central_fd(fun)
+            if not smooth:
+                continue
+            checked += 1
             assert abs(fd - gi[a, q]) <= FD_TOL * max(abs(fd), 1e-3 * np.abs(gi).max()), (a, q, fd, gi[a, q])
+    assert checked >= 12
 
 
 def test_fit_parametrisation_and_loss():
@@ -135,9 +154,15 @@ def test_autograd_vs_finite_differences(gpu_available):
         assert abs(fd - an) <= FD_TOL * abs(fd), (name, fd, an)
     gx = x.grad.numpy()
     scale = np.abs(gx).max()
-    for a, q in [(0, 0), (1, 1), (2, 2), (3, 3), (5, 0), (7, 3)]:
-        xp, xm = x.detach().clone(), x.detach().clone()
-        xp[a, q] += H
-        xm[a, q] -= H
-        fd = (f(xx=xp) - f(xx=xm)) / (2 * H)
+    checked = 0
+    for a, q in [(0, 0), (1, 1), (2, 2), (3, 3), (4, 1), (5, 0), (6, 2), (7, 3)]:
+        def fun(h, a=a, q=q):
+            xx = x.detach().clone()
+            xx[a, q] += h
+            return f(xx=xx)
+        fd, smooth = central_fd(fun)
+        if not smooth:
+            continue
+        checked += 1
         assert abs(fd - gx[a, q]) <= FD_TOL * max(abs(fd), 1e-2 * scale), (a, q, fd, gx[a, q])
+    assert checked >= 5
