@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(_HERE, "libbubble_gw_c.so")
 # BgwStatus (include/bubble_gw.h)
 OK, NULL_POINTER, INVALID_ARGUMENT, CALCULATION_ERROR, PANIC = 0, 1, 2, 3, 4
 # BgwxKernel
-KERNEL_FP64_DIRECT, KERNEL_FP64_FACTORED, KERNEL_MIXED = 0, 1, 2
+KERNEL_FP64_DIRECT, KERNEL_FP64_FACTORED, KERNEL_MIXED, KERNEL_MIXED_SIMT = 0, 1, 2, 3
 # BgwxLatticeKind / BgwxBoundaryCondition
 LATTICE_PARALLELEPIPED, LATTICE_CARTESIAN, LATTICE_SPHERICAL, LATTICE_EMPTY = 0, 1, 2, 3
 BC_PERIODIC, BC_REFLECTION, BC_NONE = 0, 1, 2

@@ -92,7 +92,7 @@ class BulkFlowSpectrum:
         self._h = h
         _call(L.lib().bgw_generalized_bulk_flow_set_resolution(h, self.n_cos, self.n_phi, True))
         k = {"fp64_direct": L.KERNEL_FP64_DIRECT, "fp64_factored": L.KERNEL_FP64_FACTORED,
-             "mixed": L.KERNEL_MIXED}[kernel]
+             "mixed": L.KERNEL_MIXED, "mixed_simt": L.KERNEL_MIXED_SIMT}[kernel]
         _call(L.lib().bgwx_generalized_bulk_flow_set_kernel(h, k))
         self.last_forward_ms = 0.0
         self.last_backward_ms = 0.0

@@ -550,7 +550,8 @@ BgwStatus bgwx_generalized_bulk_flow_set_stream(bgw_generalized_bulk_flow* bulk_
 BgwStatus bgwx_generalized_bulk_flow_set_kernel(bgw_generalized_bulk_flow* bulk_flow, BgwxKernel kernel) {
     return run_ffi([&] {
         auto* h = handle(bulk_flow);
-        if (kernel != BGWX_KERNEL_FP64_DIRECT && kernel != BGWX_KERNEL_FP64_FACTORED && kernel != BGWX_KERNEL_MIXED)
+        if (kernel != BGWX_KERNEL_FP64_DIRECT && kernel != BGWX_KERNEL_FP64_FACTORED && kernel != BGWX_KERNEL_MIXED &&
+            kernel != BGWX_KERNEL_MIXED_SIMT)
             throw Error{"unknown kernel " + std::to_string((int)kernel)};
         h->kernel = kernel;
     });

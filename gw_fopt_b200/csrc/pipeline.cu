@@ -511,9 +511,11 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
         return;
     }
     CUDA_OK(cudaMemcpyAsync(out, final_out, K * per * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
-    unsigned long long fbk = 0;
-    CUDA_OK(cudaMemcpyAsync(&fbk, dev->counters.p, sizeof fbk, cudaMemcpyDeviceToHost, dev->stream));
+    unsigned long long cnt[2] = {0, 0};
+    CUDA_OK(cudaMemcpyAsync(cnt, dev->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, dev->stream));
     CUDA_OK(cudaStreamSynchronize(dev->stream));
+    const unsigned long long fbk = cnt[0];
+    if (cnt[1] != 0) throw Error{"tensor-core GEMM: a pipeline wait gave up; the result is invalid"};
     float total = 0, ms_masks = 0, ms_spec = 0;
     CUDA_OK(cudaEventElapsedTime(&total, dev->ev[4], dev->ev[5]));
     float ms_beta = 0, ms_gemm = 0;

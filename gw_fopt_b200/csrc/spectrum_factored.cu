@@ -44,6 +44,7 @@
 #include "bgw_internal.h"
 #include "device_common.cuh"
 #include "spectrum_factored.cuh"
+#include "spectrum_tc.cuh"
 
 namespace bgw {
 
@@ -344,32 +345,6 @@ struct FactArgs {
     int tiles_per_frame;
     double2* partial;      // (kn, tiles_per_frame, 2, S, W)
 };
-
-// sin/cos of an FP64 argument: FP64 kernel uses sincos; the mixed kernel
-// reduces the argument modulo 2 pi in FP64 and evaluates sincosf on the
-// reduced FP32 argument.
-template <class Real>
-__device__ __forceinline__ void phase(double arg, double& s, double& c);
-
-template <>
-__device__ __forceinline__ void phase<double>(double arg, double& s, double& c) {
-    sincos(arg, &s, &c);
-}
-
-template <>
-__device__ __forceinline__ void phase<float>(double arg, double& s, double& c) {
-    // Cody & Waite (1980) additive reduction with 2 pi = C1 + C2; the fused
-    // multiply-add forms n*C1 exactly, so one constant pair suffices.
-    const double inv2pi = 0.15915494309189535;
-    const double C1 = 6.283185307179586;      // 2 pi rounded to double
-    const double C2 = 2.4492935982947064e-16;  // 2 pi - C1
-    const double n = rint(arg * inv2pi);
-    const double r = fma(-n, C2, fma(-n, C1, arg));
-    float sf, cf;
-    sincosf((float)r, &sf, &cf);
-    s = sf;
-    c = cf;
-}
 
 // One CTA per (64-frequency tile, column tile), looping over the rows i.
 // Thread (ty, tx) of 16 x 16 owns rows ty*8 .. ty*8+7 (frequencies ty*4 .. +3,
@@ -757,6 +732,37 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     const size_t per = (size_t)2 * S * n_w;
     dev->fact_partial.ensure((size_t)kn * G.tiles_per_frame * per * sizeof(double2));
     A.partial = (double2*)dev->fact_partial.p;
+    if (sizeof(Real) == 4 && job.kernel == BGWX_KERNEL_MIXED) {
+        TcArgs T;
+        T.bub = bub_frames;
+        T.n_tot = job.n_tot;
+        T.sel = sel;
+        T.n_sel = n_sel;
+        T.n_cos = n_cos;
+        T.n_t = n_t;
+        T.n_w = n_w;
+        T.S = S;
+        T.t_arr = t_arr;
+        T.w = w;
+        T.cos_t = cos_t;
+        T.kfirst = (const int*)dev->fact_kfirst.p;
+        T.beta = (const float*)dev->beta.p;
+        T.cols_pad = G.cols_pad;
+        T.t_pad = G.t_pad;
+        T.dt = job.dt;
+        T.bpt = G.bpt;
+        T.tiles_per_frame = G.tiles_per_frame;
+        T.partial = A.partial;
+        T.err = reinterpret_cast<unsigned int*>(static_cast<unsigned char*>(dev->counters.p) + 8);
+        launch_gemm_tc(T, kn, dev->stream);
+        ++launches;
+        CUDA_OK(cudaEventRecord(ev3[2], dev->stream));
+        dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
+        k_reduce_tiles<<<gr, 256, 0, dev->stream>>>(A.partial, G.tiles_per_frame, per, (int)kn, out);
+        CUDA_OK(cudaGetLastError());
+        ++launches;
+        return launches;
+    }
     constexpr int TN = gemm_tn<Real>();
     const size_t smem = gemm_smem_bytes<Real, TN>(S);
     if (smem > 227 * 1024) throw Error{"too many coefficient sets for the factored kernel's shared memory"};
@@ -779,7 +785,7 @@ uint64_t launch_factored(Device* dev, const SpectrumJob& job, const D4* bub_fram
                          const double* tau, const double* cos_t, const double* sin2, const double* cos2,
                          const double* coeffs, const double* powers, const double* t_arr, const double* cutw,
                          const double* w, size_t kn, double2* out, cudaEvent_t* ev3) {
-    if (job.kernel == BGWX_KERNEL_MIXED)
+    if (job.kernel == BGWX_KERNEL_MIXED || job.kernel == BGWX_KERNEL_MIXED_SIMT)
         return launch_typed<float>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w,
                                    kn, out, ev3);
     return launch_typed<double>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, kn,
@@ -787,7 +793,8 @@ uint64_t launch_factored(Device* dev, const SpectrumJob& job, const D4* bub_fram
 }
 
 size_t factored_bytes_per_frame(const SpectrumJob& job) {
-    const size_t real = job.kernel == BGWX_KERNEL_MIXED ? sizeof(float) : sizeof(double);
+    const size_t real =
+        (job.kernel == BGWX_KERNEL_MIXED || job.kernel == BGWX_KERNEL_MIXED_SIMT) ? sizeof(float) : sizeof(double);
     const FactGeom G = fact_geom(job, real);
     return (size_t)job.n_cos * G.cols_pad * G.t_pad * real +
            (size_t)G.tiles_per_frame * 2 * job.n_sets * job.n_w * sizeof(double2);

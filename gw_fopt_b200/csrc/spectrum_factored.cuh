@@ -5,6 +5,33 @@
 
 namespace bgw {
 
+// sin/cos of an FP64 argument: FP64 kernel uses sincos; the mixed kernel
+// reduces the argument modulo 2 pi in FP64 and evaluates sincosf on the
+// reduced FP32 argument.
+template <class Real>
+__device__ __forceinline__ void phase(double arg, double& s, double& c);
+
+template <>
+__device__ __forceinline__ void phase<double>(double arg, double& s, double& c) {
+    sincos(arg, &s, &c);
+}
+
+template <>
+__device__ __forceinline__ void phase<float>(double arg, double& s, double& c) {
+    // Cody & Waite (1980) additive reduction with 2 pi = C1 + C2; the fused
+    // multiply-add forms n*C1 exactly, so one constant pair suffices.
+    const double inv2pi = 0.15915494309189535;
+    const double C1 = 6.283185307179586;      // 2 pi rounded to double
+    const double C2 = 2.4492935982947064e-16;  // 2 pi - C1
+    const double n = rint(arg * inv2pi);
+    const double r = fma(-n, C2, fma(-n, C1, arg));
+    float sf, cf;
+    sincosf((float)r, &sf, &cf);
+    s = sf;
+    c = cf;
+}
+
+
 // Launches the factored spectrum for kn frames whose masks are in `tau`;
 // writes (kn, 2, S, W) complex sums into out.  Returns the number of kernel
 // launches.

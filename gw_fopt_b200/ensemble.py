@@ -94,7 +94,7 @@ class BulkFlowEnsemble:
     def set_kernel(self, kernel: str) -> None:
         """'fp64_direct', 'fp64_factored' or 'mixed'."""
         k = {"fp64_direct": L.KERNEL_FP64_DIRECT, "fp64_factored": L.KERNEL_FP64_FACTORED,
-             "mixed": L.KERNEL_MIXED}[kernel]
+             "mixed": L.KERNEL_MIXED, "mixed_simt": L.KERNEL_MIXED_SIMT}[kernel]
         _call(L.lib().bgwx_generalized_bulk_flow_set_kernel(self._h, k))
 
     def compute_c_integral_khat(self, w_arr, khat, *, t_begin=None, t_end, n_t,

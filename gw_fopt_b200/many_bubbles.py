@@ -539,7 +539,7 @@ class GeneralizedBulkFlow:
     def set_kernel(self, kernel: str) -> None:
         """Selects the spectrum kernel: 'fp64_direct', 'fp64_factored' or 'mixed' (B200 extension)."""
         k = {"fp64_direct": L.KERNEL_FP64_DIRECT, "fp64_factored": L.KERNEL_FP64_FACTORED,
-             "mixed": L.KERNEL_MIXED}[kernel]
+             "mixed": L.KERNEL_MIXED, "mixed_simt": L.KERNEL_MIXED_SIMT}[kernel]
         _call(L.lib().bgwx_generalized_bulk_flow_set_kernel(self._h, k))
 
     # --- geometry -------------------------------------------------------------

@@ -38,11 +38,15 @@ typedef enum BgwxBoundaryCondition {
  * (bubble, cos-theta row, t, w), as the reference's loop nest.
  * FP64_FACTORED: FP64 with the time phase shared across bubbles (register
  * tiled).  MIXED: FP64 phase arguments with range reduction and FP64 final
- * sums, FP32 sincos/weights/compensated partial sums. */
+ * sums, FP32 operands; the time-phase product runs on the tensor cores
+ * (TF32 split in three products, FP32 accumulation per cos-theta row).
+ * MIXED_SIMT: the same mixed form with the product on the FP32 CUDA cores
+ * and FP32 partial sums folded into FP64 every 16 steps. */
 typedef enum BgwxKernel {
     BGWX_KERNEL_FP64_DIRECT = 0,
     BGWX_KERNEL_FP64_FACTORED = 1,
     BGWX_KERNEL_MIXED = 2,
+    BGWX_KERNEL_MIXED_SIMT = 3,
 } BgwxKernel;
 
 /* Per-call device timings (milliseconds, CUDA events on the handle's stream). */

@@ -22,8 +22,8 @@ pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-12
 MIXED_TOL = 1e-6
-KERNELS = ["fp64_direct", "fp64_factored", "mixed"]
-TOL = {"fp64_direct": FP64_TOL, "fp64_factored": FP64_TOL, "mixed": MIXED_TOL}
+KERNELS = ["fp64_direct", "fp64_factored", "mixed", "mixed_simt"]
+TOL = {"fp64_direct": FP64_TOL, "fp64_factored": FP64_TOL, "mixed": MIXED_TOL, "mixed_simt": MIXED_TOL}
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_small.npz")
 
 
