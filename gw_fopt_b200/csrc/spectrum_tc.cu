@@ -14,9 +14,10 @@
 // per row the K dimension is the time steps from the tile's first active
 // block of 32 steps on.  Warp roles (13 warps):
 //   0-3   A producers: thread = tensor-memory lane = GEMM row (w, Re|Im).  The
-//         time phase advances by an FP64 complex recurrence z <- z e^{i w'dt}
-//         from an FP64 sincos at the row's first step; the FP32 value is split
-//         and stored to tensor memory (tcgen05.st), 32 steps per stage.
+//         time phase of step 32 kb + n is z_kb P_n: the block anchor z_kb
+//         advances by an FP64 complex recurrence from an FP64 sincos at the
+//         row's first block, P_n = e^{i w' n dt} is a per-row FP32 table; the
+//         FP32 value is split and stored to tensor memory (tcgen05.st).
 //   4-7   B producers: beta (FP32, HBM) -> split -> shared memory in the
 //         K-major 128-byte-swizzled layout, 32 steps per stage.
 //   8-11  epilogue: thread = lane.  Per row the phases e^{i w (t_a c_i - z_a)}
@@ -57,6 +58,7 @@ constexpr int kTcWarps = 13;
 constexpr int kTcThreads = 32 * kTcWarps;
 constexpr uint32_t kTmemCols = 512;
 constexpr int kBTileBytes = kTcCols * kTcKB * 4;  // 16 KB per (stage, hi|lo)
+constexpr int kEStride = 66;     // phase-table row (one frequency, 64 bubbles) padded against bank conflicts
 
 struct SmemLayout {
     static constexpr int b_hi = 0;
@@ -68,8 +70,9 @@ struct SmemLayout {
     static constexpr int binfo = tslot + 16;                  // int[64]
     static constexpr int bt = binfo + 64 * 4;                 // double[64]
     static constexpr int bz = bt + 64 * 8;                    // double[64]
-    static constexpr int etab = bz + 64 * 8;                  // float2[64 bubbles][64 w]
-    static constexpr int total = etab + 64 * 64 * 8;
+    static constexpr int etab = bz + 64 * 8;                  // float2[64 w][kEStride] (bubbles)
+    static constexpr int ptab = etab + 64 * 66 * 8;           // float2[32 steps][64 w]
+    static constexpr int total = ptab + 32 * 64 * 8;
 };
 
 __device__ __forceinline__ uint32_t swz128(int n, int c) {
@@ -122,7 +125,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
         *abort_flag = 0;
         tc::mbar_fence_init();
     }
-    if (warp == 12) {
+    if (warp == kTcWarps - 1) {
         tc::tmem_alloc(tslot, kTmemCols);
         tc::tmem_relinquish();
     }
@@ -147,32 +150,53 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
         const int wi = w0 + wl;
         const bool wok = wi < A.n_w;
         const uint32_t lanebase = (uint32_t)(32 * warp) << 16;
+        float2* ptab = reinterpret_cast<float2*>(sm + SmemLayout::ptab);
         int it = 0;
         for (int i = 0; active && i < A.n_cos && !failed; ++i) {
-            const double om = wok ? A.w[wi] * (1.0 - A.cos_t[i]) : 0.0;
+            // M[w, k] = z_kb P_n, k = 32 kb + n: the block anchor z_kb = e^{i w' t_k}
+            // advances in FP64 by e^{i w' 32 dt}; P_n = e^{i w' n dt} (FP32 table,
+            // each warp fills the entries of its own 16 frequencies).
+            const double om1 = 1.0 - A.cos_t[i];
+            __syncwarp();
+            for (int q = lane; q < 32 * 16; q += 32) {
+                const int n = q >> 4, l = 16 * warp + (q & 15);
+                const double oml = (w0 + l < A.n_w) ? A.w[w0 + l] * om1 : 0.0;
+                double sn, cs;
+                sincos(oml * (n * A.dt), &sn, &cs);
+                ptab[n * kTcWT + l] = make_float2((float)cs, (float)sn);
+            }
+            __syncwarp();
+            const double om = wok ? A.w[wi] * om1 : 0.0;
             double zr, zi, sr, si;
             sincos(om * A.t_arr[kb0 * kTcKB], &zi, &zr);
-            sincos(om * A.dt, &si, &sr);
+            sincos(om * (kTcKB * A.dt), &si, &sr);
             for (int kb = kb0; kb < nkb; ++kb, ++it) {
-                uint32_t hi[32], lo[32];
-#pragma unroll
-                for (int n = 0; n < 32; ++n) {
-                    const int k = kb * kTcKB + n;
-                    const float v = (k < A.n_t) ? (float)(part ? zi : zr) : 0.0f;
-                    tc::split_tf32(v, hi[n], lo[n]);
-                    const double nr = fma(zr, sr, -zi * si);
-                    const double ni = fma(zr, si, zi * sr);
-                    zr = nr;
-                    zi = ni;
-                }
+                const float ar = (float)zr, ai = (float)zi;
+                const bool tail = (kb + 1) * kTcKB > A.n_t;
+                const double nr = fma(zr, sr, -zi * si);
+                const double ni = fma(zr, si, zi * sr);
+                zr = nr;
+                zi = ni;
                 const int st = it % kTcStages;
                 if (!tc::warp_wait_bounded(&empty[st], ((it / kTcStages) & 1) ^ 1, abort_flag)) {
                     failed = true;
                     break;
                 }
                 const uint32_t acol = tbase + 256 + 64 * st;
-                tc::tmem_st32(acol | lanebase, hi);
-                tc::tmem_st32((acol + 32) | lanebase, lo);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {  // 16 steps at a time
+                    uint32_t hi[16], lo[16];
+#pragma unroll
+                    for (int n = 0; n < 16; ++n) {
+                        const int nn = 16 * h + n;
+                        const float2 p = ptab[nn * kTcWT + wl];
+                        float v = part ? fmaf(ar, p.y, ai * p.x) : fmaf(ar, p.x, -ai * p.y);
+                        if (tail && kb * kTcKB + nn >= A.n_t) v = 0.0f;
+                        tc::split_tf32_fast(v, hi[n], lo[n]);
+                    }
+                    tc::tmem_st16((acol + 16 * h) | lanebase, hi);
+                    tc::tmem_st16((acol + 32 + 16 * h) | lanebase, lo);
+                }
                 tc::tmem_wait_st();
                 tc::tc_fence_before();
                 __syncwarp();
@@ -188,17 +212,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
             const float* brow = beta + (((size_t)frame * A.n_cos + i) * A.cols_pad + col0) * A.t_pad;
             for (int kb = kb0; kb < nkb; ++kb, ++it) {
                 float4 v[8];
+                const bool tail = (kb + 1) * kTcKB > A.n_t;
 #pragma unroll
                 for (int u = 0; u < 8; ++u) {
                     const int q = tb + 128 * u;
                     const int n = q >> 3, c = q & 7;
                     const int k = kb * kTcKB + 4 * c;
                     float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (k < A.t_pad) x = __ldg(reinterpret_cast<const float4*>(brow + (size_t)n * A.t_pad + k));
-                    if (k + 0 >= A.n_t) x.x = 0.f;
-                    if (k + 1 >= A.n_t) x.y = 0.f;
-                    if (k + 2 >= A.n_t) x.z = 0.f;
-                    if (k + 3 >= A.n_t) x.w = 0.f;
+                    if (!tail) {
+                        x = __ldg(reinterpret_cast<const float4*>(brow + (size_t)n * A.t_pad + k));
+                    } else {
+                        if (k < A.t_pad) x = __ldg(reinterpret_cast<const float4*>(brow + (size_t)n * A.t_pad + k));
+                        if (k + 0 >= A.n_t) x.x = 0.f;
+                        if (k + 1 >= A.n_t) x.y = 0.f;
+                        if (k + 2 >= A.n_t) x.z = 0.f;
+                        if (k + 3 >= A.n_t) x.w = 0.f;
+                    }
                     v[u] = x;
                 }
                 const int st = it % kTcStages;
@@ -213,10 +242,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
                     const int q = tb + 128 * u;
                     const int n = q >> 3, c = q & 7;
                     uint4 h, l;
-                    tc::split_tf32(v[u].x, h.x, l.x);
-                    tc::split_tf32(v[u].y, h.y, l.y);
-                    tc::split_tf32(v[u].z, h.z, l.z);
-                    tc::split_tf32(v[u].w, h.w, l.w);
+                    tc::split_tf32_fast(v[u].x, h.x, l.x);
+                    tc::split_tf32_fast(v[u].y, h.y, l.y);
+                    tc::split_tf32_fast(v[u].z, h.z, l.z);
+                    tc::split_tf32_fast(v[u].w, h.w, l.w);
                     const uint32_t off = swz128(n, c);
                     *reinterpret_cast<uint4*>(bh + off) = h;
                     *reinterpret_cast<uint4*>(bl + off) = l;
@@ -231,33 +260,41 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
         // Tensor-core FP32 accumulation rounds each addition into a growing
         // sum, so the accumulator is handed over every kTcFoldKB blocks of 32
         // steps and its contribution, phase included (the phase is constant
-        // along a row), is added to FP64 sums per (w, set, +/x).
+        // along a row), is added to FP64 sums per (w, set, +/x).  Each lane
+        // holds one GEMM row, Re (even lane) or Im (odd lane) of its
+        // frequency, and accumulates sum_b cos_b Y_b and sum_b sin_b Y_b of
+        // that row; Re C = sum cos Yr - sum sin Yi and Im C = sum cos Yi +
+        // sum sin Yr are formed once at the end.  Products are summed in FP32
+        // over the bubbles of a 32-column chunk (two interleaved chains), then
+        // added to the FP64 sums.
         const int q4 = warp - 8;
         const int r = 32 * q4 + lane;
         const int wl = r >> 1, part = r & 1;
         const int wi = w0 + wl;
         const uint32_t lanebase = (uint32_t)(32 * q4) << 16;
         float2* etab = reinterpret_cast<float2*>(sm + SmemLayout::etab);
-        double acc[CPB];
+        double accC[CPB], accS[CPB];
 #pragma unroll
-        for (int c = 0; c < CPB; ++c) acc[c] = 0.0;
+        for (int c = 0; c < CPB; ++c) accC[c] = accS[c] = 0.0;
         int seg = 0;
         for (int i = 0; active && i < A.n_cos && !failed; ++i) {
-            // e^{i w (t_a c_i - z_a)} per (bubble, w) of this row; zero for empty columns
-            // (each warp fills and reads only the entries of its own 16 frequencies)
+            // e^{i w (t_a c_i - z_a)} per (w, bubble) of this row; zero for empty
+            // columns (each warp fills and reads only its own 16 frequencies)
             const double ci = A.cos_t[i];
             __syncwarp();
+#pragma unroll 4
             for (int q = lane; q < 64 * 16; q += 32) {
-                const int b = q >> 4, l = 16 * q4 + (q & 15);
+                const int b = q & 63, l = 16 * q4 + (q >> 6);
                 float2 e = make_float2(0.f, 0.f);
                 if (b < A.bpt && binfo[b] >= 0 && w0 + l < A.n_w) {
                     double sn, cs;
                     phase<float>(A.w[w0 + l] * (bt[b] * ci - bz[b]), sn, cs);
                     e = make_float2((float)cs, (float)sn);
                 }
-                etab[b * kTcWT + l] = e;
+                etab[l * kEStride + b] = e;
             }
             __syncwarp();
+            const float2* erow = etab + wl * kEStride;
             const int nseg = (nkb - kb0 + kTcFoldKB - 1) / kTcFoldKB;
             for (int g = 0; g < nseg; ++g, ++seg) {
                 const int buf = seg & 1;
@@ -266,40 +303,56 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
                     break;
                 }
                 tc::tc_fence_after();
-                float cs = 0.f, ssn = 0.f;
+                // columns [n0, n0 + 32) from y; the chunk's phases are loaded first
+                auto consume = [&](const uint32_t (&y)[32], const int n0) {
+                    constexpr int NB = 32 / CPB + 2;
+                    const int b_first = n0 / CPB;
+                    float2 ev[NB];
+#pragma unroll
+                    for (int j = 0; j < NB; ++j)
+                        if (b_first + j <= (n0 + 31) / CPB) ev[j] = erow[b_first + j];
+                    float pc[2][CPB], ps[2][CPB];
+#pragma unroll
+                    for (int c = 0; c < CPB; ++c) pc[0][c] = ps[0][c] = pc[1][c] = ps[1][c] = 0.f;
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) {
+                        const int n = n0 + c;
+                        const int b = n / CPB, sc = n % CPB, h2 = b & 1;
+                        const float2 e = ev[b - b_first];
+                        const float yv = __uint_as_float(y[c]);
+                        pc[h2][sc] = fmaf(e.x, yv, pc[h2][sc]);
+                        ps[h2][sc] = fmaf(e.y, yv, ps[h2][sc]);
+                    }
+#pragma unroll
+                    for (int q = 0; q < CPB; ++q) {
+                        accC[q] += (double)(pc[0][q] + pc[1][q]);
+                        accS[q] += (double)(ps[0][q] + ps[1][q]);
+                    }
+                };
+                const uint32_t dcol = (tbase + 128 * buf) | lanebase;
 #pragma unroll
                 for (int ch = 0; ch < kTcCols / 32; ++ch) {
                     uint32_t y[32];
-                    tc::tmem_ld32((tbase + 128 * buf + 32 * ch) | lanebase, y);
+                    tc::tmem_ld32(dcol + 32 * ch, y);
                     tc::tmem_wait_ld();
-#pragma unroll
-                    for (int c = 0; c < 32; ++c) {
-                        const int n = 32 * ch + c;
-                        const int b = n / CPB, sc = n % CPB;
-                        const float yv = __uint_as_float(y[c]);
-                        const float yp = __shfl_xor_sync(0xffffffffu, yv, 1);
-                        if (sc == 0 || c == 0) {
-                            const float2 e = etab[b * kTcWT + wl];
-                            cs = e.x;
-                            ssn = part ? e.y : -e.y;
-                        }
-                        // Re (even lane): cs yr - sn yi; Im (odd lane): cs yi + sn yr
-                        acc[sc] += (double)fmaf(ssn, yp, cs * yv);
+                    if (ch == kTcCols / 32 - 1) {  // every column is in registers: release the buffer
+                        tc::tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) tc::mbar_arrive(&acce[buf]);
                     }
+                    consume(y, 32 * ch);
                 }
-                tc::tc_fence_before();
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&acce[buf]);
             }
         }
-        // (Re from even lanes, Im from odd lanes) -> partial sums of this tile
+        // even lane: (sum cos Yr, sum sin Yr); odd lane: (sum cos Yi, sum sin Yi)
 #pragma unroll
         for (int sg = 0; sg < CPB; ++sg) {
-            const double other = __shfl_xor_sync(0xffffffffu, acc[sg], 1);
+            const double oc = __shfl_xor_sync(0xffffffffu, accC[sg], 1);
+            const double os = __shfl_xor_sync(0xffffffffu, accS[sg], 1);
             if (part == 0 && wi < A.n_w) {
                 const int s_ = sg >> 1, g = sg & 1;
                 const size_t o = ((((size_t)frame * A.tiles_per_frame + tile) * 2 + g) * S + s_) * A.n_w + wi;
-                A.partial[o] = make_double2(acc[sg], other);
+                A.partial[o] = make_double2(accC[sg] - os, oc + accS[sg]);
             }
         }
     } else {
@@ -355,7 +408,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == 12) {
+    if (warp == kTcWarps - 1) {
         tc::tc_fence_after();
         tc::tmem_dealloc(tbase, kTmemCols);
     }
