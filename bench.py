@@ -46,7 +46,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--config", type=int, default=3)
-    ap.add_argument("--kernel", default="mixed", choices=["fp64_direct", "fp64_factored", "mixed"])
+    ap.add_argument("--kernel", default="mixed", choices=["fp64_direct", "fp64_factored", "mixed", "mixed_simt"])
     ap.add_argument("--no-compare", action="store_true", help="skip the FP64 comparison measurements")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -149,7 +149,7 @@ def compare_fp64(cfg, kernel, res, lib, L):
     t = g.last_timings()
     pte = sub * cfg.n * cfg.n_cos * cfg.n_phi * cfg.n_t
     out["fp64_factored"] = {"value": pte / (t["total_ms"] * 1e-3), "unit": UNIT, "sample": f"{sub} of {cfg.khat.shape[0]} k-hat"}
-    if kernel == "mixed":
+    if kernel.startswith("mixed"):
         got = res[:sub]
         d = (got - ref).reshape(-1, ref.shape[-1])
         r = ref.reshape(-1, ref.shape[-1])
@@ -284,14 +284,7 @@ def run_b200(args):
     L.check(lib.bgwx_measure_compute_peaks(C.byref(p64), C.byref(p32), C.byref(psfu)))
     peaks = {"fp64_tflops": p64.value / 1e12, "fp32_tflops": p32.value / 1e12, "sfu_tops": psfu.value / 1e12}
     spec_s = tm["spectrum_ms"] * 1e-3
-    peak = (p32.value if args.kernel == "mixed" else p64.value) / 1e12
-    bound = "fp32" if args.kernel == "mixed" else "fp64"
-    achieved = cfg.counted_flops / spec_s / 1e12 if spec_s > 0 else None
-    gemm = None
-    if args.kernel != "fp64_direct" and tm["gemm_ms"] > 0:
-        gemm_flops = 2.0 * (2 * Wn) * cfg.n_t * (cfg.n * 2 * S) * cfg.n_cos * K
-        gemm = {"kernel": "k_gemm", "ms_per_step": tm["gemm_ms"], "executed_tflops": gemm_flops / (tm["gemm_ms"] * 1e-3) / 1e12,
-                "frac_of_peak": gemm_flops / (tm["gemm_ms"] * 1e-3) / 1e12 / peak, "beta_ms_per_step": tm["beta_ms"]}
+    counted = cfg.counted_flops / spec_s / 1e12 if spec_s > 0 else None
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
@@ -299,21 +292,45 @@ def run_b200(args):
             traffic = json.load(open(tpath)).get(f"config{args.config}:{args.kernel}")
         except Exception:
             traffic = None
-    roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "kernel": f"spectrum stage ({args.kernel}): k_time_tables + k_beta + k_gemm + k_reduce_tiles"
-                          if args.kernel != "fp64_direct" else "k_spec_direct + k_reduce",
-                "work": "counted F = 6 PTE + 8 Phi + 20 Phi_t per step",
-                "spectrum_ms": tm["spectrum_ms"], "masks_ms": tm["masks_ms"], "dominant_gemm": gemm,
-                "peak_source": "measured on this GPU (bgwx_measure_compute_peaks: FMA chains, of measured); "
-                               "MEASURED_PEAKS.json holds HBM/bf16 only", "peaks": peaks}
+    # the time-phase product: 2 (2W) n_t columns n_cos flops per frame
+    gemm_flops = 2.0 * (2 * Wn) * cfg.n_t * (cfg.n * 2 * S) * cfg.n_cos * K
+    stage = {"work": "counted F = 6 PTE + 8 Phi + 20 Phi_t per step", "achieved_counted_tflops": counted,
+             "spectrum_ms": tm["spectrum_ms"], "masks_ms": tm["masks_ms"], "beta_ms": tm["beta_ms"],
+             "gemm_ms": tm["gemm_ms"]}
+    if args.kernel == "mixed" and tm["gemm_ms"] > 0:
+        # k_gemm_tc: three TF32 products per FP32 product on the tensor cores; peak = TF32 dense,
+        # half of the measured bf16 dense figure (sustained: the kernel runs inside a long step)
+        mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+        peak = mp["bf16_tflops_sustained"] / 2.0
+        achieved = 3.0 * gemm_flops / (tm["gemm_ms"] * 1e-3) / 1e12
+        roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": achieved / peak, "traffic": traffic, "kernel": "k_gemm_tc",
+                    "work": "3 x 2 x (2 n_w) x n_t x columns x n_cos TF32 flops per frame (FP32 split in three)",
+                    "peak_source": "of measured: MEASURED_PEAKS.json bf16_tflops_sustained / 2 (TF32 dense)",
+                    "spectrum_stage": stage, "peaks": peaks}
+    else:
+        peak = (p32.value if args.kernel == "mixed_simt" else p64.value) / 1e12
+        bound = "fp32" if args.kernel == "mixed_simt" else "fp64"
+        if args.kernel != "fp64_direct" and tm["gemm_ms"] > 0:
+            achieved = gemm_flops / (tm["gemm_ms"] * 1e-3) / 1e12
+            kname = "k_gemm"
+            work = "2 x (2 n_w) x n_t x columns x n_cos flops per frame"
+        else:
+            achieved = counted
+            kname = "k_spec_direct + k_reduce"
+            work = "counted F = 6 PTE + 8 Phi + 20 Phi_t per step"
+        roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                    "frac": (achieved / peak) if achieved else None, "traffic": traffic, "kernel": kname,
+                    "work": work, "peak_source": "of measured: bgwx_measure_compute_peaks (FMA chains on this GPU); "
+                                                 "MEASURED_PEAKS.json holds HBM/bf16 only",
+                    "spectrum_stage": stage, "peaks": peaks}
 
     compare = None
     if not args.no_compare and world == 1:
         compare = compare_fp64(cfg, args.kernel, res, lib, L)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64" if args.kernel != "mixed" else "f32+f64", "data": "synthetic",
+            "vs_baseline": None, "dtype": "f64" if not args.kernel.startswith("mixed") else ("tf32x3+f64" if args.kernel == "mixed" else "f32+f64"), "data": "synthetic",
             "config": {"workload": cfg.name, "bubbles": int(cfg.n), "colliders": int(cfg.n + cfg.exterior.shape[0]),
                        "n_cos": cfg.n_cos, "n_phi": cfg.n_phi, "n_t": cfg.n_t, "n_w": int(Wn),
                        "n_khat_per_gpu": int(K), "kernel": args.kernel, "pte_per_step": pte_total,
