@@ -50,15 +50,28 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
     return ok != 0;
 }
 
-// Waits for the phase of `bar` with the given parity, giving up after about
-// `limit` polls (with a short sleep between late polls) or as soon as *abort
-// is set by another role of the block.  Returns false when it gave up.
+// try_wait with a suspend-time hint: the thread sleeps in hardware until the
+// phase completes or about `hint_ns` pass, instead of spinning on the issue slots.
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t* bar, uint32_t parity, uint32_t hint_ns) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+
+// Waits for the phase of `bar` with the given parity, giving up after `limit`
+// suspended tries of at most 20 us each (about 1 s) or as soon as *abort is set
+// by another role of the block.  Returns false when it gave up.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, volatile int* abort,
-                                                  uint32_t limit = 1u << 22) {
+                                                  uint32_t limit = 50000) {
     for (uint32_t it = 0; it < limit; ++it) {
-        if (mbar_try_wait(bar, parity)) return true;
+        if (mbar_try_wait_hint(bar, parity, 20000u)) return true;
         if (*abort) return false;
-        if (it > 64) __nanosleep(64);
     }
     return false;
 }
