@@ -181,6 +181,7 @@ def run_b200(args):
     from gw_fopt_b200 import _lib as L
     from gw_fopt_b200 import many_bubbles as mb
     from gw_fopt_b200 import workloads as W
+    from gw_fopt_b200.sharding import khat_shard, max_over_ranks
 
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -194,7 +195,7 @@ def run_b200(args):
 
     cfg = W.config(args.config)
     K = cfg.khat.shape[0]
-    cfg.khat = W.fibonacci_khat(K * world)[rank::world]
+    cfg.khat = khat_shard(K, rank, world)
     g = make_flow(cfg, args.kernel)
     lib = L.lib()
     S, Wn = cfg.coefficients.shape[0], cfg.w.size
@@ -234,11 +235,7 @@ def run_b200(args):
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
-    ms = e0.elapsed_time(e1)
-    if pg is not None:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), device="cuda")
     ms_step = ms / args.steps
     pte_total = cfg.pte * world
     value = pte_total / (ms_step * 1e-3)
@@ -267,11 +264,7 @@ def run_b200(args):
         f1.record(stream)
         torch.cuda.synchronize()
         barrier()
-        ms_e = f0.elapsed_time(f1)
-        if pg is not None:
-            t = torch.tensor([ms_e], device="cuda", dtype=torch.float64)
-            pg.all_reduce(t, op=pg.ReduceOp.MAX)
-            ms_e = float(t.item())
+        ms_e = max_over_ranks(f0.elapsed_time(f1), device="cuda")
         e2e = {"value": pte_total / (ms_e / args.steps * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h), "ms_per_step": ms_e / args.steps}
         assert np.array_equal(host_out, res)
