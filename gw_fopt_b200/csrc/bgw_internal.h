@@ -92,6 +92,12 @@ void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out
 void run_adjoint(Device* dev, const SpectrumJob& job, const double* gbar, double* g_par, double* g_bub,
                  BgwxTimings* timings);
 
+// Time-resolved integrand of the unrotated frame (job.rot ignored): out
+// (2, n_sets, n_w, n_t) complex as interleaved doubles, the sum over the
+// selected bubbles in selection order; job.cutoff must be all ones (the
+// reference applies no time cutoff to the integrand).
+void run_integrand(Device* dev, const SpectrumJob& job, double* out, BgwxTimings* timings);
+
 // Uses `stream` (a cudaStream_t) for all later work; nullptr = own stream.
 void device_set_stream(Device* dev, void* stream);
 

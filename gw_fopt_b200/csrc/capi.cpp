@@ -536,6 +536,62 @@ BgwStatus bgwx_generalized_bulk_flow_set_bubbles(bgw_generalized_bulk_flow* bulk
     });
 }
 
+BgwStatus bgwx_generalized_bulk_flow_compute_c_integrand(bgw_generalized_bulk_flow* bulk_flow, const double* w_arr,
+                                                         size_t n_w, bool has_t_begin, double t_begin, double t_end,
+                                                         size_t n_t, const size_t* selected_bubbles,
+                                                         size_t n_selected_bubbles, BgwComplex64* out,
+                                                         size_t out_len) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        const size_t S = h->n_sets;
+        const size_t expected =
+            checked_mul(checked_mul(checked_mul(2, S, "out"), n_w, "out"), n_t, "out");
+        // generalized_bulk_flow.rs:883-906: n_t, then the selection
+        if (n_t < 2) throw Error{"Invalid resolution: n_t must be >= 2"};
+        std::vector<uint32_t> ids;
+        if (selected_bubbles) {
+            const size_t* sel = slice(selected_bubbles, n_selected_bubbles, "selected_bubbles");
+            for (size_t q = 0; q < n_selected_bubbles; ++q) {
+                if (sel[q] >= h->n_int) {
+                    Error e{"Index " + std::to_string(sel[q]) + " out of bounds for max " + std::to_string(h->n_int)};
+                    e.index_error = true;
+                    throw e;
+                }
+                ids.push_back((uint32_t)sel[q]);
+            }
+        } else {
+            for (size_t a = 0; a < h->n_int; ++a) ids.push_back((uint32_t)a);
+        }
+        if (out_len != expected)
+            throw Error{"out_len=" + std::to_string(out_len) + " does not match expected length " +
+                        std::to_string(expected)};
+        BgwComplex64* o = const_cast<BgwComplex64*>(slice(out, out_len, "out"));
+        for (size_t q = 0; q < expected; ++q) o[q] = BgwComplex64{0.0, 0.0};
+        const double tb = has_t_begin ? t_begin : 0.0;
+        // bubbles nucleating at or after t_end contribute zeros before the range check (:786-797)
+        std::vector<uint32_t> live;
+        for (uint32_t a : ids)
+            if (h->bubbles[4 * (size_t)a] < t_end) live.push_back(a);
+        if (live.empty() || S == 0 || n_w == 0) return;
+        if (tb > t_end)
+            throw Error{"Invalid time range: t_begin=" + bgw::rust_f64(tb) + " > t_end=" + bgw::rust_f64(t_end)};
+        require_resolution(h);
+        const double* w = slice(w_arr, n_w, "w_arr");
+        std::vector<double> t_arr = bgw::linspace(tb, t_end, n_t);
+        std::vector<double> ones(n_t, 1.0);  // no time cutoff on the integrand
+        bgw::SpectrumJob job = settings_job(h, t_arr, ones, w, n_w, nullptr, 1);
+        job.bubbles = h->bubbles.data();
+        job.n_int = h->n_int;
+        job.n_tot = h->n_int + h->n_ext;
+        job.sel = live.data();
+        job.n_sel = live.size();
+        std::vector<double> result(2 * expected);
+        h->timings = BgwxTimings{};
+        bgw::run_integrand(device(h), job, result.data(), &h->timings);
+        for (size_t q = 0; q < expected; ++q) o[q] = BgwComplex64{result[2 * q], result[2 * q + 1]};
+    });
+}
+
 BgwStatus bgwx_generalized_bulk_flow_drop_resident_inputs(bgw_generalized_bulk_flow* bulk_flow) {
     return run_ffi([&] {
         auto* h = handle(bulk_flow);

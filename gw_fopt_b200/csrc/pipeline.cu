@@ -128,7 +128,7 @@ struct SpecArgs {
     double dt;
     const double* w;
     int n_w;
-    double2* partial;  // (K, n_sel, 2, S, W)
+    double2* partial;  // (K, n_sel, 2, S, W); with PER_T: (n_sel, 2, S, W, n_t)
     int tau_in_smem;
 };
 
@@ -143,6 +143,11 @@ __device__ __forceinline__ double unrolled_sum8(const double* p8, double tail) {
     return __dadd_rn(acc, tail);
 }
 
+// PER_T: the time-resolved integrand of compute_c_integrand_fixed_bubble
+// (generalized_bulk_flow.rs:776-866): each step's A e^{i w (t - z_a)} times the
+// trapezoid dt weight and 1/(6 pi), one output per step (no time cutoff),
+// instead of the sum over steps.
+template <bool PER_T>
 __global__ void __launch_bounds__(kSpecThreads) k_spec_direct(SpecArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int k = blockIdx.y;
@@ -269,7 +274,27 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_direct(SpecArgs A) {
                 }
                 __syncthreads();
                 // ---- C stage (GBF:832-851) ----
-                if (wvalid && ig == 0) {
+                if (PER_T && wvalid && ig == 0) {
+                    double sn, cs;
+                    sincos(wv * (t - za), &sn, &cs);
+                    const double dtw = A.dt * ((kt == 0 || kt == A.n_t - 1) ? 0.5 : 1.0);
+                    for (int s = 0; s < sc; ++s) {
+                        for (int g = 0; g < 2; ++g) {
+                            double2 at = make_double2(0.0, 0.0);
+                            for (int q = 0; q < n_ig; ++q) {
+                                const double2 v = red[((size_t)(q * W_eff + wl) * kSetChunk + s) * 2 + g];
+                                at.x += v.x;
+                                at.y += v.y;
+                            }
+                            // (A e^{i w (t - z_a)}) (dt w_t) / (6 pi), GBF:832-840 and 862-863
+                            const double re = (at.x * cs - at.y * sn) * dtw * inv6pi;
+                            const double im = (at.x * sn + at.y * cs) * dtw * inv6pi;
+                            const size_t o = ((((size_t)slot * 2 + g) * A.n_sets + (s0 + s)) * A.n_w + wi) * A.n_t + kt;
+                            A.partial[o] = make_double2(re, im);
+                        }
+                    }
+                }
+                if (!PER_T && wvalid && ig == 0) {
                     double sn, cs;
                     sincos(wv * (t - za), &sn, &cs);
                     const double uw = (kt == 0 || kt == A.n_t - 1) ? 0.5 : 1.0;
@@ -291,7 +316,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_direct(SpecArgs A) {
                 }
                 __syncthreads();
             }
-            if (wvalid && ig == 0) {
+            if (!PER_T && wvalid && ig == 0) {
                 for (int s = 0; s < sc; ++s)
                     for (int g = 0; g < 2; ++g) {
                         size_t o = ((((size_t)k * A.n_sel + slot) * 2 + g) * A.n_sets + (s0 + s)) * A.n_w + wi;
@@ -444,7 +469,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     int tau_in_smem = smem_fixed + smem_tau <= (size_t)max_optin ? 1 : 0;
     size_t smem = smem_fixed + (tau_in_smem ? smem_tau : 0);
     if (smem > (size_t)max_optin) throw Error{"n_cos_thetax too large for the shared-memory layout"};
-    CUDA_OK(cudaFuncSetAttribute(k_spec_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CUDA_OK(cudaFuncSetAttribute(k_spec_direct<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
     uint64_t launches = 0;
     CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
@@ -491,7 +516,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             A.tau_in_smem = tau_in_smem;
             if (job.n_sel > 0x7fffffffULL) throw Error{"too many radiating bubbles"};
             dim3 g((unsigned)job.n_sel, (unsigned)kn);
-            k_spec_direct<<<g, kSpecThreads, smem, dev->stream>>>(A);
+            k_spec_direct<false><<<g, kSpecThreads, smem, dev->stream>>>(A);
             CUDA_OK(cudaGetLastError());
             ++launches;
             dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
@@ -657,6 +682,108 @@ void run_adjoint(Device* dev, const SpectrumJob& job, const double* gbar, double
         tm->launches += launches;
         tm->directions += K * job.n_sel * nd;
         tm->d2h_bytes += (double)((4 * job.n_tot + 2 * SM) * sizeof(double));
+    }
+}
+
+// out += sum over the chunk's bubbles, in slot order, of their per-step values.
+__global__ void k_reduce_integrand(const double2* __restrict__ partial, size_t n, size_t per, double2* __restrict__ out) {
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= per) return;
+    double2 acc = out[q];
+    for (size_t a = 0; a < n; ++a) {
+        const double2 v = partial[a * per + q];
+        acc.x += v.x;
+        acc.y += v.y;
+    }
+    out[q] = acc;
+}
+
+void run_integrand(Device* dev, const SpectrumJob& job, double* out, BgwxTimings* tm) {
+    CUDA_OK(cudaSetDevice(dev->id));
+    const size_t nd = job.n_cos * job.n_phi;
+    const size_t S = job.n_sets, W = job.n_w, T = job.n_t;
+    const size_t per = 2 * S * W * T;  // complex values of one bubble's integrand
+    if (job.n_cos > 4096 || job.n_phi > 65536) throw Error{"angular resolution too large for the GPU kernels"};
+    D4* bub = reinterpret_cast<D4*>(upload(dev, dev->bub, job.bubbles, 4 * job.n_tot, tm));
+    D4* dirs = reinterpret_cast<D4*>(upload(dev, dev->dirs, job.dirs, 4 * nd, tm));
+    double* cos_t = upload(dev, dev->cos_t, job.cos_thetax, job.n_cos, tm);
+    double* sin2 = upload(dev, dev->sin2, job.sin2phi, job.n_phi, tm);
+    double* cos2 = upload(dev, dev->cos2, job.cos2phi, job.n_phi, tm);
+    double* coeffs = upload(dev, dev->coeffs, job.coeffs, S * job.n_terms, tm);
+    double* powers = upload(dev, dev->powers, job.powers, S * job.n_terms, tm);
+    double* t_arr = upload(dev, dev->t_arr, job.t_arr, T, tm);
+    double* cutw = upload(dev, dev->cutw, job.cutoff, T, tm);
+    double* w = upload(dev, dev->w, job.w, W, tm);
+    uint32_t* sel = upload(dev, dev->sel, job.sel, job.n_sel, tm);
+    // bubbles per chunk: bounded by the per-bubble integrand buffer
+    const size_t budget = mask_budget_bytes();
+    size_t chunk = std::max<size_t>(1, std::min(job.n_sel, budget / std::max<size_t>(per * sizeof(double2), 1)));
+    chunk = std::min<size_t>(chunk, 65535);
+    dev->tau.ensure(job.n_sel * nd * sizeof(double));
+    dev->partial.ensure(chunk * per * sizeof(double2));
+    dev->out.ensure(per * sizeof(double2));
+    dev->counters.ensure(64);
+    CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
+    CUDA_OK(cudaMemsetAsync(dev->out.p, 0, per * sizeof(double2), dev->stream));
+    size_t smem = (size_t)job.n_cos * kSetChunk * 2 * sizeof(double) +
+                  (size_t)kSpecThreads * kSetChunk * 2 * sizeof(double2);
+    const size_t smem_tau = ((nd + 1) & ~(size_t)1) * sizeof(double);
+    int max_optin = 0;
+    CUDA_OK(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev->id));
+    const int tau_in_smem = smem + smem_tau <= (size_t)max_optin ? 1 : 0;
+    if (tau_in_smem) smem += smem_tau;
+    if (smem > (size_t)max_optin) throw Error{"n_cos_thetax too large for the shared-memory layout"};
+    CUDA_OK(cudaFuncSetAttribute(k_spec_direct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    uint64_t launches = 0;
+    CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
+    launch_mask_pipeline(dev, bub, bub, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, 1, (double*)dev->tau.p,
+                         nullptr, (unsigned long long*)dev->counters.p, true, &launches);
+    for (size_t s0 = 0; s0 < job.n_sel; s0 += chunk) {
+        const size_t n = std::min(chunk, job.n_sel - s0);
+        CUDA_OK(cudaMemsetAsync(dev->partial.p, 0, n * per * sizeof(double2), dev->stream));
+        SpecArgs A;
+        A.bub = bub;
+        A.n_tot = job.n_tot;
+        A.sel = sel + s0;
+        A.n_sel = n;
+        A.tau = (const double*)dev->tau.p + s0 * nd;
+        A.n_cos = (int)job.n_cos;
+        A.n_phi = (int)job.n_phi;
+        A.cos_thetax = cos_t;
+        A.sin2phi = sin2;
+        A.cos2phi = cos2;
+        A.coeffs = coeffs;
+        A.powers = powers;
+        A.n_sets = (int)S;
+        A.n_terms = (int)job.n_terms;
+        A.has_damping = job.has_damping ? 1 : 0;
+        A.damping = job.damping;
+        A.t_arr = t_arr;
+        A.cutw = cutw;
+        A.n_t = (int)T;
+        A.dt = job.dt;
+        A.w = w;
+        A.n_w = (int)W;
+        A.partial = (double2*)dev->partial.p;
+        A.tau_in_smem = tau_in_smem;
+        k_spec_direct<true><<<dim3((unsigned)n, 1), kSpecThreads, smem, dev->stream>>>(A);
+        CUDA_OK(cudaGetLastError());
+        k_reduce_integrand<<<(unsigned)((per + 255) / 256), 256, 0, dev->stream>>>((const double2*)dev->partial.p, n,
+                                                                                   per, (double2*)dev->out.p);
+        CUDA_OK(cudaGetLastError());
+        launches += 2;
+    }
+    CUDA_OK(cudaEventRecord(dev->ev[5], dev->stream));
+    CUDA_OK(cudaMemcpyAsync(out, dev->out.p, per * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
+    CUDA_OK(cudaStreamSynchronize(dev->stream));
+    float total = 0;
+    CUDA_OK(cudaEventElapsedTime(&total, dev->ev[4], dev->ev[5]));
+    if (tm) {
+        tm->total_ms += total;
+        tm->spectrum_ms += total;
+        tm->launches += launches;
+        tm->directions += job.n_sel * nd;
+        tm->d2h_bytes += (double)(per * sizeof(double2));
     }
 }
 

@@ -683,10 +683,38 @@ class GeneralizedBulkFlow:
         return out
 
     def compute_c_integrand_fixed_bubble(self, a_idx, w_arr, t_begin, t_end, n_t):
-        raise NotImplementedError("compute_c_integrand_fixed_bubble is not built in this library yet")
+        """(2, n_sets, n_w, n_t) complex128: bubble a_idx's time-resolved integrand
+        (generalized_bulk_flow.rs:776-866), computed on the GPU."""
+        self._check_a(int(a_idx))
+        n_t = int(n_t)
+        S = self._coefficients.shape[0]
+        w = np.ascontiguousarray(np.asarray(w_arr, dtype=np.float64).ravel())
+        if float(self._interior[int(a_idx), 0]) >= float(t_end) or n_t < 2:
+            # a bubble nucleating at or after t_end gives zeros (:786-789); with fewer
+            # than two steps dt is 0 and every value vanishes (:798-799)
+            tb = 0.0 if t_begin is None else float(t_begin)
+            if float(self._interior[int(a_idx), 0]) < float(t_end) and tb > float(t_end):
+                raise ValueError(f"Invalid time range: t_begin={_rust_f64(tb)} > t_end={_rust_f64(float(t_end))}")
+            return np.zeros((2, S, w.size, max(n_t, 0)), dtype=np.complex128)
+        return self.compute_c_integrand(w, t_begin=t_begin, t_end=t_end, n_t=n_t,
+                                        selected_bubbles=np.array([int(a_idx)]))
 
     def compute_c_integrand(self, w_arr, *, t_begin=None, t_end, n_t, selected_bubbles=None):
-        raise NotImplementedError("compute_c_integrand is not built in this library yet")
+        """(2, n_sets, n_w, n_t) complex128: the time-resolved integrand summed over
+        the selected bubbles (generalized_bulk_flow.rs:875-920), computed on the GPU."""
+        self._push_params()
+        w = np.ascontiguousarray(np.asarray(w_arr, dtype=np.float64).ravel())
+        S = self._coefficients.shape[0]
+        if int(n_t) < 0:
+            raise OverflowError("can't convert negative int to unsigned")
+        out = np.zeros((2, S, w.size, int(n_t)), dtype=np.complex128)
+        sel = self._selected(selected_bubbles)
+        psel = sel.ctypes.data_as(C.POINTER(C.c_size_t)) if sel is not None else None
+        _call(L.lib().bgwx_generalized_bulk_flow_compute_c_integrand(
+            self._h, L.ptr(w), w.size, t_begin is not None, 0.0 if t_begin is None else float(t_begin),
+            float(t_end), int(n_t), psel, 0 if sel is None else sel.size,
+            out.ctypes.data_as(C.POINTER(L.BgwComplex64)), out.size))
+        return out
 
     # --- properties -------------------------------------------------------------
     @property

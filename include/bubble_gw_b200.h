@@ -179,6 +179,21 @@ BgwStatus bgwx_generalized_bulk_flow_spectrum_vjp(bgw_generalized_bulk_flow *bul
 BgwStatus bgwx_generalized_bulk_flow_set_bubbles(bgw_generalized_bulk_flow *bulk_flow, const double *interior,
                                                  size_t n_interior, const double *exterior, size_t n_exterior);
 
+/* Time-resolved integrand of the spectrum: out (2, n_sets, n_w, n_t), the
+ * sum over `selected_bubbles` (NULL = all interior bubbles; an empty selection
+ * gives zeros) of each bubble's A_{+,x}(w, t) e^{i w (t - z_a)} times the
+ * trapezoid dt weight and 1/(6 pi), zero at steps t <= t_a; no time cutoff.
+ * Summing over the last axis gives compute_c_integral without cutoff.
+ * Errors as the reference: n_t < 2, then an index out of range, then (for a
+ * bubble with t_a < t_end) t_begin > t_end.  Replaces
+ * GeneralizedBulkFlow::compute_c_integrand and, with a one-bubble selection,
+ * compute_c_integrand_fixed_bubble (generalized_bulk_flow.rs:776-920). */
+BgwStatus bgwx_generalized_bulk_flow_compute_c_integrand(bgw_generalized_bulk_flow *bulk_flow, const double *w_arr,
+                                                         size_t n_w, bool has_t_begin, double t_begin, double t_end,
+                                                         size_t n_t, const size_t *selected_bubbles,
+                                                         size_t n_selected_bubbles, BgwComplex64 *out,
+                                                         size_t out_len);
+
 /* Runs this handle's device work on `stream` (a cudaStream_t created by the
  * caller; NULL selects the handle's own non-blocking stream, so the legacy
  * default stream cannot be chosen).  No counterpart in the reference. */

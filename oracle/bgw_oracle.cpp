@@ -294,10 +294,12 @@ void b_integral(const Problem& P, size_t i, const int32_t* first, const double* 
 }
 
 // GBF:588-664 (A integral) followed by the per-t C increment of GBF:821-851.
-// `inc` receives (2, S, W) complex values already multiplied by dt.
+// `inc` receives (2, S, W) complex values already multiplied by dt.  With
+// `integrand` the tail is that of compute_c_integrand_fixed_bubble
+// (GBF:820-840): A e^{i w (t - z_a)} (dt weight), no time cutoff.
 void c_increment(const Problem& P, size_t a, const int32_t* first, const double* dtab, const double* w,
                  size_t W, double t, size_t t_idx, size_t n_t, double dt, const Cutoff& cut, Cplx* inc,
-                 std::vector<double>& scratch) {
+                 std::vector<double>& scratch, bool integrand = false) {
     size_t S = P.n_sets, nc = P.n_cos;
     double ta = P.interior[a].t, za = P.interior[a].z;
     double delta_ta = t - ta;
@@ -322,8 +324,18 @@ void c_increment(const Problem& P, size_t a, const int32_t* first, const double*
             }
         }
     }
-    double cw = cut.eval(t);
     double uw = (t_idx == 0 || t_idx == n_t - 1) ? 0.5 : 1.0;
+    if (integrand) {
+        Cplx dtw{dt * uw, 0.0};
+        for (size_t s = 0; s < S; ++s)
+            for (size_t k = 0; k < W; ++k) {
+                Cplx ph = cexp_i(w[k] * (t - za));
+                inc[(0 * S + s) * W + k] = cmul(cmul(ap[s * W + k], ph), dtw);
+                inc[(1 * S + s) * W + k] = cmul(cmul(am[s * W + k], ph), dtw);
+            }
+        return;
+    }
+    double cw = cut.eval(t);
     Cplx dtc{dt, 0.0};
     for (size_t s = 0; s < S; ++s)
         for (size_t k = 0; k < W; ++k) {
@@ -500,6 +512,64 @@ int orc_compute_c_integral(const double* interior, size_t n_int, const double* e
         out[2 * q] = acc[q].re;
         out[2 * q + 1] = acc[q].im;
         if (abs_out) abs_out[q] = absacc[q] / (6.0 * M_PI);
+    }
+    return 0;
+}
+
+// compute_c_integrand (GBF:875-920) over compute_c_integrand_fixed_bubble
+// (GBF:776-866): out (2, S, W, T) complex as interleaved doubles, the sum over
+// the selected bubbles in selection order of each bubble's time-resolved
+// integrand (already multiplied by the trapezoid dt weight and 1/(6 pi)).
+int orc_compute_c_integrand(const double* interior, size_t n_int, const double* exterior, size_t n_ext,
+                            size_t n_cos, size_t n_phi, const double* coeffs, const double* powers, size_t n_sets,
+                            size_t n_terms, double damping, const double* w, size_t n_w, int has_t_begin,
+                            double t_begin, double t_end, size_t n_t, const size_t* selected, size_t n_sel,
+                            double* out, int threads) {
+    if (n_cos < 2 || n_phi < 2) return fail("Invalid resolution: Angular resolutions must be greater than one");
+    if (n_t < 2) return fail("Invalid resolution: n_t must be >= 2");
+    Problem P;
+    load(P, interior, n_int, exterior, n_ext);
+    set_resolution(P, n_cos, n_phi);
+    set_params(P, coeffs, powers, n_sets, n_terms, damping);
+    const size_t S = n_sets, W = n_w, per = 2 * S * W;
+    std::vector<Cplx> total(per * n_t, Cplx{0, 0});
+    std::vector<size_t> ids;
+    if (selected) {
+        for (size_t q = 0; q < n_sel; ++q) {
+            if (selected[q] >= n_int)
+                return fail("Index " + std::to_string(selected[q]) + " out of bounds for max " + std::to_string(n_int));
+            ids.push_back(selected[q]);
+        }
+    } else {
+        for (size_t a = 0; a < n_int; ++a) ids.push_back(a);
+    }
+    double tb = has_t_begin ? t_begin : 0.0;
+    Cutoff unit = make_cutoff(0, 0.0, NAN, NAN);
+    std::vector<int32_t> first(n_cos * n_phi);
+    std::vector<double> dtab(n_cos * n_phi);
+    Cplx f{1.0 / (6.0 * M_PI), 0.0};
+    for (size_t a : ids) {
+        const double tn = P.interior[a].t;
+        if (tn >= t_end) continue;  // GBF:786-789
+        if (tb > t_end) return fail("Invalid time range");
+        masks_for(P, a, first.data(), threads);
+        delta_tab(P, a, first.data(), dtab.data());
+        std::vector<double> t_arr = linspace(tb, t_end, n_t);
+        const double dt = t_arr[1] - t_arr[0];
+        std::vector<Cplx> incs(n_t * per, Cplx{0, 0});
+        parallel_for<std::vector<double>>(n_t, threads, [&](size_t ti, std::vector<double>& scratch) {
+            const double t = t_arr[ti];
+            if (t <= tn) return;  // GBF:818-822
+            c_increment(P, a, first.data(), dtab.data(), w, W, t, ti, n_t, dt, unit, &incs[ti * per], scratch,
+                        true);
+        });
+        for (size_t ti = 0; ti < n_t; ++ti)
+            for (size_t q = 0; q < per; ++q)
+                total[q * n_t + ti] = cadd(total[q * n_t + ti], cmul(incs[ti * per + q], f));
+    }
+    for (size_t q = 0; q < per * n_t; ++q) {
+        out[2 * q] = total[q].re;
+        out[2 * q + 1] = total[q].im;
     }
     return 0;
 }

@@ -52,6 +52,9 @@ def lib():
             _dp, C.c_size_t, _dp, C.c_size_t, _dp, C.c_size_t, C.c_size_t, C.c_size_t, _dp, _dp, C.c_size_t,
             C.c_size_t, C.c_double, _dp, C.c_size_t, C.c_double, C.c_double, C.c_size_t, C.c_int, C.c_double,
             C.c_double, C.c_double, _dp, C.c_int]
+        L.orc_compute_c_integrand.argtypes = [
+            _dp, C.c_size_t, _dp, C.c_size_t, C.c_size_t, C.c_size_t, _dp, _dp, C.c_size_t, C.c_size_t,
+            C.c_double, _dp, C.c_size_t, C.c_int, C.c_double, C.c_double, C.c_size_t, _szp, C.c_size_t, _dp, C.c_int]
         L.orc_rotation_for_khat.argtypes = [C.c_double, C.c_double, C.c_double, _dp]
         L.orc_rotate.argtypes = [_dp, _dp, C.c_size_t, _dp]
         L.orc_time_cutoff.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _dp, C.c_size_t, _dp]
@@ -135,6 +138,29 @@ def compute_c_integral(interior, exterior, n_cos, n_phi, w, t_end, n_t, t_begin=
         0.0 if t_begin is None else float(t_begin), float(t_end), n_t, psel, nsel, kind, smax, rc, r0,
         out.ctypes.data_as(_dp), absout.ctypes.data_as(_dp) if want_abs else None, threads or max_threads()))
     return (out, absout) if want_abs else out
+
+
+def compute_c_integrand(interior, exterior, n_cos, n_phi, w, t_end, n_t, t_begin=None, coefficients=((1.0,),),
+                        powers=((3.0,),), damping=None, selected=None, threads=None):
+    """(2, n_sets, n_w, n_t) complex128, the reference's compute_c_integrand output."""
+    ai, pi, ni = _bubbles(interior)
+    ae, pe, ne = _bubbles(np.zeros((0, 4)) if exterior is None else exterior)
+    co = np.ascontiguousarray(np.asarray(coefficients, dtype=np.float64))
+    po = np.ascontiguousarray(np.asarray(powers, dtype=np.float64))
+    S, M = co.shape
+    w, pw = _d(np.asarray(w, dtype=np.float64).ravel())
+    out = np.zeros((2, S, w.size, n_t), dtype=np.complex128)
+    if selected is not None:
+        sel = np.ascontiguousarray(np.asarray(selected, dtype=np.uint64).ravel())
+        psel, nsel = sel.ctypes.data_as(_szp), sel.size
+    else:
+        psel, nsel = None, 0
+    _check(lib().orc_compute_c_integrand(
+        pi, ni, pe, ne, n_cos, n_phi, co.ctypes.data_as(_dp), po.ctypes.data_as(_dp), S, M,
+        np.nan if damping is None else float(damping), pw, w.size, 0 if t_begin is None else 1,
+        0.0 if t_begin is None else float(t_begin), float(t_end), n_t, psel, nsel, out.ctypes.data_as(_dp),
+        threads or max_threads()))
+    return out
 
 
 def rotation_for_khat(k):

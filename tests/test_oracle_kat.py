@@ -213,3 +213,18 @@ def test_golden_fixtures_reproduce():
         assert np.array_equal(out, p["out"]), name
         codes = O.first_colliding(p["interior"], p["exterior"], int(p["n_cos"]), int(p["n_phi"]))
         assert np.array_equal(codes, p["codes"]), name
+
+
+def test_integrand_sums_to_integral():
+    """compute_c_integrand summed over t equals compute_c_integral without a time cutoff
+    (generalized_bulk_flow.rs:776-866 against :775-873)."""
+    c = W.config(1)
+    kw = dict(t_begin=0.0, coefficients=[[1.0], [0.5]], powers=[[5.0], [3.0]], damping=0.7)
+    it = O.compute_c_integrand(c.interior, c.exterior, 10, 12, c.w[:5], 1.5, 33, **kw)
+    ci = O.compute_c_integral(c.interior, c.exterior, 10, 12, c.w[:5], 1.5, 33, **kw)
+    assert it.shape == (2, 2, 5, 33)
+    assert np.abs(it.sum(-1) - ci).max() <= 1e-13 * np.abs(ci).max()
+    tn = c.interior[:, 0]
+    t = np.linspace(0.0, 1.5, 33)
+    one = O.compute_c_integrand(c.interior, c.exterior, 10, 12, c.w[:5], 1.5, 33, selected=[2], **kw)
+    assert not one[..., t <= tn[2]].any()
