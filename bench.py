@@ -297,7 +297,8 @@ def run_b200(args):
         peak = mp["bf16_tflops_sustained"] / 2.0
         achieved = 3.0 * gemm_flops / (tm["gemm_ms"] * 1e-3) / 1e12
         roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": achieved / peak, "traffic": traffic, "kernel": "k_gemm_tc",
+                    "frac": achieved / peak, "traffic": traffic,
+                    "traffic_unit": "DRAM bytes per k-hat frame (ncu, profiles/traffic.json)", "kernel": "k_gemm_tc",
                     "work": "3 x 2 x (2 n_w) x n_t x columns x n_cos TF32 flops per frame (FP32 split in three)",
                     "peak_source": "of measured: MEASURED_PEAKS.json bf16_tflops_sustained / 2 (TF32 dense)",
                     "spectrum_stage": stage, "peaks": peaks}
