@@ -370,7 +370,7 @@ size_t mask_budget_bytes() {
     size_t free_b = 0, total_b = 0;
     if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) return (size_t)1 << 30;
     size_t b = free_b / 3;
-    const size_t cap = (size_t)24 << 30;
+    const size_t cap = (size_t)64 << 30;
     return std::max<size_t>((size_t)256 << 20, std::min(b, cap));
 }
 

@@ -45,6 +45,7 @@
 #include "device_common.cuh"
 #include "spectrum_factored.cuh"
 #include "spectrum_tc.cuh"
+#include "tc_ptx.cuh"
 
 namespace bgw {
 
@@ -107,7 +108,19 @@ struct BetaArgs {
     int bpt;               // bubbles per tile
     int t_pad;             // row length of beta
     int per_warp_bytes;
+    int tc_layout;         // beta as pre-split, pre-swizzled blocks of the tensor-core GEMM (Real = float)
+    int tiles;             // column tiles per frame (tc_layout)
 };
+
+// One beta value into the tensor-core GEMM's block layout: the hi and lo TF32
+// parts at (column n, step kk) of the block pair at `blk`.
+__device__ __forceinline__ void tc_store(float* blk, int n, int kk, float x) {
+    uint32_t hi, lo;
+    tc::split_tf32_fast(x, hi, lo);
+    const size_t o = tc_swz(n, kk);
+    blk[o] = __uint_as_float(hi);
+    blk[kTcBlockFloats + o] = __uint_as_float(lo);
+}
 
 template <class Real, int SMC>
 __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ beta) {
@@ -279,6 +292,13 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
 #pragma unroll
             for (int q = 0; q < 2 * SMC; ++q) P[q] = pstart[q];
         }
+        float* blk = nullptr;  // tc_layout: this bubble's block pair of step block b
+        int nbase = 0;
+        if (A.tc_layout) {
+            nbase = (slot % A.bpt) * 2 * A.S;
+            blk = reinterpret_cast<float*>(beta) +
+                  ((((size_t)frame * A.n_cos + i) * A.tiles + slot / A.bpt) * NB + b) * 2 * kTcBlockFloats;
+        }
         if (k < A.n_t) {
             const double* Drow = Dslot + (size_t)k * (1 + SMC);
             const double d3 = Drow[0];
@@ -293,9 +313,17 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
                     vs += f * P[2 * t + 1];
                 }
                 const bool on = d3 != 0.0;
-                brow[(size_t)(2 * s) * A.t_pad + k] = on ? (Real)(wk * vc) : (Real)0;
-                brow[(size_t)(2 * s + 1) * A.t_pad + k] = on ? (Real)(wk * vs) : (Real)0;
+                const Real xc = on ? (Real)(wk * vc) : (Real)0, xs = on ? (Real)(wk * vs) : (Real)0;
+                if (A.tc_layout) {
+                    tc_store(blk, nbase + 2 * s, lane, (float)xc);
+                    tc_store(blk, nbase + 2 * s + 1, lane, (float)xs);
+                } else {
+                    brow[(size_t)(2 * s) * A.t_pad + k] = xc;
+                    brow[(size_t)(2 * s + 1) * A.t_pad + k] = xs;
+                }
             }
+        } else if (A.tc_layout) {
+            for (int c = 0; c < 2 * A.S; ++c) tc_store(blk, nbase + c, lane, 0.0f);
         } else if (k < A.t_pad) {
             for (int c = 0; c < 2 * A.S; ++c) brow[(size_t)c * A.t_pad + k] = (Real)0;
         }
@@ -659,7 +687,10 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     }
     // beta
     CUDA_OK(cudaEventRecord(ev3[0], dev->stream));
-    const size_t beta_elems = (size_t)kn * n_cos * G.cols_pad * G.t_pad;
+    const bool tc = sizeof(Real) == 4 && job.kernel == BGWX_KERNEL_MIXED;
+    const int nkb = G.nblk;
+    const size_t beta_elems = tc ? (size_t)kn * n_cos * G.tiles_per_frame * nkb * 2 * kTcBlockFloats
+                                 : (size_t)kn * n_cos * G.cols_pad * G.t_pad;
     dev->beta.ensure(beta_elems * sizeof(Real));
     if ((long)n_sel * 2 * S != G.cols_pad) {  // unused tile columns must read as zero
         // padding columns of the last tile are read by the GEMM: keep them zero
@@ -700,6 +731,8 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
                     ((size_t)n_phi + 2 * G.nblk + 1) * sizeof(int);
         pw = (pw + 15) & ~(size_t)15;
         B.per_warp_bytes = (int)pw;
+        B.tc_layout = tc ? 1 : 0;
+        B.tiles = G.tiles_per_frame;
         int warps = (int)std::min<size_t>(8, (200 * 1024) / pw);
         if (warps < 1) throw Error{"n_phi too large for the beta kernel"};
         const size_t smem = (size_t)warps * pw;
@@ -732,7 +765,25 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     const size_t per = (size_t)2 * S * n_w;
     dev->fact_partial.ensure((size_t)kn * G.tiles_per_frame * per * sizeof(double2));
     A.partial = (double2*)dev->fact_partial.p;
-    if (sizeof(Real) == 4 && job.kernel == BGWX_KERNEL_MIXED) {
+    if (tc) {
+        // time-phase table: frame independent, rebuilt only when w, cos-theta or t change
+        const int n_wt = (n_w + 63) / 64;
+        const size_t atab_floats = (size_t)n_cos * n_wt * nkb * 2 * kTcBlockFloats;
+        std::vector<double> key;
+        key.reserve(3 + n_w + n_cos + n_t);
+        key.push_back((double)n_w);
+        key.push_back((double)n_cos);
+        key.push_back((double)n_t);
+        key.insert(key.end(), job.w, job.w + n_w);
+        key.insert(key.end(), job.cos_thetax, job.cos_thetax + n_cos);
+        key.insert(key.end(), job.t_arr, job.t_arr + n_t);
+        const bool had = dev->tc_atab.p && dev->tc_atab.cap >= atab_floats * sizeof(float);
+        dev->tc_atab.ensure(atab_floats * sizeof(float));
+        if (!had || dev->tc_key != key) {
+            launch_tc_phase_table(w, cos_t, t_arr, n_cos, n_w, n_t, (float*)dev->tc_atab.p, dev->stream);
+            ++launches;
+            dev->tc_key = key;
+        }
         TcArgs T;
         T.bub = bub_frames;
         T.n_tot = job.n_tot;
@@ -742,14 +793,13 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         T.n_t = n_t;
         T.n_w = n_w;
         T.S = S;
-        T.t_arr = t_arr;
         T.w = w;
         T.cos_t = cos_t;
         T.kfirst = (const int*)dev->fact_kfirst.p;
-        T.beta = (const float*)dev->beta.p;
-        T.cols_pad = G.cols_pad;
-        T.t_pad = G.t_pad;
-        T.dt = job.dt;
+        T.atab = (const float*)dev->tc_atab.p;
+        T.btab = (const float*)dev->beta.p;
+        T.n_wt = n_wt;
+        T.nkb = nkb;
         T.bpt = G.bpt;
         T.tiles_per_frame = G.tiles_per_frame;
         T.partial = A.partial;
@@ -796,8 +846,10 @@ size_t factored_bytes_per_frame(const SpectrumJob& job) {
     const size_t real =
         (job.kernel == BGWX_KERNEL_MIXED || job.kernel == BGWX_KERNEL_MIXED_SIMT) ? sizeof(float) : sizeof(double);
     const FactGeom G = fact_geom(job, real);
-    return (size_t)job.n_cos * G.cols_pad * G.t_pad * real +
-           (size_t)G.tiles_per_frame * 2 * job.n_sets * job.n_w * sizeof(double2);
+    const size_t beta = job.kernel == BGWX_KERNEL_MIXED
+                            ? (size_t)job.n_cos * G.tiles_per_frame * G.nblk * 2 * kTcBlockFloats * sizeof(float)
+                            : (size_t)job.n_cos * G.cols_pad * G.t_pad * real;
+    return beta + (size_t)G.tiles_per_frame * 2 * job.n_sets * job.n_w * sizeof(double2);
 }
 
 }  // namespace bgw

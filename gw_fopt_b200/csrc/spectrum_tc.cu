@@ -10,33 +10,35 @@
 // A_hi B_lo + A_lo B_hi + A_hi B_hi per K step (the A_lo B_lo term is below
 // FP32 rounding), which keeps FP32-level operand accuracy.
 //
+// Both operands arrive pre-split and pre-swizzled from HBM: the time phases
+// from a per-call table (k_tc_phase_table, frame and bubble independent), beta
+// from k_beta, in 16 KB blocks of 128 rows x 32 steps.  One thread streams the
+// blocks of a 32-step stage into shared memory with bulk copies that complete
+// on the stage's mbarrier (transaction bytes); one thread issues the MMAs with
+// both operands in shared memory.
+//
 // One CTA per (64-frequency tile, 128-column tile), looping over the rows i;
 // per row the K dimension is the time steps from the tile's first active
-// block of 32 steps on.  Warp roles (13 warps):
-//   0-3   A producers: thread = tensor-memory lane = GEMM row (w, Re|Im).  The
-//         time phase of step 32 kb + n is z_kb P_n: the block anchor z_kb
-//         advances by an FP64 complex recurrence from an FP64 sincos at the
-//         row's first block, P_n = e^{i w' n dt} is a per-row FP32 table; the
-//         FP32 value is split and stored to tensor memory (tcgen05.st).
-//   4-7   B producers: beta (FP32, HBM) -> split -> shared memory in the
-//         K-major 128-byte-swizzled layout, 32 steps per stage.
-//   8-11  epilogue: thread = lane.  Per row the phases e^{i w (t_a c_i - z_a)}
-//         (FP64 argument reduction, FP32 sincos) go to a shared-memory table;
-//         every block of 32 steps the accumulator (tcgen05.ld) is multiplied by
-//         them and summed per (w, set, +/x) in FP64.
-//   12    MMA issue (one thread) and tensor-memory allocation.
-// Stages: 4 (A in tensor memory, B in shared memory), full/empty mbarriers;
-// the accumulator is double-buffered across blocks of 32 steps.  Every wait is bounded:
-// on a timeout the block records an error flag, tells the other roles to
-// stop, waits for its issued MMAs to finish and frees its tensor memory.
+// block of 32 steps on.  Warp roles (10 warps):
+//   0     bulk-copy producer (one thread)
+//   1     MMA issue (one thread) and tensor-memory allocation
+//   2-9   epilogue, two warpgroups of 64 columns each: thread = tensor-memory
+//         lane.  Per row the phases e^{i w (t_a c_i - z_a)} (FP64 argument
+//         reduction, FP32 sincos) go to a shared-memory table; every block of
+//         32 steps the accumulator (tcgen05.ld) is multiplied by them and
+//         summed per (w, set, +/x) in FP64.
+// Stages: 3 x 64 KB (A hi/lo, B hi/lo); the FP32 accumulator is double-
+// buffered in tensor memory across blocks of 32 steps.  Every wait is bounded:
+// on a timeout the block records an error flag, tells the other roles to stop,
+// waits for its issued MMAs and copies to finish and frees its tensor memory.
 //
-// Tensor memory (512 columns): accumulators at columns 0 and 128; stage s's
-// A_hi at 256 + 64 s and A_lo at 256 + 64 s + 32.
+// Tensor memory: 256 columns, accumulators at columns 0 and 128.
 
 #include <cuda_runtime.h>
 
 #include <cstdint>
 #include <string>
+#include <type_traits>
 
 #include "bgw_internal.h"
 #include "device_common.cuh"
@@ -52,31 +54,57 @@ constexpr int kTcRows = 128;     // GEMM rows: 64 frequencies x (Re, Im)
 constexpr int kTcWT = 64;        // frequencies per CTA
 constexpr int kTcCols = 128;     // GEMM columns per CTA
 constexpr int kTcKB = 32;        // time steps per stage (128 bytes of TF32)
-constexpr int kTcStages = 4;
+constexpr int kTcStages = 3;
 constexpr int kTcFoldKB = 1;     // blocks of 32 steps accumulated in tensor memory before the FP64 fold
-constexpr int kTcWarps = 13;
+constexpr int kTcWarps = 10;
 constexpr int kTcThreads = 32 * kTcWarps;
-constexpr uint32_t kTmemCols = 512;
-constexpr int kBTileBytes = kTcCols * kTcKB * 4;  // 16 KB per (stage, hi|lo)
-constexpr int kEStride = 66;     // phase-table row (one frequency, 64 bubbles) padded against bank conflicts
+constexpr uint32_t kTmemCols = 256;
+constexpr int kBlockBytes = kTcBlockFloats * 4;   // 16 KB
+constexpr int kStageBytes = 4 * kBlockBytes;      // A hi, A lo, B hi, B lo
 
 struct SmemLayout {
-    static constexpr int b_hi = 0;
-    static constexpr int b_lo = kTcStages * kBTileBytes;
-    static constexpr int bars = 2 * kTcStages * kBTileBytes;  // full[S], empty[S], accf[2], acce[2], drain
+    static constexpr int stages = 0;
+    static constexpr int bars = kTcStages * kStageBytes;      // full[S], empty[S], accf[2], acce[2], drain
     static constexpr int n_bars = 2 * kTcStages + 5;
     static constexpr int tslot = bars + 8 * n_bars;
     static constexpr int abort_flag = tslot + 4;
-    static constexpr int binfo = tslot + 16;                  // int[64]
-    static constexpr int bt = binfo + 64 * 4;                 // double[64]
-    static constexpr int bz = bt + 64 * 8;                    // double[64]
-    static constexpr int etab = bz + 64 * 8;                  // float2[64 w][kEStride] (bubbles)
-    static constexpr int ptab = etab + 64 * 66 * 8;           // float2[32 steps][64 w]
-    static constexpr int total = ptab + 32 * 64 * 8;
+    static constexpr int binfo = tslot + 16;                   // int[64]
+    static constexpr int bt = binfo + 64 * 4;                  // double[64]
+    static constexpr int bz = bt + 64 * 8;                     // double[64]
+    static constexpr int etab = bz + 64 * 8;                   // float2[64 w][64 bubbles], XOR-swizzled
+    static constexpr int total = etab + 64 * 64 * 8;
 };
 
-__device__ __forceinline__ uint32_t swz128(int n, int c) {
-    return (uint32_t)((n >> 3) * 1024 + (n & 7) * 128 + ((c ^ (n & 7)) << 4));
+// Phase-table slot of (frequency l, bubble b): rows of 64 bubbles, the bubble
+// index XORed with l % 16 so that the 16 frequencies read by a warp fall in
+// distinct banks.
+__device__ __forceinline__ int eslot(int l, int b) { return l * 64 + (b ^ (l & 15)); }
+
+__global__ void k_tc_phase_table(const double* __restrict__ w, const double* __restrict__ cos_t,
+                                 const double* __restrict__ t_arr, int n_cos, int n_w, int n_t, int n_wt, int nkb,
+                                 float* __restrict__ atab) {
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const size_t n_el = (size_t)n_cos * n_wt * nkb * kTcBlockFloats;
+    if (q >= n_el) return;
+    const int e = (int)(q % kTcBlockFloats);
+    const size_t blk = q / kTcBlockFloats;  // (i, wt, kb)
+    const int kb = (int)(blk % nkb);
+    const int wt = (int)((blk / nkb) % n_wt);
+    const int i = (int)(blk / ((size_t)nkb * n_wt));
+    const int r = e >> 5, kk = e & 31;
+    const int wi = wt * kTcWT + (r >> 1), k = kb * kTcKB + kk;
+    float v = 0.0f;
+    if (wi < n_w && k < n_t) {
+        double sn, cs;
+        sincos(w[wi] * ((1.0 - cos_t[i]) * t_arr[k]), &sn, &cs);
+        v = (float)((r & 1) ? sn : cs);
+    }
+    uint32_t hi, lo;
+    tc::split_tf32_fast(v, hi, lo);
+    float* out = atab + blk * 2 * kTcBlockFloats;
+    const size_t o = tc_swz(r, kk);
+    out[o] = __uint_as_float(hi);
+    out[kTcBlockFloats + o] = __uint_as_float(lo);
 }
 
 template <int S>
@@ -98,7 +126,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
 
     constexpr int CPB = 2 * S;  // columns per bubble
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int w0 = blockIdx.x * kTcWT;
+    const int wt = blockIdx.x;
+    const int w0 = wt * kTcWT;
     const int frame = blockIdx.y / A.tiles_per_frame;
     const int tile = blockIdx.y % A.tiles_per_frame;
     const D4* B = A.bub + (size_t)frame * A.n_tot;
@@ -116,16 +145,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
         }
     }
     if (tid == 0) {
-        for (int q = 0; q < 2 * kTcStages; ++q) tc::mbar_init(&bars[q], q < kTcStages ? 8u : 1u);
+        for (int q = 0; q < kTcStages; ++q) {
+            tc::mbar_init(&full[q], 1);   // the producer's arrive; the copies' bytes complete the phase
+            tc::mbar_init(&empty[q], 1);  // the MMA thread's commit
+        }
         tc::mbar_init(&accf[0], 1);
         tc::mbar_init(&accf[1], 1);
-        tc::mbar_init(&acce[0], 4);
-        tc::mbar_init(&acce[1], 4);
+        tc::mbar_init(&acce[0], 8);
+        tc::mbar_init(&acce[1], 8);
         tc::mbar_init(drain, 1);
         *abort_flag = 0;
         tc::mbar_fence_init();
     }
-    if (warp == kTcWarps - 1) {
+    if (warp == 1) {
         tc::tmem_alloc(tslot, kTmemCols);
         tc::tmem_relinquish();
     }
@@ -137,225 +169,42 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
     int kstart = A.n_t;
     for (int b = 0; b < A.bpt && b < 64; ++b)
         if (binfo[b] >= 0) kstart = min(kstart, A.kfirst[binfo[b]]);
-    const int nkb = (A.n_t + kTcKB - 1) / kTcKB;
+    const int nkb = A.nkb;
     const int kb0 = kstart / kTcKB;
     const bool active = kb0 < nkb;
-    const long col0 = (long)tile * kTcCols;
     bool failed = false;
 
-    if (warp < 4) {
-        // ---------------- A producers ----------------
-        const int r = 32 * warp + lane;
-        const int wl = r >> 1, part = r & 1;
-        const int wi = w0 + wl;
-        const bool wok = wi < A.n_w;
-        const uint32_t lanebase = (uint32_t)(32 * warp) << 16;
-        float2* ptab = reinterpret_cast<float2*>(sm + SmemLayout::ptab);
-        int it = 0;
-        for (int i = 0; active && i < A.n_cos && !failed; ++i) {
-            // M[w, k] = z_kb P_n, k = 32 kb + n: the block anchor z_kb = e^{i w' t_k}
-            // advances in FP64 by e^{i w' 32 dt}; P_n = e^{i w' n dt} (FP32 table,
-            // each warp fills the entries of its own 16 frequencies).
-            const double om1 = 1.0 - A.cos_t[i];
-            __syncwarp();
-            for (int q = lane; q < 32 * 16; q += 32) {
-                const int n = q >> 4, l = 16 * warp + (q & 15);
-                const double oml = (w0 + l < A.n_w) ? A.w[w0 + l] * om1 : 0.0;
-                double sn, cs;
-                sincos(oml * (n * A.dt), &sn, &cs);
-                ptab[n * kTcWT + l] = make_float2((float)cs, (float)sn);
-            }
-            __syncwarp();
-            const double om = wok ? A.w[wi] * om1 : 0.0;
-            double zr, zi, sr, si;
-            sincos(om * A.t_arr[kb0 * kTcKB], &zi, &zr);
-            sincos(om * (kTcKB * A.dt), &si, &sr);
-            for (int kb = kb0; kb < nkb; ++kb, ++it) {
-                const float ar = (float)zr, ai = (float)zi;
-                const bool tail = (kb + 1) * kTcKB > A.n_t;
-                const double nr = fma(zr, sr, -zi * si);
-                const double ni = fma(zr, si, zi * sr);
-                zr = nr;
-                zi = ni;
-                const int st = it % kTcStages;
-                if (!tc::warp_wait_bounded(&empty[st], ((it / kTcStages) & 1) ^ 1, abort_flag)) {
-                    failed = true;
-                    break;
-                }
-                const uint32_t acol = tbase + 256 + 64 * st;
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {  // 16 steps at a time
-                    uint32_t hi[16], lo[16];
-#pragma unroll
-                    for (int n = 0; n < 16; ++n) {
-                        const int nn = 16 * h + n;
-                        const float2 p = ptab[nn * kTcWT + wl];
-                        float v = part ? fmaf(ar, p.y, ai * p.x) : fmaf(ar, p.x, -ai * p.y);
-                        if (tail && kb * kTcKB + nn >= A.n_t) v = 0.0f;
-                        tc::split_tf32_fast(v, hi[n], lo[n]);
+    if (warp == 0) {
+        // ---------------- bulk-copy producer ----------------
+        if (lane == 0 && active) {
+            int it = 0;
+            for (int i = 0; i < A.n_cos && !failed; ++i) {
+                const float* arow = A.atab + ((size_t)(i * A.n_wt + wt) * nkb) * 2 * kTcBlockFloats;
+                const float* brow =
+                    A.btab + ((((size_t)frame * A.n_cos + i) * A.tiles_per_frame + tile) * nkb) * 2 * kTcBlockFloats;
+                for (int kb = kb0; kb < nkb; ++kb, ++it) {
+                    const int st = it % kTcStages;
+                    if (!tc::mbar_wait_bounded_poll(&empty[st], ((it / kTcStages) & 1) ^ 1, abort_flag)) {
+                        failed = true;
+                        break;
                     }
-                    tc::tmem_st16((acol + 16 * h) | lanebase, hi);
-                    tc::tmem_st16((acol + 32 + 16 * h) | lanebase, lo);
+                    unsigned char* dst = sm + SmemLayout::stages + st * kStageBytes;
+                    tc::mbar_arrive_expect_tx(&full[st], kStageBytes);
+                    tc::bulk_g2s(dst, arow + (size_t)kb * 2 * kTcBlockFloats, 2 * kBlockBytes, &full[st]);
+                    tc::bulk_g2s(dst + 2 * kBlockBytes, brow + (size_t)kb * 2 * kTcBlockFloats, 2 * kBlockBytes,
+                                 &full[st]);
                 }
-                tc::tmem_wait_st();
-                tc::tc_fence_before();
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&full[st]);
+            }
+            // before the block ends, the copies this thread issued must have landed:
+            // wait (bounded) for the last phase of every stage it filled
+            const int n_it = it;
+            for (int q = 0; q < kTcStages && q < n_it; ++q) {
+                const int last = n_it - 1 - q;  // the last kTcStages iterations cover each used stage once
+                volatile int never = 0;
+                if (!tc::mbar_wait_bounded_poll(&full[last % kTcStages], (last / kTcStages) & 1, &never)) failed = true;
             }
         }
-    } else if (warp < 8) {
-        // ---------------- B producers ----------------
-        const int tb = tid - 128;
-        const float* beta = A.beta;
-        int it = 0;
-        for (int i = 0; active && i < A.n_cos && !failed; ++i) {
-            const float* brow = beta + (((size_t)frame * A.n_cos + i) * A.cols_pad + col0) * A.t_pad;
-            for (int kb = kb0; kb < nkb; ++kb, ++it) {
-                float4 v[8];
-                const bool tail = (kb + 1) * kTcKB > A.n_t;
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int q = tb + 128 * u;
-                    const int n = q >> 3, c = q & 7;
-                    const int k = kb * kTcKB + 4 * c;
-                    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (!tail) {
-                        x = __ldg(reinterpret_cast<const float4*>(brow + (size_t)n * A.t_pad + k));
-                    } else {
-                        if (k < A.t_pad) x = __ldg(reinterpret_cast<const float4*>(brow + (size_t)n * A.t_pad + k));
-                        if (k + 0 >= A.n_t) x.x = 0.f;
-                        if (k + 1 >= A.n_t) x.y = 0.f;
-                        if (k + 2 >= A.n_t) x.z = 0.f;
-                        if (k + 3 >= A.n_t) x.w = 0.f;
-                    }
-                    v[u] = x;
-                }
-                const int st = it % kTcStages;
-                if (!tc::warp_wait_bounded(&empty[st], ((it / kTcStages) & 1) ^ 1, abort_flag)) {
-                    failed = true;
-                    break;
-                }
-                unsigned char* bh = sm + SmemLayout::b_hi + st * kBTileBytes;
-                unsigned char* bl = sm + SmemLayout::b_lo + st * kBTileBytes;
-#pragma unroll
-                for (int u = 0; u < 8; ++u) {
-                    const int q = tb + 128 * u;
-                    const int n = q >> 3, c = q & 7;
-                    uint4 h, l;
-                    tc::split_tf32_fast(v[u].x, h.x, l.x);
-                    tc::split_tf32_fast(v[u].y, h.y, l.y);
-                    tc::split_tf32_fast(v[u].z, h.z, l.z);
-                    tc::split_tf32_fast(v[u].w, h.w, l.w);
-                    const uint32_t off = swz128(n, c);
-                    *reinterpret_cast<uint4*>(bh + off) = h;
-                    *reinterpret_cast<uint4*>(bl + off) = l;
-                }
-                tc::fence_proxy_async_smem();
-                __syncwarp();
-                if (lane == 0) tc::mbar_arrive(&full[st]);
-            }
-        }
-    } else if (warp < 12) {
-        // ---------------- epilogue ----------------
-        // Tensor-core FP32 accumulation rounds each addition into a growing
-        // sum, so the accumulator is handed over every kTcFoldKB blocks of 32
-        // steps and its contribution, phase included (the phase is constant
-        // along a row), is added to FP64 sums per (w, set, +/x).  Each lane
-        // holds one GEMM row, Re (even lane) or Im (odd lane) of its
-        // frequency, and accumulates sum_b cos_b Y_b and sum_b sin_b Y_b of
-        // that row; Re C = sum cos Yr - sum sin Yi and Im C = sum cos Yi +
-        // sum sin Yr are formed once at the end.  Products are summed in FP32
-        // over the bubbles of a 32-column chunk (two interleaved chains), then
-        // added to the FP64 sums.
-        const int q4 = warp - 8;
-        const int r = 32 * q4 + lane;
-        const int wl = r >> 1, part = r & 1;
-        const int wi = w0 + wl;
-        const uint32_t lanebase = (uint32_t)(32 * q4) << 16;
-        float2* etab = reinterpret_cast<float2*>(sm + SmemLayout::etab);
-        double accC[CPB], accS[CPB];
-#pragma unroll
-        for (int c = 0; c < CPB; ++c) accC[c] = accS[c] = 0.0;
-        int seg = 0;
-        for (int i = 0; active && i < A.n_cos && !failed; ++i) {
-            // e^{i w (t_a c_i - z_a)} per (w, bubble) of this row; zero for empty
-            // columns (each warp fills and reads only its own 16 frequencies)
-            const double ci = A.cos_t[i];
-            __syncwarp();
-#pragma unroll 4
-            for (int q = lane; q < 64 * 16; q += 32) {
-                const int b = q & 63, l = 16 * q4 + (q >> 6);
-                float2 e = make_float2(0.f, 0.f);
-                if (b < A.bpt && binfo[b] >= 0 && w0 + l < A.n_w) {
-                    double sn, cs;
-                    phase<float>(A.w[w0 + l] * (bt[b] * ci - bz[b]), sn, cs);
-                    e = make_float2((float)cs, (float)sn);
-                }
-                etab[l * kEStride + b] = e;
-            }
-            __syncwarp();
-            const float2* erow = etab + wl * kEStride;
-            const int nseg = (nkb - kb0 + kTcFoldKB - 1) / kTcFoldKB;
-            for (int g = 0; g < nseg; ++g, ++seg) {
-                const int buf = seg & 1;
-                if (!tc::warp_wait_bounded(&accf[buf], (seg >> 1) & 1, abort_flag)) {
-                    failed = true;
-                    break;
-                }
-                tc::tc_fence_after();
-                // columns [n0, n0 + 32) from y; the chunk's phases are loaded first
-                auto consume = [&](const uint32_t (&y)[32], const int n0) {
-                    constexpr int NB = 32 / CPB + 2;
-                    const int b_first = n0 / CPB;
-                    float2 ev[NB];
-#pragma unroll
-                    for (int j = 0; j < NB; ++j)
-                        if (b_first + j <= (n0 + 31) / CPB) ev[j] = erow[b_first + j];
-                    float pc[2][CPB], ps[2][CPB];
-#pragma unroll
-                    for (int c = 0; c < CPB; ++c) pc[0][c] = ps[0][c] = pc[1][c] = ps[1][c] = 0.f;
-#pragma unroll
-                    for (int c = 0; c < 32; ++c) {
-                        const int n = n0 + c;
-                        const int b = n / CPB, sc = n % CPB, h2 = b & 1;
-                        const float2 e = ev[b - b_first];
-                        const float yv = __uint_as_float(y[c]);
-                        pc[h2][sc] = fmaf(e.x, yv, pc[h2][sc]);
-                        ps[h2][sc] = fmaf(e.y, yv, ps[h2][sc]);
-                    }
-#pragma unroll
-                    for (int q = 0; q < CPB; ++q) {
-                        accC[q] += (double)(pc[0][q] + pc[1][q]);
-                        accS[q] += (double)(ps[0][q] + ps[1][q]);
-                    }
-                };
-                const uint32_t dcol = (tbase + 128 * buf) | lanebase;
-#pragma unroll
-                for (int ch = 0; ch < kTcCols / 32; ++ch) {
-                    uint32_t y[32];
-                    tc::tmem_ld32(dcol + 32 * ch, y);
-                    tc::tmem_wait_ld();
-                    if (ch == kTcCols / 32 - 1) {  // every column is in registers: release the buffer
-                        tc::tc_fence_before();
-                        __syncwarp();
-                        if (lane == 0) tc::mbar_arrive(&acce[buf]);
-                    }
-                    consume(y, 32 * ch);
-                }
-            }
-        }
-        // even lane: (sum cos Yr, sum sin Yr); odd lane: (sum cos Yi, sum sin Yi)
-#pragma unroll
-        for (int sg = 0; sg < CPB; ++sg) {
-            const double oc = __shfl_xor_sync(0xffffffffu, accC[sg], 1);
-            const double os = __shfl_xor_sync(0xffffffffu, accS[sg], 1);
-            if (part == 0 && wi < A.n_w) {
-                const int s_ = sg >> 1, g = sg & 1;
-                const size_t o = ((((size_t)frame * A.tiles_per_frame + tile) * 2 + g) * S + s_) * A.n_w + wi;
-                A.partial[o] = make_double2(accC[sg] - os, oc + accS[sg]);
-            }
-        }
-    } else {
+    } else if (warp == 1) {
         // ---------------- MMA issue ----------------
         if (lane == 0 && active) {
             const uint32_t idesc = tc::idesc_tf32(kTcRows, kTcCols);
@@ -365,7 +214,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
                 for (int kb = kb0; kb < nkb; ++kb, ++it) {
                     if ((kb - kb0) % kTcFoldKB == 0) {  // a new accumulation segment
                         const int buf = seg & 1;
-                        if (!tc::mbar_wait_bounded(&acce[buf], ((seg >> 1) & 1) ^ 1, abort_flag)) {
+                        if (!tc::mbar_wait_bounded_poll(&acce[buf], ((seg >> 1) & 1) ^ 1, abort_flag)) {
                             failed = true;
                             break;
                         }
@@ -374,20 +223,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
                         accumulate = 0;
                     }
                     const int st = it % kTcStages;
-                    if (!tc::mbar_wait_bounded(&full[st], (it / kTcStages) & 1, abort_flag)) {
+                    if (!tc::mbar_wait_bounded_poll(&full[st], (it / kTcStages) & 1, abort_flag)) {
                         failed = true;
                         break;
                     }
                     tc::tc_fence_after();
-                    const uint32_t a_hi = tbase + 256 + 64 * st, a_lo = a_hi + 32;
-                    const uint32_t b_hi = tc::smem_u32(sm + SmemLayout::b_hi + st * kBTileBytes);
-                    const uint32_t b_lo = tc::smem_u32(sm + SmemLayout::b_lo + st * kBTileBytes);
+                    const uint32_t base = tc::smem_u32(sm + SmemLayout::stages + st * kStageBytes);
+                    const uint32_t a_hi = base, a_lo = base + kBlockBytes;
+                    const uint32_t b_hi = base + 2 * kBlockBytes, b_lo = base + 3 * kBlockBytes;
 #pragma unroll
                     for (int j = 0; j < kTcKB / 8; ++j) {
-                        tc::mma_tf32_ts(dcol, a_hi + 8 * j, tc::sdesc_k128(b_lo + 32 * j), idesc, accumulate);
+                        tc::mma_tf32_ss(dcol, tc::sdesc_k128(a_hi + 32 * j), tc::sdesc_k128(b_lo + 32 * j), idesc,
+                                        accumulate);
                         accumulate = 1;
-                        tc::mma_tf32_ts(dcol, a_lo + 8 * j, tc::sdesc_k128(b_hi + 32 * j), idesc, 1);
-                        tc::mma_tf32_ts(dcol, a_hi + 8 * j, tc::sdesc_k128(b_hi + 32 * j), idesc, 1);
+                        tc::mma_tf32_ss(dcol, tc::sdesc_k128(a_lo + 32 * j), tc::sdesc_k128(b_hi + 32 * j), idesc, 1);
+                        tc::mma_tf32_ss(dcol, tc::sdesc_k128(a_hi + 32 * j), tc::sdesc_k128(b_hi + 32 * j), idesc, 1);
                     }
                     tc::mma_commit(&empty[st]);
                     if ((kb - kb0) % kTcFoldKB == kTcFoldKB - 1 || kb == nkb - 1) {
@@ -399,7 +249,132 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
             // wait for every MMA issued by this thread before the memory is freed
             tc::mma_commit(drain);
             volatile int never = 0;
-            if (!tc::mbar_wait_bounded(drain, 0, &never)) failed = true;
+            if (!tc::mbar_wait_bounded_poll(drain, 0, &never)) failed = true;
+        }
+    } else {
+        // ---------------- epilogue ----------------
+        // Tensor-core FP32 accumulation rounds each addition into a growing
+        // sum, so the accumulator is handed over every kTcFoldKB blocks of 32
+        // steps and its contribution, phase included (the phase is constant
+        // along a row), is added to FP64 sums per (w, set, +/x).  Each lane
+        // holds one GEMM row, Re (even lane) or Im (odd lane) of its
+        // frequency, and accumulates sum_b cos_b Y_b and sum_b sin_b Y_b of
+        // that row; Re C = sum cos Yr - sum sin Yi and Im C = sum cos Yi +
+        // sum sin Yr are formed once at the end.  Products are summed in FP32
+        // over the bubbles of a 32-column chunk (two interleaved chains), then
+        // added to the FP64 sums.
+        const int q4 = warp & 3;             // tensor-memory lane quadrant of this warp
+        const int half = (warp - 2) >> 2;    // which 64 columns
+        const int r = 32 * q4 + lane;
+        const int wl = r >> 1, part = r & 1;
+        const int wi = w0 + wl;
+        const uint32_t lanebase = (uint32_t)(32 * q4) << 16;
+        float2* etab = reinterpret_cast<float2*>(sm + SmemLayout::etab);
+        double accC[CPB], accS[CPB];
+#pragma unroll
+        for (int c = 0; c < CPB; ++c) accC[c] = accS[c] = 0.0;
+        // the column offset is a compile-time constant in each instance, so that
+        // every per-column index below is too (no dynamically indexed arrays)
+        auto run = [&](auto half_c) {
+            constexpr int c_lo = decltype(half_c)::value * (kTcCols / 2);
+            constexpr int b_lo = c_lo / CPB, b_hi = (c_lo + kTcCols / 2 - 1) / CPB;
+            constexpr int nb = b_hi - b_lo + 1;
+            int seg = 0;
+            for (int i = 0; active && i < A.n_cos && !failed; ++i) {
+                // e^{i w (t_a c_i - z_a)} per (w, bubble) of this row; zero for empty columns.
+                // Each warp fills the entries it reads (its 16 frequencies, its bubbles).
+                const double ci = A.cos_t[i];
+                __syncwarp();
+#pragma unroll 4
+                for (int q = lane; q < 16 * nb; q += 32) {
+                    const int b = b_lo + q % nb, l = 16 * q4 + q / nb;
+                    float2 e = make_float2(0.f, 0.f);
+                    if (b < A.bpt && binfo[b] >= 0 && w0 + l < A.n_w) {
+                        double sn, cs;
+                        phase<float>(A.w[w0 + l] * (bt[b] * ci - bz[b]), sn, cs);
+                        e = make_float2((float)cs, (float)sn);
+                    }
+                    etab[eslot(l, b)] = e;
+                }
+                __syncwarp();
+                const int nseg = (nkb - kb0 + kTcFoldKB - 1) / kTcFoldKB;
+                for (int g = 0; g < nseg; ++g, ++seg) {
+                    const int buf = seg & 1;
+                    if (!tc::warp_wait_bounded(&accf[buf], (seg >> 1) & 1, abort_flag)) {
+                        failed = true;
+                        break;
+                    }
+                    tc::tc_fence_after();
+                    // columns [n0, n0 + 32) from y; the chunk's phases are loaded first
+                    auto consume = [&](const uint32_t (&y)[32], auto n0_c) {
+                        constexpr int n0 = decltype(n0_c)::value;
+                        constexpr int b_first = n0 / CPB;
+                        constexpr int NB = (n0 + 31) / CPB - b_first + 1;
+                        float2 ev[NB];
+#pragma unroll
+                        for (int j = 0; j < NB; ++j) ev[j] = etab[eslot(wl, b_first + j)];
+                        float pc[2][CPB], ps[2][CPB];
+#pragma unroll
+                        for (int c = 0; c < CPB; ++c) pc[0][c] = ps[0][c] = pc[1][c] = ps[1][c] = 0.f;
+#pragma unroll
+                        for (int c = 0; c < 32; ++c) {
+                            const int n = n0 + c;
+                            const int b = n / CPB, sc = n % CPB, h2 = b & 1;
+                            const float2 e = ev[b - b_first];
+                            const float yv = __uint_as_float(y[c]);
+                            pc[h2][sc] = fmaf(e.x, yv, pc[h2][sc]);
+                            ps[h2][sc] = fmaf(e.y, yv, ps[h2][sc]);
+                        }
+#pragma unroll
+                        for (int q = 0; q < CPB; ++q) {
+                            accC[q] += (double)(pc[0][q] + pc[1][q]);
+                            accS[q] += (double)(ps[0][q] + ps[1][q]);
+                        }
+                    };
+                    const uint32_t dcol = (tbase + 128 * buf + c_lo) | lanebase;
+                    uint32_t y0[32], y1[32];
+                    tc::tmem_ld32(dcol, y0);
+                    tc::tmem_ld32(dcol + 32, y1);
+                    tc::tmem_wait_ld();
+                    tc::tc_fence_before();
+                    __syncwarp();
+                    if (lane == 0) tc::mbar_arrive(&acce[buf]);  // this warp's columns are in registers
+                    consume(y0, std::integral_constant<int, c_lo>{});
+                    consume(y1, std::integral_constant<int, c_lo + 32>{});
+                }
+            }
+        };
+        if (half == 0)
+            run(std::integral_constant<int, 0>{});
+        else
+            run(std::integral_constant<int, 1>{});
+        // The second warpgroup hands its sums to the first through the stage
+        // area: once the last accumulator is ready every MMA and copy has
+        // completed, so no stage is in use any more.
+        double* xch = reinterpret_cast<double*>(sm + SmemLayout::stages);
+        if (half == 1) {
+#pragma unroll
+            for (int sg = 0; sg < CPB; ++sg) {
+                xch[(2 * sg) * kTcRows + r] = accC[sg];
+                xch[(2 * sg + 1) * kTcRows + r] = accS[sg];
+            }
+        }
+        asm volatile("bar.sync 1, 256;" ::: "memory");  // the eight epilogue warps only
+        if (half == 0) {
+            // even lane: (sum cos Yr, sum sin Yr); odd lane: (sum cos Yi, sum sin Yi)
+#pragma unroll
+            for (int sg = 0; sg < CPB; ++sg) {
+                const double ac = accC[sg] + xch[(2 * sg) * kTcRows + r];
+                const double as = accS[sg] + xch[(2 * sg + 1) * kTcRows + r];
+                const double oc = __shfl_xor_sync(0xffffffffu, ac, 1);
+                const double os = __shfl_xor_sync(0xffffffffu, as, 1);
+                if (part == 0 && wi < A.n_w) {
+                    const int s_ = sg >> 1, g = sg & 1;
+                    const size_t o =
+                        ((((size_t)frame * A.tiles_per_frame + tile) * 2 + g) * S + s_) * A.n_w + wi;
+                    A.partial[o] = make_double2(ac - os, oc + as);
+                }
+            }
         }
     }
     if (failed) {
@@ -408,7 +383,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
     }
     tc::tc_fence_before();
     __syncthreads();
-    if (warp == kTcWarps - 1) {
+    if (warp == 1) {
         tc::tc_fence_after();
         tc::tmem_dealloc(tbase, kTmemCols);
     }
@@ -422,12 +397,22 @@ void launch_s(const TcArgs& A, dim3 grid, size_t smem, cudaStream_t st) {
 
 }  // namespace
 
+void launch_tc_phase_table(const double* w, const double* cos_t, const double* t_arr, int n_cos, int n_w, int n_t,
+                           float* atab, cudaStream_t st) {
+    const int n_wt = (n_w + kTcWT - 1) / kTcWT, nkb = (n_t + kTcKB - 1) / kTcKB;
+    const size_t n_el = (size_t)n_cos * n_wt * nkb * kTcBlockFloats;
+    if (n_el / 256 + 1 > 0x7fffffffULL) throw Error{"time-phase table too large"};
+    k_tc_phase_table<<<(unsigned)((n_el + 255) / 256), 256, 0, st>>>(w, cos_t, t_arr, n_cos, n_w, n_t, n_wt, nkb,
+                                                                     atab);
+    CUDA_OK(cudaGetLastError());
+}
+
 void launch_gemm_tc(const TcArgs& A, size_t kn, cudaStream_t st) {
     if (A.bpt * 2 * A.S > kTcCols) throw Error{"tensor-core GEMM: too many columns per tile"};
     const size_t smem = SmemLayout::total + 1024;
     const size_t gy = kn * (size_t)A.tiles_per_frame;
     if (gy > 65535) throw Error{"too many column tiles in one k-hat chunk"};
-    dim3 grid((unsigned)((A.n_w + kTcWT - 1) / kTcWT), (unsigned)gy);
+    dim3 grid((unsigned)A.n_wt, (unsigned)gy);
     switch (A.S) {
         case 1: launch_s<1>(A, grid, smem, st); break;
         case 2: launch_s<2>(A, grid, smem, st); break;

@@ -12,6 +12,7 @@
 //    1024 bytes between 8-row groups.  The k-th group of 8 K elements starts
 //    32*k bytes after the base (the hardware applies the swizzle to the
 //    address it forms).
+//  * A operand in shared memory: the same layout as B with M rows.
 //  * A operand and accumulator in TMEM: lane m holds row m, one 32-bit column
 //    per K element (A) or per N element (accumulator).
 //  * tcgen05.ld/st of shape 32x32b: thread t of a warp whose index is w
@@ -76,13 +77,43 @@ __device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity
     return false;
 }
 
+// The same bound with plain polling (a short sleep between late polls): for
+// phases completed by bulk-copy transaction bytes, whose completion does not
+// end a suspended try_wait early.
+__device__ __forceinline__ bool mbar_wait_bounded_poll(uint64_t* bar, uint32_t parity, volatile int* abort,
+                                                       uint32_t limit = 1u << 22) {
+    for (uint32_t it = 0; it < limit; ++it) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (*abort) return false;
+        if (it > 64) __nanosleep(32);
+    }
+    return false;
+}
+
 // mbar_wait_bounded by lane 0 of the calling warp with the outcome broadcast,
 // so that the whole warp continues (or gives up) together before its
 // .sync.aligned tensor-memory instructions.  Call with the full warp.
 __device__ __forceinline__ bool warp_wait_bounded(uint64_t* bar, uint32_t parity, volatile int* abort) {
     int ok = 0;
-    if ((threadIdx.x & 31) == 0) ok = mbar_wait_bounded(bar, parity, abort) ? 1 : 0;
+    if ((threadIdx.x & 31) == 0) ok = mbar_wait_bounded_poll(bar, parity, abort) ? 1 : 0;
     return __shfl_sync(0xffffffffu, ok, 0) != 0;
+}
+
+// Arrives on `bar` and adds `bytes` to the transaction count its phase waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Bulk copy (no tensor map, no multicast) of `bytes` contiguous bytes from
+// global to this CTA's shared memory; completes `bytes` transactions on `bar`.
+// Both addresses 16-byte aligned, `bytes` a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src_gmem, uint32_t bytes, uint64_t* bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst_smem)),
+        "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
 }
 
 // Generic-proxy writes to shared memory made visible to the tensor cores.
@@ -174,6 +205,17 @@ __device__ __forceinline__ void mma_tf32_ts(uint32_t d_tmem, uint32_t a_tmem, ui
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::1.kind::tf32 [%0], [%1], %2, %3, p;\n\t}" ::"r"(d_tmem),
         "r"(a_tmem), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T; issued by one thread.
+__device__ __forceinline__ void mma_tf32_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                            uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
 
