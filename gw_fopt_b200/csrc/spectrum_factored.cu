@@ -143,6 +143,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
     const double ta = A.bub[A.sel[slot]].t;
     const double* trow = A.tau + (size_t)row * A.n_phi;
     const unsigned full = 0xffffffffu;
+    const double inv_dt = 1.0 / A.dt;  // the estimate below is only a starting point
     auto block_of = [&](int j, int& kj) -> int {
         kj = A.n_t;
         if (j >= A.n_phi) return -2;  // not a patch
@@ -150,7 +151,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         if (!(tj > 0.0)) return -1;    // never collides
         // first k with (t_k - t_a) >= tau_j: arithmetic estimate, then exact
         // comparisons (the predicate is monotone in k) settle the boundary
-        const double est = ceil((ta + tj - A.t_arr[0]) / A.dt);
+        const double est = ceil((ta + tj - A.t_arr[0]) * inv_dt);
         int lo = est < 0.0 ? 0 : (est > (double)A.n_t ? A.n_t : (int)est);
         while (lo > 0 && A.t_arr[lo - 1] - ta >= tj) --lo;
         while (lo < A.n_t && !(A.t_arr[lo] - ta >= tj)) ++lo;
@@ -159,12 +160,12 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
     };
     for (int b = lane; b < NB; b += 32) boff[b] = 0;
     __syncwarp();
-    // pass 1: events per block; never-colliding weights (lane sums, fixed-order reduction)
+    // pass 1: events per block; never-colliding weights (lane sums, fixed-order reduction).
+    // The first collided step of patches j = lane + 32 jj, jj < kMaxJ, is kept for pass 2.
+    constexpr int kMaxJ = 8;
+    int kj_c[kMaxJ], b_c[kMaxJ];
     double nc = 0.0, ns = 0.0;
-    for (int j0 = 0; j0 < A.n_phi; j0 += 32) {
-        const int j = j0 + lane;
-        int kj;
-        const int b = block_of(j, kj);
+    auto pass1 = [&](int j, int b) {
         if (b == -1) {
             const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
             nc += wj * A.cos2[j];
@@ -173,6 +174,19 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         const unsigned m = __match_any_sync(full, b);
         if (b >= 0 && lane == __ffs(m) - 1) boff[b] += __popc(m);
         __syncwarp();
+    };
+#pragma unroll
+    for (int jj = 0; jj < kMaxJ; ++jj) {
+        if (32 * jj >= A.n_phi) break;
+        const int j = 32 * jj + lane;
+        kj_c[jj] = 0;
+        b_c[jj] = block_of(j, kj_c[jj]);
+        pass1(j, b_c[jj]);
+    }
+    for (int j0 = 32 * kMaxJ; j0 < A.n_phi; j0 += 32) {
+        int kj;
+        const int b = block_of(j0 + lane, kj);
+        pass1(j0 + lane, b);
     }
     for (int o = 16; o > 0; o >>= 1) {
         nc += __shfl_down_sync(full, nc, o);
@@ -191,10 +205,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
     __syncwarp();
     // pass 2: scatter events (stable in j within a block)
     const unsigned lt = (1u << lane) - 1u;
-    for (int j0 = 0; j0 < A.n_phi; j0 += 32) {
-        const int j = j0 + lane;
-        int kj;
-        const int b = block_of(j, kj);
+    auto pass2 = [&](int j, int kj, int b) {
         const unsigned m = __match_any_sync(full, b);
         int pos = 0;
         if (b >= 0) pos = brun[b] + __popc(m & lt);
@@ -217,6 +228,16 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
                 q[3 + 2 * t] = qs * f;
             }
         }
+    };
+#pragma unroll
+    for (int jj = 0; jj < kMaxJ; ++jj) {
+        if (32 * jj >= A.n_phi) break;
+        pass2(32 * jj + lane, kj_c[jj], b_c[jj]);
+    }
+    for (int j0 = 32 * kMaxJ; j0 < A.n_phi; j0 += 32) {
+        int kj;
+        const int b = block_of(j0 + lane, kj);
+        pass2(j0 + lane, kj, b);
     }
     __syncwarp();
     // block totals of the uncollided weights (each in event order), then the
@@ -256,37 +277,33 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         double Uc = uend[2 * b], Us = uend[2 * b + 1];
         double P[2 * SMC];
         if (boff[b] != boff[b + 1]) {  // warp-uniform: this block has events
-            double h[NQ];
+            // Each lane walks the block's few events (in event order): those
+            // collided at its step k_j <= k join the collided sums, the others
+            // the uncollided sum still to come; the block totals of the
+            // collided sums (every lane forms them alike) carry to the next block.
+            double uadd_c = 0.0, uadd_s = 0.0, pin[2 * SMC], ptot[2 * SMC];
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) h[q] = 0.0;
+            for (int q = 0; q < 2 * SMC; ++q) pin[q] = ptot[q] = 0.0;
             for (int e = boff[b]; e < boff[b + 1]; ++e) {
-                if (evk[e] != k) continue;
+                const double* qe = evq + (size_t)e * NQ;
+                const bool in = evk[e] <= k;
+                if (!in) {
+                    uadd_c += qe[0];
+                    uadd_s += qe[1];
+                }
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) h[q] += evq[(size_t)e * NQ + q];
-            }
-            // exclusive suffix over lanes of the uncollided weights
-            double uc = h[0], us = h[1];
-            for (int o = 1; o < 32; o <<= 1) {
-                const double tc = __shfl_down_sync(full, uc, o), ts = __shfl_down_sync(full, us, o);
-                if (lane + o < 32) {
-                    uc += tc;
-                    us += ts;
+                for (int q = 0; q < 2 * SMC; ++q) {
+                    const double v = qe[2 + q];
+                    ptot[q] += v;
+                    if (in) pin[q] += v;
                 }
             }
-            double xc = __shfl_down_sync(full, uc, 1), xs = __shfl_down_sync(full, us, 1);
-            if (lane == 31) xc = xs = 0.0;
-            Uc += xc;
-            Us += xs;
-            // inclusive prefix over lanes of the collided weights
+            Uc += uadd_c;
+            Us += uadd_s;
 #pragma unroll
             for (int q = 0; q < 2 * SMC; ++q) {
-                double v = h[2 + q];
-                for (int o = 1; o < 32; o <<= 1) {
-                    const double t = __shfl_up_sync(full, v, o);
-                    if (lane >= o) v += t;
-                }
-                P[q] = pstart[q] + v;
-                pstart[q] += __shfl_sync(full, v, 31);
+                P[q] = pstart[q] + pin[q];
+                pstart[q] += ptot[q];
             }
         } else {
 #pragma unroll
