@@ -63,74 +63,123 @@ __device__ __forceinline__ bool check_pre(const D4& dba, double nb, const D4& dc
     return mdot(cv, x) > 0.0;
 }
 
-// Exhaustive decision for one direction (global memory): argmin, check it
-// against everything, then the failures; the reference loop if more than
-// kMaxFail failures.
-__device__ long exhaustive(const D4* __restrict__ B, size_t n_tot, uint32_t a, const D4& xa, const D4& x) {
-    long best = -1;
-    double best_tau = CUDART_INF;
-    for (size_t b = 0; b < n_tot; ++b) {
+// Exhaustive decision for one direction, by a whole warp (all 32 lanes call it
+// with the same arguments).  It returns what the sequential procedure returns:
+// the argmin of tau in collider order (first index on ties), checked against
+// every collider; when it fails, the first of its failures (in collider order)
+// that passes every check, or the reference loop (GBF:162-199) when it failed
+// more than kMaxFail times.  Lanes take colliders lane, lane + 32, ...; a
+// check over all colliders is the AND of the lanes' checks, so its order does
+// not matter.
+__device__ __forceinline__ double tau_of(const D4& dba, const D4& x, bool& ok) {
+    const double dot = mdot(dba, x);
+    ok = false;
+    double tau = CUDART_INF;
+    if (dot > 1e-10) {
+        tau = __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
+        ok = tau > 0.0;
+    }
+    return tau;
+}
+
+// true when check(b, c) passes for every collider c other than a and b
+__device__ bool warp_all_pass(const D4* __restrict__ B, size_t n_tot, uint32_t a, size_t b, const D4& xa,
+                              const D4& dba, double nb, const D4& x) {
+    const unsigned full = 0xffffffffu;
+    for (size_t base = 0; base < n_tot; base += 32) {
+        const size_t c = base + (threadIdx.x & 31);
+        bool pass = true;
+        if (c < n_tot && c != a && c != b) pass = check_pt(dba, nb, dsub4(B[c], xa), x);
+        if (!__all_sync(full, pass)) return false;
+    }
+    return true;
+}
+
+__device__ long exhaustive_warp(const D4* __restrict__ B, size_t n_tot, uint32_t a, const D4& xa, const D4& x) {
+    const unsigned full = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    // 1. argmin: lane-local first minimum, then the (tau, index) minimum over lanes
+    double bt = CUDART_INF;
+    long bi = -1;
+    for (size_t b = lane; b < n_tot; b += 32) {
         if (b == a) continue;
-        const D4 dba = dsub4(B[b], xa);
-        const double dot = mdot(dba, x);
-        if (dot > 1e-10) {
-            const double tau = __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
-            if (tau > 0.0 && tau < best_tau) {
-                best_tau = tau;
-                best = (long)b;
-            }
+        bool ok;
+        const double tau = tau_of(dsub4(B[b], xa), x, ok);
+        if (ok && tau < bt) {
+            bt = tau;
+            bi = (long)b;
         }
     }
-    if (best < 0) return -1;
+    for (int o = 16; o > 0; o >>= 1) {
+        const double t2 = __shfl_xor_sync(full, bt, o);
+        const long i2 = __shfl_xor_sync(full, bi, o);
+        if (i2 >= 0 && (bi < 0 || t2 < bt || (t2 == bt && i2 < bi))) {
+            bt = t2;
+            bi = i2;
+        }
+    }
+    if (bi < 0) return -1;
+    const long best = bi;
+    // 2. check the argmin against every collider; keep its first kMaxFail failures
     const D4 dm = dsub4(B[best], xa);
     const double nm = mdot(dm, dm);
-    size_t fails[kMaxFail];
+    long my_fail = -1;  // lane f holds failure f
     int nfail = 0;
-    for (size_t c = 0; c < n_tot; ++c) {
-        if (c == a || (long)c == best) continue;
-        if (!check_pt(dm, nm, dsub4(B[c], xa), x)) {
-            if (nfail < kMaxFail) fails[nfail] = c;
+    for (size_t base = 0; base < n_tot; base += 32) {
+        const size_t c = base + lane;
+        bool fail = false;
+        if (c < n_tot && c != a && (long)c != best) fail = !check_pt(dm, nm, dsub4(B[c], xa), x);
+        unsigned m = __ballot_sync(full, fail);
+        while (m && nfail < kMaxFail) {
+            const int bit = __ffs(m) - 1;
+            m &= m - 1;
+            if (lane == nfail) my_fail = (long)(base + bit);
             ++nfail;
         }
+        nfail += __popc(m);
     }
     if (nfail == 0) return best;
     if (nfail > kMaxFail) {
-        // the reference loop (GBF:162-199)
+        // the reference loop (GBF:162-199): candidates in collider order with tau below the current result's
         long r = -1;
         double rt = CUDART_INF;
-        for (size_t b = 0; b < n_tot; ++b) {
-            if (b == a) continue;
-            const D4 dba = dsub4(B[b], xa);
-            const double dsq = mdot(dba, dba);
-            const double dot = mdot(dba, x);
-            if (dot <= 1e-10) continue;
-            const double tau = __ddiv_rn(dsq, dmul(2.0, dot));
-            if (tau <= 0.0 || tau >= rt) continue;
-            bool first = true;
-            for (size_t c = 0; c < n_tot && first; ++c) {
-                if (c == a || c == b) continue;
-                first = check_pt(dba, dsq, dsub4(B[c], xa), x);
+        for (size_t base = 0; base < n_tot; base += 32) {
+            const size_t b = base + lane;
+            bool ok = false;
+            double tau = CUDART_INF;
+            if (b < n_tot && b != a) {
+                // the reference's skips: dot <= 1e-10, tau <= 0 (NaN goes on, as there)
+                const D4 dba = dsub4(B[b], xa);
+                const double dot = mdot(dba, x);
+                if (!(dot <= 1e-10)) {
+                    tau = __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
+                    ok = !(tau <= 0.0);
+                }
             }
-            if (first) {
-                r = (long)b;
-                rt = tau;
+            unsigned m = __ballot_sync(full, ok);
+            while (m) {
+                const int bit = __ffs(m) - 1;
+                m &= m - 1;
+                const double tb = __shfl_sync(full, tau, bit);
+                if (tb >= rt) continue;
+                const size_t cb = base + bit;
+                const D4 dba = dsub4(B[cb], xa);
+                if (warp_all_pass(B, n_tot, a, cb, xa, dba, mdot(dba, dba), x)) {
+                    r = (long)cb;
+                    rt = tb;
+                }
             }
         }
         return r;
     }
+    // 3. the first failure (in collider order) that passes every check
     for (int f = 0; f < nfail; ++f) {
-        const size_t c = fails[f];
+        const long c = __shfl_sync(full, my_fail, f);
         const D4 dc = dsub4(B[c], xa);
-        const double dot = mdot(dc, x);
-        if (!(dot > 1e-10)) continue;
-        const double nc = mdot(dc, dc);
-        if (!(__ddiv_rn(nc, dmul(2.0, dot)) > 0.0)) continue;
-        bool ok = true;
-        for (size_t e = 0; e < n_tot && ok; ++e) {
-            if (e == a || e == c) continue;
-            ok = check_pt(dc, nc, dsub4(B[e], xa), x);
-        }
-        if (ok) return (long)c;
+        bool ok;
+        tau_of(dc, x, ok);
+        if (!ok) continue;
+        if (warp_all_pass(B, n_tot, a, (size_t)c, xa, dc, mdot(dc, dc), x)) return c;
     }
     return -1;
 }
@@ -285,10 +334,13 @@ __global__ void __launch_bounds__(kNbThreads)
 }
 
 // ------------------------------------------------------------ k_masks_list
+// One block per (radiating bubble, direction range, frame): the candidate list
+// is gathered into shared memory once, then every warp walks 32-direction
+// chunks of the range independently (no block barrier after the prologue).
 __global__ void __launch_bounds__(kMaskListThreads)
     k_masks_list(const D4* __restrict__ bub, size_t n_int, size_t n_tot, const uint32_t* __restrict__ sel,
                  size_t n_sel, const NbList* __restrict__ lists, const D4* __restrict__ dirs, size_t nd,
-                 unsigned n_dblocks, double* __restrict__ tau_out, int32_t* __restrict__ code_out,
+                 unsigned n_split, double* __restrict__ tau_out, int32_t* __restrict__ code_out,
                  unsigned long long* __restrict__ counters) {
     // per listed collider: Delta = x_c - x_a and its Minkowski norm, computed once
     // per block with the reference's operations (direction independent)
@@ -300,17 +352,22 @@ __global__ void __launch_bounds__(kMaskListThreads)
     __shared__ double s_onrm[kMaxOutliers];
     __shared__ int s_oidx[kMaxOutliers];
     const int k = blockIdx.y;
-    const size_t slot = blockIdx.x / n_dblocks;
-    const size_t d = (size_t)(blockIdx.x % n_dblocks) * kMaskListThreads + threadIdx.x;
+    const size_t slot = blockIdx.x / n_split;
+    const unsigned part = blockIdx.x % n_split;
+    const size_t chunks = (nd + 31) / 32;
+    const size_t c_begin = chunks * part / n_split, c_end = chunks * (part + 1) / n_split;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    constexpr int kWarps = kMaskListThreads / 32;
     const D4* B = bub + (size_t)k * n_tot;
     const uint32_t a = sel[slot];
     const NbList* L = lists + slot;
     const int n = L->count;
+    double* tau_row = tau_out + ((size_t)k * n_sel + slot) * nd;
+    int32_t* code_row = code_out ? code_out + ((size_t)k * n_sel + slot) * nd : nullptr;
     if (a >= n_int || n < 0) {  // invalid radiating bubble: sentinel outputs
-        if (d < nd) {
-            const size_t o = ((size_t)k * n_sel + slot) * nd + d;
-            tau_out[o] = CUDART_NAN;
-            if (code_out) code_out[o] = INT32_MIN;
+        for (size_t d = c_begin * 32 + threadIdx.x; d < min(c_end * 32, nd); d += kMaskListThreads) {
+            tau_row[d] = CUDART_NAN;
+            if (code_row) code_row[d] = INT32_MIN;
         }
         return;
     }
@@ -331,125 +388,164 @@ __global__ void __launch_bounds__(kMaskListThreads)
         s_onrm[q] = mdot(dc, dc);
     }
     __syncthreads();
-    if (d >= nd) return;
-    const D4 x = dirs[d];
     const double kmax = L->kmax, rho1 = L->rho1, rho2 = L->rho2;
     const double u64 = 64.0 * 1.1102230246251565e-16;
-    long result = -1;
-    bool full = no < 0;
+    unsigned long long n_full = 0;
 
-    // verifies candidate c (position pc) against the list up to key theta and the outliers
-    auto verify = [&](int c, const D4& dc, double nc, double theta, int* fails, int& nfail) -> bool {
-        bool ok = true;
-        for (int e = 0; e < n; ++e) {
-            if (s_key[e] > theta) break;
-            const int ce = s_idx[e];
-            if (ce == c) continue;
-            if (!check_pre(dc, nc, s_pos[e], s_nrm[e], x)) {
-                ok = false;
-                if (fails) {
-                    if (nfail < kMaxFail) fails[nfail] = e;
-                    ++nfail;
-                } else {
-                    return false;
-                }
-            }
-        }
-        for (int e = 0; e < no; ++e) {
-            const int ce = s_oidx[e];
-            if (ce == c) continue;
-            bool in_list = false;  // already checked above when listed with key <= theta
-            for (int q = 0; q < n && s_key[q] <= theta; ++q) in_list |= (s_idx[q] == ce);
-            if (in_list) continue;
-            if (!check_pre(dc, nc, s_opos[e], s_onrm[e], x)) {
-                ok = false;
-                if (!fails) return false;
-                nfail = kMaxFail + 1;  // outliers are resolved by the exhaustive path
-            }
-        }
-        return ok;
-    };
-    auto theta_of = [&](const D4& dc, double tau, double dot) {
-        const double dx = sqrt(dc.x * dc.x + dc.y * dc.y + dc.z * dc.z);
-        const double A = fabs(dc.t) + dx, Q = dc.t * dc.t + dx * dx;
-        return tau * (1.0 + 1e-12) + u64 * (A * rho1 + Q * rho2) / dot;
-    };
+    for (size_t ch = c_begin + warp; ch < c_end; ch += kWarps) {
+        // the whole warp takes the same chunks; the barrier at the end of each
+        // chunk reconverges lanes whose searches ended at different steps
+        __syncwarp();
+        const size_t d = min(ch * 32 + lane, nd - 1);
+        const bool live = ch * 32 + lane < nd;
+        const D4 x = dirs[d];
+        long result = -1;
+        double res_tau = 0.0;  // tau of the result when it came from the list (same operations)
+        bool full = no < 0;
 
-    if (!full) {
-        // 1. argmin of tau in key order
-        double best = CUDART_INF;
-        int bi = -1;
-        bool ended = true;
-        for (int e = 0; e < n; ++e) {
-            if (s_key[e] > best * (1.0 + 1e-12)) {
-                ended = false;
-                break;
-            }
-            const double dot = mdot(s_pos[e], x);
-            if (dot > 1e-10) {
-                // cheap filter before the exact quotient: tau < best needs nrm < 2 dot best
-                const double nrm = s_nrm[e];
-                if (nrm > 0.0 && nrm < dmul(dmul(2.0, dot), best) * (1.0 + 1e-12)) {
-                    const double tau = __ddiv_rn(nrm, dmul(2.0, dot));
-                    if (tau > 0.0 && tau < best) {
-                        best = tau;
-                        bi = e;
+        // verifies candidate c against the list up to key theta and the outliers
+        auto verify = [&](int c, const D4& dc, double nc, double theta, int* fails, int& nfail) -> bool {
+            bool ok = true;
+            for (int e = 0; e < n; ++e) {
+                if (s_key[e] > theta) break;
+                const int ce = s_idx[e];
+                if (ce == c) continue;
+                if (!check_pre(dc, nc, s_pos[e], s_nrm[e], x)) {
+                    ok = false;
+                    if (fails) {
+                        if (nfail < kMaxFail) fails[nfail] = e;
+                        ++nfail;
+                    } else {
+                        return false;
                     }
                 }
             }
-        }
-        if (ended && !(kmax > best * (1.0 + 1e-12))) full = !(bi < 0 && kmax == CUDART_INF);
-        if (!full && bi >= 0) {
-            // 2. verify the argmin
-            const D4 dm = s_pos[bi];
-            const double nm = s_nrm[bi], dotm = mdot(dm, x);
-            const double th = theta_of(dm, best, dotm);
-            if (!(th < kmax)) {
-                full = true;
-            } else {
-                int fails[kMaxFail];
-                int nfail = 0;
-                if (verify(s_idx[bi], dm, nm, th, fails, nfail)) {
-                    result = s_idx[bi];
-                } else if (nfail > kMaxFail) {
+            for (int e = 0; e < no; ++e) {
+                const int ce = s_oidx[e];
+                if (ce == c) continue;
+                bool in_list = false;  // already checked above when listed with key <= theta
+                for (int q = 0; q < n && s_key[q] <= theta; ++q) in_list |= (s_idx[q] == ce);
+                if (in_list) continue;
+                if (!check_pre(dc, nc, s_opos[e], s_onrm[e], x)) {
+                    ok = false;
+                    if (!fails) return false;
+                    nfail = kMaxFail + 1;  // outliers are resolved by the exhaustive path
+                }
+            }
+            return ok;
+        };
+        auto theta_of = [&](const D4& dc, double tau, double dot) {
+            const double dx = sqrt(dc.x * dc.x + dc.y * dc.y + dc.z * dc.z);
+            const double A = fabs(dc.t) + dx, Q = dc.t * dc.t + dx * dx;
+            return tau * (1.0 + 1e-12) + u64 * (A * rho1 + Q * rho2) / dot;
+        };
+
+        if (!full) {
+            // 1. argmin of tau in key order
+            double best = CUDART_INF;
+            int bi = -1;
+            bool ended = true;
+            for (int e = 0; e < n; ++e) {
+                if (s_key[e] > best * (1.0 + 1e-12)) {
+                    ended = false;
+                    break;
+                }
+                const double dot = mdot(s_pos[e], x);
+                if (dot > 1e-10) {
+                    // cheap filter before the exact quotient: tau < best needs nrm < 2 dot best
+                    const double nrm = s_nrm[e];
+                    if (nrm > 0.0 && nrm < dmul(dmul(2.0, dot), best) * (1.0 + 1e-12)) {
+                        const double tau = __ddiv_rn(nrm, dmul(2.0, dot));
+                        if (tau > 0.0 && tau < best) {
+                            best = tau;
+                            bi = e;
+                        }
+                    }
+                }
+            }
+            if (ended && !(kmax > best * (1.0 + 1e-12))) full = !(bi < 0 && kmax == CUDART_INF);
+            if (!full && bi >= 0) {
+                // 2. verify the argmin
+                const D4 dm = s_pos[bi];
+                const double nm = s_nrm[bi], dotm = mdot(dm, x);
+                const double th = theta_of(dm, best, dotm);
+                if (!(th < kmax)) {
                     full = true;
                 } else {
-                    // 3. the passer, if any, is among the failures
-                    for (int f = 0; f < nfail && result < 0 && !full; ++f) {
-                        const int e = fails[f];
-                        const D4 dc = s_pos[e];
-                        const double dot = mdot(dc, x);
-                        if (!(dot > 1e-10)) continue;
-                        const double nc = s_nrm[e];
-                        const double tau = __ddiv_rn(nc, dmul(2.0, dot));
-                        if (!(tau > 0.0)) continue;
-                        const double thf = theta_of(dc, tau, dot);
-                        if (!(thf < kmax)) {
-                            full = true;
-                            break;
+                    int fails[kMaxFail];
+                    int nfail = 0;
+                    if (verify(s_idx[bi], dm, nm, th, fails, nfail)) {
+                        result = s_idx[bi];
+                        res_tau = best;
+                    } else if (nfail > kMaxFail) {
+                        full = true;
+                    } else {
+                        // 3. the passer, if any, is among the failures
+                        for (int f = 0; f < nfail && result < 0 && !full; ++f) {
+                            const int e = fails[f];
+                            const D4 dc = s_pos[e];
+                            const double dot = mdot(dc, x);
+                            if (!(dot > 1e-10)) continue;
+                            const double nc = s_nrm[e];
+                            const double tau = __ddiv_rn(nc, dmul(2.0, dot));
+                            if (!(tau > 0.0)) continue;
+                            const double thf = theta_of(dc, tau, dot);
+                            if (!(thf < kmax)) {
+                                full = true;
+                                break;
+                            }
+                            int dummy = 0;
+                            if (verify(s_idx[e], dc, nc, thf, nullptr, dummy)) {
+                                result = s_idx[e];
+                                res_tau = tau;
+                            }
                         }
-                        int dummy = 0;
-                        if (verify(s_idx[e], dc, nc, thf, nullptr, dummy)) result = s_idx[e];
                     }
                 }
             }
         }
+        // directions that left the list are decided by the whole warp, one at a time
+        unsigned fm = __ballot_sync(0xffffffffu, full && live);
+        n_full += (full && live) ? 1 : 0;
+        while (fm) {
+            const int src = __ffs(fm) - 1;
+            fm &= fm - 1;
+            D4 xs;
+            xs.t = __shfl_sync(0xffffffffu, x.t, src);
+            xs.x = __shfl_sync(0xffffffffu, x.x, src);
+            xs.y = __shfl_sync(0xffffffffu, x.y, src);
+            xs.z = __shfl_sync(0xffffffffu, x.z, src);
+            const long r = exhaustive_warp(B, n_tot, a, xa, xs);
+            if (lane == src) result = r;
+        }
+        if (full && result >= 0) {
+            // compute_delta_tab (GBF:457-466)
+            const D4 dba = dsub4(B[result], xa);
+            const double dot = mdot(dba, x);
+            res_tau = fabs(dot) < 1e-10 ? 0.0 : __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
+        }
+        // compute_delta_tab (GBF:457-466): a listed result has dot > 1e-10, and its
+        // tau above was formed with the same operations from the same Delta.
+        if (live) {
+            tau_row[d] = result >= 0 ? res_tau : 0.0;
+            if (code_row)
+                code_row[d] =
+                    result < 0 ? -1 : ((size_t)result < n_int ? (int32_t)result : -((int32_t)(result - n_int) + 2));
+        }
     }
-    if (full) {
-        atomicAdd(counters, 1ull);
-        result = exhaustive(B, n_tot, a, xa, x);
-    }
-    const size_t o = ((size_t)k * n_sel + slot) * nd + d;
-    double tau = 0.0;
-    if (result >= 0) {
-        // compute_delta_tab (GBF:457-466)
-        const D4 dba = dsub4(B[result], xa);
-        const double dot = mdot(dba, x);
-        tau = fabs(dot) < 1e-10 ? 0.0 : __ddiv_rn(mdot(dba, dba), dmul(2.0, dot));
-    }
-    tau_out[o] = tau;
-    if (code_out)
-        code_out[o] = result < 0 ? -1 : ((size_t)result < n_int ? (int32_t)result : -((int32_t)(result - n_int) + 2));
+    if (n_full) atomicAdd(counters, n_full);
+}
+
+// Blocks per radiating bubble and frame: a few thousand directions per block
+// amortise the list gather; ranges shrink when there are too few blocks to
+// fill the GPU.
+static unsigned mask_split(size_t nd, size_t n_pairs) {
+    const size_t chunks = (nd + 31) / 32;
+    size_t split = (nd + 4095) / 4096;
+    const size_t want = 148 * 16;  // blocks for about four waves of resident blocks
+    while (split * n_pairs < want && split * 4 <= chunks) split *= 2;
+    if (split > chunks) split = chunks;
+    return (unsigned)(split < 1 ? 1 : split);
 }
 
 // ------------------------------------------------------------------ host
@@ -464,11 +560,11 @@ void launch_masks_with_lists(cudaStream_t stream, const D4* bub, size_t n_int, s
     if (n_sel > 0x7fffffffULL) throw Error{"too many radiating bubbles"};
     k_neighbors<<<(unsigned)n_sel, kNbThreads, 0, stream>>>(bub, n_int, n_tot, sel, lists);
     CUDA_OK(cudaGetLastError());
-    const unsigned n_dblocks = (unsigned)((nd + kMaskListThreads - 1) / kMaskListThreads);
-    const size_t gx = (size_t)n_dblocks * n_sel;
+    const unsigned n_split = mask_split(nd, n_sel);
+    const size_t gx = (size_t)n_split * n_sel;
     if (gx > 0x7fffffffULL) throw Error{"too many (bubble, patch) pairs for one launch"};
     k_masks_list<<<dim3((unsigned)gx, 1), kMaskListThreads, 0, stream>>>(bub, n_int, n_tot, sel, n_sel, lists, dirs,
-                                                                        nd, n_dblocks, tau, codes, counters);
+                                                                        nd, n_split, tau, codes, counters);
     CUDA_OK(cudaGetLastError());
 }
 
@@ -489,12 +585,12 @@ void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames
         CUDA_OK(cudaGetLastError());
         if (launches) ++*launches;
     }
-    const unsigned n_dblocks = (unsigned)((nd + kMaskListThreads - 1) / kMaskListThreads);
-    const size_t gx = (size_t)n_dblocks * n_sel;
+    const unsigned n_split = mask_split(nd, n_sel * kn);
+    const size_t gx = (size_t)n_split * n_sel;
     if (gx > 0x7fffffffULL || kn > 65535) throw Error{"too many (bubble, patch) pairs for one launch"};
     dim3 grid((unsigned)gx, (unsigned)kn);
     k_masks_list<<<grid, kMaskListThreads, 0, dev->stream>>>(bub_frames, n_int, n_tot, sel, n_sel,
-                                                             (const NbList*)dev->nblists.p, dirs, nd, n_dblocks, tau,
+                                                             (const NbList*)dev->nblists.p, dirs, nd, n_split, tau,
                                                              codes, counters);
     CUDA_OK(cudaGetLastError());
     if (launches) ++*launches;

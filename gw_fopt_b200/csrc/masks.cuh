@@ -5,7 +5,7 @@
 
 namespace bgw {
 
-constexpr int kList = 128;           // candidate colliders per radiating bubble
+constexpr int kList = 512;           // candidate colliders per radiating bubble
 constexpr int kMaxOutliers = 8;      // always-checked near-lightlike colliders
 constexpr int kMaxFail = 8;          // failures of the argmin resolved without the reference loop
 constexpr int kNbThreads = 256;

@@ -112,6 +112,40 @@ def test_delta_tab_bitwise(gpu_available):
     assert np.array_equal(tau, rt)
 
 
+def crowded_hemisphere(seed=11, n_near=700, n_far=300):
+    """Radiating bubble 0 at the origin; n_near colliders within 0.05-0.1 of it on the +z side
+    (more than one candidate list holds) and n_far colliders at 0.6-0.8 on the -z side, all
+    nucleating at t = 0.  Directions into -z find their first collider only past the list,
+    so the search takes its exhaustive path there."""
+    rng = np.random.default_rng(seed)
+
+    def shell(n, r0, r1, sign):
+        v = rng.normal(size=(n, 3))
+        v /= np.linalg.norm(v, axis=1, keepdims=True)
+        v[:, 2] = sign * np.abs(v[:, 2])
+        return v * rng.uniform(r0, r1, size=(n, 1))
+
+    pts = np.concatenate([np.zeros((1, 3)), shell(n_near, 0.05, 0.1, 1.0), shell(n_far, 0.6, 0.8, -1.0)])
+    return np.concatenate([np.zeros((pts.shape[0], 1)), pts], axis=1)
+
+
+def test_masks_exhaustive_path_bitwise(gpu_available):
+    import ctypes as C
+    from gw_fopt_b200 import _lib as L
+    interior = crowded_hemisphere()
+    n_cos = n_phi = 24
+    g = mb.GeneralizedBulkFlow(mb.LatticeBubbles(mb.EmptyLattice(), interior, np.zeros((0, 4))))
+    g.set_resolution(n_cos, n_phi)
+    codes = np.empty((2, n_cos, n_phi), dtype=np.int32)
+    tau = np.empty((2, n_cos, n_phi))
+    L.check(L.lib().bgwx_generalized_bulk_flow_first_colliding(
+        g._h, 0, 2, codes.ctypes.data_as(C.POINTER(C.c_int32)), tau.ctypes.data_as(C.POINTER(C.c_double))))
+    assert g.last_timings()["fallbacks"] > 0  # the exhaustive path ran
+    rc, rt = O.first_colliding(interior, None, n_cos, n_phi, 0, 2, with_delta_tab=True)
+    assert np.array_equal(codes, rc)
+    assert np.array_equal(tau, rt)
+
+
 @pytest.mark.parametrize("kernel", KERNELS)
 @pytest.mark.parametrize("name", ["capi2", "bench5", "confY", "cfg1_damped"])
 def test_spectrum_vs_golden(gpu_available, name, kernel):
