@@ -346,6 +346,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
     // per block with the reference's operations (direction independent)
     __shared__ D4 s_pos[kList];
     __shared__ double s_nrm[kList];
+    __shared__ double s_l1[kList];  // |dt| + |dx| + |dy| + |dz|
     __shared__ double s_key[kList];
     __shared__ int s_idx[kList];
     __shared__ D4 s_opos[kMaxOutliers];
@@ -358,10 +359,14 @@ __global__ void __launch_bounds__(kMaskListThreads)
     const size_t c_begin = chunks * part / n_split, c_end = chunks * (part + 1) / n_split;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int kWarps = kMaskListThreads / 32;
+    constexpr int kBatch = 2;
     const D4* B = bub + (size_t)k * n_tot;
     const uint32_t a = sel[slot];
     const NbList* L = lists + slot;
     const int n = L->count;
+    __shared__ bool s_big;  // a listed Delta too large for the candidate filter's margin
+    if (threadIdx.x == 0) s_big = false;
+    __syncthreads();
     double* tau_row = tau_out + ((size_t)k * n_sel + slot) * nd;
     int32_t* code_row = code_out ? code_out + ((size_t)k * n_sel + slot) * nd : nullptr;
     if (a >= n_int || n < 0) {  // invalid radiating bubble: sentinel outputs
@@ -380,6 +385,8 @@ __global__ void __launch_bounds__(kMaskListThreads)
         const D4 dc = dsub4(B[c], xa);
         s_pos[q] = dc;
         s_nrm[q] = mdot(dc, dc);
+        s_l1[q] = fabs(dc.t) + fabs(dc.x) + fabs(dc.y) + fabs(dc.z);
+        if (!(s_l1[q] < 1e5)) s_big = true;  // benign race: every writer stores true
     }
     for (int q = threadIdx.x; q < no; q += kMaskListThreads) {
         s_oidx[q] = L->outlier[q];
@@ -401,22 +408,58 @@ __global__ void __launch_bounds__(kMaskListThreads)
         const D4 x = dirs[d];
         long result = -1;
         double res_tau = 0.0;  // tau of the result when it came from the list (same operations)
-        bool full = no < 0;
+        bool full = no < 0 || s_big;
 
-        // verifies candidate c against the list up to key theta and the outliers
+        // Approximate Minkowski product with the direction (FMA chain): within
+        // 4.01 u L1(d) of the exact value, since |x_i| <= 1.
+        auto adot = [&](const D4& p) { return fma(p.z, x.z, fma(p.y, x.y, fma(p.x, x.x, -(p.t * x.t)))); };
+
+        // Verifies candidate c (Delta dc, norm nc) against the list up to key theta and the
+        // outliers.  check(c, e) is the sign of the reference's expression V_ref; the filter value
+        //   V = fma(ne, adot(c), -(nc adot(e)))
+        // is within 6.03 u S of the exact value and V_ref within 6.01 u S, where
+        // S = |ne| L1(c) + |nc| L1(e); |V| > 32 u S (plus an underflow guard) fixes
+        // the sign, otherwise the reference's expression is evaluated.
         auto verify = [&](int c, const D4& dc, double nc, double theta, int* fails, int& nfail) -> bool {
+            const double dotc = adot(dc);
+            const double l1c = fabs(dc.t) + fabs(dc.x) + fabs(dc.y) + fabs(dc.z);
+            const double am = 32.0 * 1.1102230246251565e-16 * l1c;
+            const double bm = 32.0 * 1.1102230246251565e-16 * fabs(nc);
             bool ok = true;
-            for (int e = 0; e < n; ++e) {
-                if (s_key[e] > theta) break;
-                const int ce = s_idx[e];
-                if (ce == c) continue;
-                if (!check_pre(dc, nc, s_pos[e], s_nrm[e], x)) {
-                    ok = false;
-                    if (fails) {
-                        if (nfail < kMaxFail) fails[nfail] = e;
-                        ++nfail;
-                    } else {
-                        return false;
+            // entries in batches of kBatch: their filter values are independent
+            // (instruction-level parallelism); decisions are taken in list order
+            bool done = false;
+            for (int e0 = 0; e0 < n && !done; e0 += kBatch) {
+                double vb[kBatch], bb[kBatch], kb[kBatch];
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j) {
+                    const int e = min(e0 + j, n - 1);
+                    kb[j] = s_key[e];
+                    const D4 pe = s_pos[e];
+                    const double ne = s_nrm[e];
+                    vb[j] = fma(ne, dotc, -(nc * adot(pe)));
+                    bb[j] = fma(fabs(ne), am, bm * s_l1[e]) + 1e-300;
+                }
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j) {
+                    const int e = e0 + j;
+                    if (e >= n || kb[j] > theta) {
+                        done = true;
+                        break;
+                    }
+                    if (s_idx[e] == c) continue;
+                    bool pass;
+                    if (vb[j] > bb[j]) pass = true;
+                    else if (vb[j] < -bb[j]) pass = false;
+                    else pass = check_pre(dc, nc, s_pos[e], s_nrm[e], x);
+                    if (!pass) {
+                        ok = false;
+                        if (fails) {
+                            if (nfail < kMaxFail) fails[nfail] = e;
+                            ++nfail;
+                        } else {
+                            return false;
+                        }
                     }
                 }
             }
@@ -441,33 +484,51 @@ __global__ void __launch_bounds__(kMaskListThreads)
         };
 
         if (!full) {
-            // 1. argmin of tau in key order
-            double best = CUDART_INF;
+            // 1. a candidate: the approximate argmin of tau = nrm / (2 dot) in key order
+            //    (quotients compared by cross-multiplication), stopping once key exceeds
+            //    the best quotient with a margin.  Any candidate serves: steps 2-3 decide
+            //    exactly whatever it is; the exact argmin only keeps step 3 idle.
+            double bn = 0.0, bd = 0.0;  // best quotient bn / bd, bd > 0
             int bi = -1;
-            bool ended = true;
-            for (int e = 0; e < n; ++e) {
-                if (s_key[e] > best * (1.0 + 1e-12)) {
-                    ended = false;
-                    break;
+            bool ended = true, stop = false;
+            for (int e0 = 0; e0 < n && !stop; e0 += kBatch) {
+                double kb[kBatch], nb[kBatch], db[kBatch];
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j) {
+                    const int e = min(e0 + j, n - 1);
+                    kb[j] = s_key[e];
+                    nb[j] = s_nrm[e];
+                    db[j] = 2.0 * adot(s_pos[e]);
                 }
-                const double dot = mdot(s_pos[e], x);
-                if (dot > 1e-10) {
-                    // cheap filter before the exact quotient: tau < best needs nrm < 2 dot best
-                    const double nrm = s_nrm[e];
-                    if (nrm > 0.0 && nrm < dmul(dmul(2.0, dot), best) * (1.0 + 1e-12)) {
-                        const double tau = __ddiv_rn(nrm, dmul(2.0, dot));
-                        if (tau > 0.0 && tau < best) {
-                            best = tau;
-                            bi = e;
-                        }
+#pragma unroll
+                for (int j = 0; j < kBatch; ++j) {
+                    if (e0 + j >= n) break;
+                    if (bi >= 0 && kb[j] * bd > bn * (1.0 + 1e-11)) {
+                        ended = false;
+                        stop = true;
+                        break;
+                    }
+                    // every collider of the exact test (dot > 1e-10, nrm > 0) has den > 0 here,
+                    // since the block's L1 norms keep 4.01 u L1 below 1e-10
+                    if (db[j] > 0.0 && nb[j] > 0.0 && (bi < 0 || nb[j] * bd < bn * db[j])) {
+                        bn = nb[j];
+                        bd = db[j];
+                        bi = e0 + j;
                     }
                 }
             }
-            if (ended && !(kmax > best * (1.0 + 1e-12))) full = !(bi < 0 && kmax == CUDART_INF);
+            double best = CUDART_INF, dotm = 0.0;
+            if (bi >= 0) {
+                // the candidate's tau with the reference's operations (compute_delta_tab)
+                dotm = mdot(s_pos[bi], x);
+                if (dotm > 1e-10) best = __ddiv_rn(s_nrm[bi], dmul(2.0, dotm));
+                if (!(dotm > 1e-10) || !(best > 0.0)) full = true;  // not a collider by the exact test
+            }
+            if (!full && ended && !(kmax > best * (1.0 + 1e-11))) full = !(bi < 0 && kmax == CUDART_INF);
             if (!full && bi >= 0) {
-                // 2. verify the argmin
+                // 2. verify the candidate
                 const D4 dm = s_pos[bi];
-                const double nm = s_nrm[bi], dotm = mdot(dm, x);
+                const double nm = s_nrm[bi];
                 const double th = theta_of(dm, best, dotm);
                 if (!(th < kmax)) {
                     full = true;

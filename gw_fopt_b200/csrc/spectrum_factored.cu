@@ -58,7 +58,8 @@ constexpr int kTM = 8;           // register tile rows per thread (columns: TN =
 
 // ---------------------------------------------------------------------------
 __global__ void k_time_tables(const D4* __restrict__ bub, const uint32_t* __restrict__ sel, int n_sel,
-                              const double* __restrict__ t_arr, int n_t, const double* __restrict__ powers, int SM,
+                              const double* __restrict__ t_arr, int n_t, const double* __restrict__ powers,
+                              const double* __restrict__ coeffs, const double* __restrict__ cutw, int SM,
                               int has_damp, double damp, double* __restrict__ D, int* __restrict__ kfirst) {
     const int slot = blockIdx.y;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -67,9 +68,12 @@ __global__ void k_time_tables(const D4* __restrict__ bub, const uint32_t* __rest
     const double dt = t_arr[k] - ta;
     double* row = D + ((size_t)slot * n_t + k) * (1 + SM);
     const bool on = dt > 0.0;
-    row[0] = on ? dt * (dt * dt) : 0.0;
+    // step weight (time cutoff x trapezoid end weight) folded into the table
+    const double wk = cutw[k] * ((k == 0 || k == n_t - 1) ? 0.5 : 1.0);
+    const double d3 = on ? dt * (dt * dt) : 0.0;
+    row[0] = wk * d3;
     const double e = has_damp ? exp(-dt / damp) : 1.0;
-    for (int q = 0; q < SM; ++q) row[1 + q] = on ? pow(dt, 3.0 - powers[q]) * e : 0.0;
+    for (int q = 0; q < SM; ++q) row[1 + q] = d3 != 0.0 ? wk * coeffs[q] * (pow(dt, 3.0 - powers[q]) * e) : 0.0;
     // first active step (t_a <= t_k and dt > 0): monotone in k
     if (on && (k == 0 || !(t_arr[k - 1] - ta > 0.0))) kfirst[slot] = k;
     if (k == n_t - 1 && !on) kfirst[slot] = n_t;
@@ -132,11 +136,13 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
     const int NB = A.nblk;
     unsigned char* base = sm_b + (size_t)warp * A.per_warp_bytes;
     double* evq = reinterpret_cast<double*>(base);             // [n_phi][NQ]
-    double* btot = evq + (size_t)A.n_phi * NQ;                  // [NB][2] block totals of q0
-    double* uend = btot + 2 * NB;                               // [NB][2] uncollided after block
-    int* evk = reinterpret_cast<int*>(uend + 2 * NB);           // [n_phi]
+    double* btot = evq + (size_t)A.n_phi * NQ;                  // [NB][NQ] block totals
+    double* uend = btot + (size_t)NQ * NB;                      // [NB][2] uncollided after block
+    double* pbeg = uend + 2 * NB;                               // [NB][2 SMC] collided before block
+    int* evk = reinterpret_cast<int*>(pbeg + (size_t)2 * SMC * NB);  // [n_phi]
     int* boff = evk + A.n_phi;                                  // [NB+1]
     int* brun = boff + NB + 1;                                  // [NB]
+    uint8_t* evs = reinterpret_cast<uint8_t*>(brun + NB);       // [n_phi + 4] step of each event within its block
     const int slot = (int)((row / A.n_cos) % A.n_sel);
     const int i = (int)(row % A.n_cos);
     const long frame = row / ((long)A.n_cos * A.n_sel);
@@ -214,6 +220,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         __syncwarp();
         if (b >= 0) {
             evk[pos] = kj;
+            evs[pos] = (uint8_t)(kj & 31);
             const double tj = trow[j];
             const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
             const double qc = wj * A.cos2[j], qs = wj * A.sin2[j];
@@ -240,16 +247,19 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         pass2(j0 + lane, kj, b);
     }
     __syncwarp();
-    // block totals of the uncollided weights (each in event order), then the
-    // uncollided sums after each block, accumulated backwards
+    // block totals of every weight (each in event order); then the uncollided
+    // sums after each block (accumulated backwards) and the collided sums
+    // before each block (accumulated forwards)
     for (int b = lane; b < NB; b += 32) {
-        double c = 0.0, d = 0.0;
+        double t[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) t[q] = 0.0;
         for (int e = boff[b]; e < boff[b + 1]; ++e) {
-            c += evq[(size_t)e * NQ];
-            d += evq[(size_t)e * NQ + 1];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) t[q] += evq[(size_t)e * NQ + q];
         }
-        btot[2 * b] = c;
-        btot[2 * b + 1] = d;
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) btot[(size_t)b * NQ + q] = t[q];
     }
     __syncwarp();
     if (lane == 0) {
@@ -257,92 +267,167 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         for (int b = NB - 1; b >= 0; --b) {
             uend[2 * b] = uc;
             uend[2 * b + 1] = us;
-            uc += btot[2 * b];
-            us += btot[2 * b + 1];
+            uc += btot[(size_t)b * NQ];
+            us += btot[(size_t)b * NQ + 1];
+        }
+    } else if (lane == 1) {
+        double p[2 * SMC];
+#pragma unroll
+        for (int q = 0; q < 2 * SMC; ++q) p[q] = 0.0;
+        for (int b = 0; b < NB; ++b) {
+#pragma unroll
+            for (int q = 0; q < 2 * SMC; ++q) {
+                pbeg[(size_t)b * 2 * SMC + q] = p[q];
+                p[q] += btot[(size_t)b * NQ + 2 + q];
+            }
         }
     }
     __syncwarp();
-    // pass 3: beta over the blocks of 32 steps (lane = step within the block)
+    // pass 3.  Blocks holding events ("event blocks") are formed one at a time
+    // with lane = step: each lane sums the events at its own step (their block
+    // offsets are compared four at a time as bytes), then warp scans give the
+    // collided sums up to and the uncollided sums after every step.  Blocks
+    // without events have constant sums: each lane forms 4 consecutive steps,
+    // 8 lanes a block, 4 such blocks at a time.
     const double ci = A.cos_t[i];
     const double vi = (i == 0 || i == A.n_cos - 1) ? 0.5 : 1.0;
     const double rf = (0.5 * (1.0 - ci * ci) * A.dphi) * (A.dcos * vi) * A.dt * (1.0 / (6.0 * CUDART_PI));
     const long col = (long)(slot / A.bpt) * A.tile_cols + (long)(slot % A.bpt) * 2 * A.S;
     Real* brow = beta + (((size_t)frame * A.n_cos + i) * A.cols_pad + col) * A.t_pad;
     const double* Dslot = A.D + (size_t)slot * A.n_t * (1 + SMC);
-    double pstart[2 * SMC];
+    const int nbase = (slot % A.bpt) * 2 * A.S;
+    float* blk_row = A.tc_layout ? reinterpret_cast<float*>(beta) +
+                                       (((size_t)frame * A.n_cos + i) * A.tiles + slot / A.bpt) * NB * 2 *
+                                           kTcBlockFloats
+                                 : nullptr;
+    // beta of coefficient set s at step k from the sums there: the table row
+    // holds the step weight times dt^3 and times a_m dt^{3-p_m} e^{-dt/w}
+    auto value = [&](int k, int s, const double* P, double Uc, double Us, double& xc, double& xs) {
+        const double* Dk = Dslot + (size_t)min(k, A.n_t - 1) * (1 + SMC);
+        double g[1 + SMC];
+        if constexpr ((1 + SMC) % 2 == 0) {
 #pragma unroll
-    for (int q = 0; q < 2 * SMC; ++q) pstart[q] = 0.0;
-    for (int b = 0; b < NB; ++b) {
-        const int k = (b << 5) + lane;
-        double Uc = uend[2 * b], Us = uend[2 * b + 1];
-        double P[2 * SMC];
-        if (boff[b] != boff[b + 1]) {  // warp-uniform: this block has events
-            // Each lane walks the block's few events (in event order): those
-            // collided at its step k_j <= k join the collided sums, the others
-            // the uncollided sum still to come; the block totals of the
-            // collided sums (every lane forms them alike) carry to the next block.
-            double uadd_c = 0.0, uadd_s = 0.0, pin[2 * SMC], ptot[2 * SMC];
-#pragma unroll
-            for (int q = 0; q < 2 * SMC; ++q) pin[q] = ptot[q] = 0.0;
-            for (int e = boff[b]; e < boff[b + 1]; ++e) {
-                const double* qe = evq + (size_t)e * NQ;
-                const bool in = evk[e] <= k;
-                if (!in) {
-                    uadd_c += qe[0];
-                    uadd_s += qe[1];
-                }
-#pragma unroll
-                for (int q = 0; q < 2 * SMC; ++q) {
-                    const double v = qe[2 + q];
-                    ptot[q] += v;
-                    if (in) pin[q] += v;
-                }
-            }
-            Uc += uadd_c;
-            Us += uadd_s;
-#pragma unroll
-            for (int q = 0; q < 2 * SMC; ++q) {
-                P[q] = pstart[q] + pin[q];
-                pstart[q] += ptot[q];
+            for (int q = 0; q < 1 + SMC; q += 2) {
+                const double2 v = __ldg(reinterpret_cast<const double2*>(Dk + q));
+                g[q] = v.x;
+                g[q + 1] = v.y;
             }
         } else {
 #pragma unroll
-            for (int q = 0; q < 2 * SMC; ++q) P[q] = pstart[q];
+            for (int q = 0; q < 1 + SMC; ++q) g[q] = __ldg(Dk + q);
         }
-        float* blk = nullptr;  // tc_layout: this bubble's block pair of step block b
-        int nbase = 0;
-        if (A.tc_layout) {
-            nbase = (slot % A.bpt) * 2 * A.S;
-            blk = reinterpret_cast<float*>(beta) +
-                  ((((size_t)frame * A.n_cos + i) * A.tiles + slot / A.bpt) * NB + b) * 2 * kTcBlockFloats;
-        }
-        if (k < A.n_t) {
-            const double* Drow = Dslot + (size_t)k * (1 + SMC);
-            const double d3 = Drow[0];
-            const double wk = rf * A.cutw[k] * ((k == 0 || k == A.n_t - 1) ? 0.5 : 1.0);
-            for (int s = 0; s < A.S; ++s) {
-                double vc = d3 * Uc, vs = d3 * Us;
+        double vc = g[0] * Uc, vs = g[0] * Us;
 #pragma unroll
-                for (int t = 0; t < SMC; ++t) {
-                    if (t / A.M != s) continue;
-                    const double f = A.coeffs[t] * Drow[1 + t];
-                    vc += f * P[2 * t];
-                    vs += f * P[2 * t + 1];
-                }
-                const bool on = d3 != 0.0;
-                const Real xc = on ? (Real)(wk * vc) : (Real)0, xs = on ? (Real)(wk * vs) : (Real)0;
-                if (A.tc_layout) {
-                    tc_store(blk, nbase + 2 * s, lane, (float)xc);
-                    tc_store(blk, nbase + 2 * s + 1, lane, (float)xs);
-                } else {
-                    brow[(size_t)(2 * s) * A.t_pad + k] = xc;
-                    brow[(size_t)(2 * s + 1) * A.t_pad + k] = xs;
+        for (int t = 0; t < SMC; ++t) {
+            if (t / A.M != s) continue;
+            vc += g[1 + t] * P[2 * t];
+            vs += g[1 + t] * P[2 * t + 1];
+        }
+        const double r = k < A.n_t ? rf : 0.0;
+        xc = r * vc;
+        xs = r * vs;
+    };
+    for (int bc = 0; bc < NB; bc += 32) {
+        const int bl = bc + lane;
+        const bool has = bl < NB && boff[bl] != boff[bl + 1];
+        const unsigned ev_blocks = __ballot_sync(full, has);
+        unsigned quiet = __ballot_sync(full, bl < NB && !has);
+        // ---- event blocks, lane = step
+        for (unsigned h = ev_blocks; h; h &= h - 1) {
+            const int b = bc + __ffs(h) - 1;
+            const int e0 = boff[b], e1 = boff[b + 1];
+            double dq[NQ];
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) dq[q] = 0.0;
+            const uint32_t pat = 0x01010101u * (uint32_t)lane;
+            for (int e4 = e0 & ~3; e4 < e1; e4 += 4) {
+                uint32_t eq = __vcmpeq4(*reinterpret_cast<const uint32_t*>(evs + e4), pat);
+                if (e4 < e0) eq &= 0xffffffffu << (8 * (e0 - e4));
+                if (e1 - e4 < 4) eq &= (1u << (8 * (e1 - e4))) - 1u;
+                while (eq) {
+                    const int by = (__ffs(eq) - 1) >> 3;
+                    eq &= ~(0xffu << (8 * by));
+                    const double* qe = evq + (size_t)(e4 + by) * NQ;
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) dq[q] += qe[q];
                 }
             }
-        } else if (A.tc_layout) {
-            for (int c = 0; c < 2 * A.S; ++c) tc_store(blk, nbase + c, lane, 0.0f);
-        } else if (k < A.t_pad) {
-            for (int c = 0; c < 2 * A.S; ++c) brow[(size_t)c * A.t_pad + k] = (Real)0;
+            // collided sums through this step (inclusive scan), uncollided after it (suffix scan)
+            double P[2 * SMC], uc = dq[0], us = dq[1];
+#pragma unroll
+            for (int q = 0; q < 2 * SMC; ++q) P[q] = dq[2 + q];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+                for (int q = 0; q < 2 * SMC; ++q) {
+                    const double v = __shfl_up_sync(full, P[q], o);
+                    if (lane >= o) P[q] += v;
+                }
+                const double vc = __shfl_down_sync(full, uc, o), vs = __shfl_down_sync(full, us, o);
+                if (lane + o < 32) {
+                    uc += vc;
+                    us += vs;
+                }
+            }
+            // uncollided after this step: the next step's inclusive suffix sum
+            double Uc = __shfl_down_sync(full, uc, 1), Us = __shfl_down_sync(full, us, 1);
+            if (lane == 31) Uc = Us = 0.0;
+            Uc += uend[2 * b];
+            Us += uend[2 * b + 1];
+#pragma unroll
+            for (int q = 0; q < 2 * SMC; ++q) P[q] = pbeg[(size_t)b * 2 * SMC + q] + P[q];
+            const int k = (b << 5) + lane;
+            for (int s2 = 0; s2 < A.S; ++s2) {
+                double xc, xs;
+                value(k, s2, P, Uc, Us, xc, xs);
+                if (A.tc_layout) {
+                    float* blk = blk_row + (size_t)b * 2 * kTcBlockFloats;
+                    tc_store(blk, nbase + 2 * s2, lane, (float)(Real)xc);
+                    tc_store(blk, nbase + 2 * s2 + 1, lane, (float)(Real)xs);
+                } else if (k < A.t_pad) {
+                    brow[(size_t)(2 * s2) * A.t_pad + k] = (Real)xc;
+                    brow[(size_t)(2 * s2 + 1) * A.t_pad + k] = (Real)xs;
+                }
+            }
+        }
+        // ---- blocks without events, 4 steps per lane
+        const int sub = lane >> 3, s0 = (lane & 7) * 4;
+        while (quiet) {
+            unsigned t = quiet;
+            for (int g = 0; g < sub && t; ++g) t &= t - 1;
+            const int b = t ? bc + __ffs(t) - 1 : -1;
+            for (int g = 0; g < 4 && quiet; ++g) quiet &= quiet - 1;
+            if (b < 0) continue;
+            const double* P = pbeg + (size_t)b * 2 * SMC;
+            const double Uc = uend[2 * b], Us = uend[2 * b + 1];
+            const int k0 = (b << 5) + s0;
+            for (int s2 = 0; s2 < A.S; ++s2) {
+                double xc[4], xs[4];
+#pragma unroll
+                for (int m = 0; m < 4; ++m) value(k0 + m, s2, P, Uc, Us, xc[m], xs[m]);
+                if (A.tc_layout) {
+                    float* blk = blk_row + (size_t)b * 2 * kTcBlockFloats;
+#pragma unroll
+                    for (int g = 0; g < 2; ++g) {
+                        const int n = nbase + 2 * s2 + g;
+                        uint32_t h[4], l[4];
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) tc::split_tf32_fast((float)(Real)(g ? xs[m] : xc[m]), h[m], l[m]);
+                        const size_t o = tc_swz(n, s0);
+                        *reinterpret_cast<uint4*>(blk + o) = make_uint4(h[0], h[1], h[2], h[3]);
+                        *reinterpret_cast<uint4*>(blk + kTcBlockFloats + o) = make_uint4(l[0], l[1], l[2], l[3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const int k = k0 + m;
+                        if (k < A.t_pad) {
+                            brow[(size_t)(2 * s2) * A.t_pad + k] = (Real)xc[m];
+                            brow[(size_t)(2 * s2 + 1) * A.t_pad + k] = (Real)xs[m];
+                        }
+                    }
+                }
+            }
         }
     }
 }
@@ -696,7 +781,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     if (n_sel > 65535) throw Error{"too many radiating bubbles for the time-table grid"};
     {
         dim3 g((unsigned)((n_t + 127) / 128), (unsigned)n_sel);
-        k_time_tables<<<g, 128, 0, dev->stream>>>(bub_frames, sel, n_sel, t_arr, n_t, powers, SM,
+        k_time_tables<<<g, 128, 0, dev->stream>>>(bub_frames, sel, n_sel, t_arr, n_t, powers, coeffs, cutw, SM,
                                                   job.has_damping ? 1 : 0, job.damping, (double*)dev->fact_D.p,
                                                   (int*)dev->fact_kfirst.p);
         CUDA_OK(cudaGetLastError());
@@ -744,8 +829,8 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         B.bpt = G.bpt;
         B.t_pad = G.t_pad;
         const int NQ = 2 + 2 * SM;
-        size_t pw = (size_t)n_phi * NQ * sizeof(double) + 4 * (size_t)G.nblk * sizeof(double) +
-                    ((size_t)n_phi + 2 * G.nblk + 1) * sizeof(int);
+        size_t pw = (size_t)n_phi * NQ * sizeof(double) + 2 * (size_t)NQ * G.nblk * sizeof(double) +
+                    ((size_t)n_phi + 2 * G.nblk + 1) * sizeof(int) + ((size_t)n_phi + 4);
         pw = (pw + 15) & ~(size_t)15;
         B.per_warp_bytes = (int)pw;
         B.tc_layout = tc ? 1 : 0;
