@@ -116,6 +116,22 @@ struct BetaArgs {
     int tiles;             // column tiles per frame (tc_layout)
 };
 
+// x^p: binary powering for integral |p| <= 32 (a few ulp), pow() otherwise.
+__device__ __forceinline__ double tpow(double x, double p) {
+    const double r = rint(p);
+    if (r == p && fabs(r) <= 32.0) {
+        unsigned n = (unsigned)fabs(r);
+        double acc = 1.0, b = x;
+        while (n) {
+            if (n & 1u) acc *= b;
+            b *= b;
+            n >>= 1;
+        }
+        return r < 0.0 ? 1.0 / acc : acc;
+    }
+    return pow(x, p);
+}
+
 // One beta value into the tensor-core GEMM's block layout: the hi and lo TF32
 // parts at (column n, step kk) of the block pair at `blk`.
 __device__ __forceinline__ void tc_store(float* blk, int n, int kk, float x) {
@@ -230,7 +246,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             const double ed = A.has_damp ? exp(tj / A.damp) : 1.0;
 #pragma unroll
             for (int t = 0; t < SMC; ++t) {
-                const double f = pow(tj, A.powers[t]) * ed;
+                const double f = tpow(tj, A.powers[t]) * ed;
                 q[2 + 2 * t] = qc * f;
                 q[3 + 2 * t] = qs * f;
             }
@@ -247,39 +263,85 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         pass2(j0 + lane, kj, b);
     }
     __syncwarp();
-    // block totals of every weight (each in event order); then the uncollided
-    // sums after each block (accumulated backwards) and the collided sums
-    // before each block (accumulated forwards)
-    for (int b = lane; b < NB; b += 32) {
-        double t[NQ];
+    // block totals of every weight: the lanes take a block's events in strides
+    // of 32 and a butterfly reduction adds the lane sums (a fixed order for a
+    // given event count); then the collided sums before each block (exclusive
+    // prefix over blocks) and the uncollided sums after each block (exclusive
+    // suffix plus the never-colliding weights), as warp scans over lanes = blocks
+    for (int b = lane; b < NB; b += 32)
+        if (boff[b] == boff[b + 1]) {
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) t[q] = 0.0;
-        for (int e = boff[b]; e < boff[b + 1]; ++e) {
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) t[q] += evq[(size_t)e * NQ + q];
+            for (int q = 0; q < NQ; ++q) btot[(size_t)b * NQ + q] = 0.0;
         }
+    for (int bc = 0; bc < NB; bc += 32) {
+        const int bl = bc + lane;
+        for (unsigned h = __ballot_sync(full, bl < NB && boff[bl] != boff[bl + 1]); h; h &= h - 1) {
+            const int b = bc + __ffs(h) - 1;
+            double t[NQ];
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) btot[(size_t)b * NQ + q] = t[q];
+            for (int q = 0; q < NQ; ++q) t[q] = 0.0;
+            for (int e = boff[b] + lane; e < boff[b + 1]; e += 32) {
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) t[q] += evq[(size_t)e * NQ + q];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) t[q] += __shfl_xor_sync(full, t[q], o);
+            }
+            if (lane == 0) {
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) btot[(size_t)b * NQ + q] = t[q];
+            }
+        }
     }
     __syncwarp();
-    if (lane == 0) {
-        double uc = nc, us = ns;
-        for (int b = NB - 1; b >= 0; --b) {
-            uend[2 * b] = uc;
-            uend[2 * b + 1] = us;
-            uc += btot[(size_t)b * NQ];
-            us += btot[(size_t)b * NQ + 1];
-        }
-    } else if (lane == 1) {
-        double p[2 * SMC];
+    {
+        double carry[2 * SMC];
 #pragma unroll
-        for (int q = 0; q < 2 * SMC; ++q) p[q] = 0.0;
-        for (int b = 0; b < NB; ++b) {
+        for (int q = 0; q < 2 * SMC; ++q) carry[q] = 0.0;
+        for (int bc = 0; bc < NB; bc += 32) {
+            const int b = bc + lane;
+            double v[2 * SMC];
+#pragma unroll
+            for (int q = 0; q < 2 * SMC; ++q) v[q] = b < NB ? btot[(size_t)b * NQ + 2 + q] : 0.0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+#pragma unroll
+                for (int q = 0; q < 2 * SMC; ++q) {
+                    const double u = __shfl_up_sync(full, v[q], o);
+                    if (lane >= o) v[q] += u;
+                }
+            }
 #pragma unroll
             for (int q = 0; q < 2 * SMC; ++q) {
-                pbeg[(size_t)b * 2 * SMC + q] = p[q];
-                p[q] += btot[(size_t)b * NQ + 2 + q];
+                double ex = __shfl_up_sync(full, v[q], 1);
+                if (lane == 0) ex = 0.0;
+                if (b < NB) pbeg[(size_t)b * 2 * SMC + q] = carry[q] + ex;
+                carry[q] += __shfl_sync(full, v[q], 31);
             }
+        }
+        // the never-colliding sums were reduced into lane 0
+        double cc = __shfl_sync(full, nc, 0), cs = __shfl_sync(full, ns, 0);
+        for (int bc = ((NB - 1) >> 5) << 5; bc >= 0; bc -= 32) {
+            const int b = bc + lane;
+            double vc = b < NB ? btot[(size_t)b * NQ] : 0.0, vs = b < NB ? btot[(size_t)b * NQ + 1] : 0.0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const double uc = __shfl_down_sync(full, vc, o), us = __shfl_down_sync(full, vs, o);
+                if (lane + o < 32) {
+                    vc += uc;
+                    vs += us;
+                }
+            }
+            double xc = __shfl_down_sync(full, vc, 1), xs = __shfl_down_sync(full, vs, 1);
+            if (lane == 31) xc = xs = 0.0;
+            if (b < NB) {
+                uend[2 * b] = cc + xc;
+                uend[2 * b + 1] = cs + xs;
+            }
+            cc += __shfl_sync(full, vc, 0);
+            cs += __shfl_sync(full, vs, 0);
         }
     }
     __syncwarp();
