@@ -69,6 +69,7 @@ struct DevBuf {
 
 struct Device {
     int id = 0;
+    int n_sm = 148;                 // multiprocessors of this device
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;  // own_stream or a caller-provided stream
     cudaEvent_t ev[8] = {};

@@ -43,6 +43,7 @@ Device* device_create() {
     auto* d = new Device();
     try {
         CUDA_OK(cudaGetDevice(&d->id));
+        CUDA_OK(cudaDeviceGetAttribute(&d->n_sm, cudaDevAttrMultiProcessorCount, d->id));
         CUDA_OK(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
         d->stream = d->own_stream;
         for (auto& e : d->ev) CUDA_OK(cudaEventCreate(&e));

@@ -927,7 +927,11 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     A.bpt = G.bpt;
     A.tiles_per_frame = G.tiles_per_frame;
     const size_t per = (size_t)2 * S * n_w;
-    dev->fact_partial.ensure((size_t)kn * G.tiles_per_frame * per * sizeof(double2));
+    // tensor-core path: each column tile's CTAs split the cos-theta rows so that
+    // the grid fills whole waves of one CTA per SM
+    const int row_parts =
+        tc ? tc_row_parts((size_t)((n_w + 63) / 64) * kn * G.tiles_per_frame, n_cos, dev->n_sm) : 1;
+    dev->fact_partial.ensure((size_t)kn * G.tiles_per_frame * row_parts * per * sizeof(double2));
     A.partial = (double2*)dev->fact_partial.p;
     if (tc) {
         // time-phase table: frame independent, rebuilt only when w, cos-theta or t change
@@ -966,13 +970,14 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         T.nkb = nkb;
         T.bpt = G.bpt;
         T.tiles_per_frame = G.tiles_per_frame;
+        T.row_parts = row_parts;
         T.partial = A.partial;
         T.err = reinterpret_cast<unsigned int*>(static_cast<unsigned char*>(dev->counters.p) + 8);
         launch_gemm_tc(T, kn, dev->stream);
         ++launches;
         CUDA_OK(cudaEventRecord(ev3[2], dev->stream));
         dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
-        k_reduce_tiles<<<gr, 256, 0, dev->stream>>>(A.partial, G.tiles_per_frame, per, (int)kn, out);
+        k_reduce_tiles<<<gr, 256, 0, dev->stream>>>(A.partial, G.tiles_per_frame * row_parts, per, (int)kn, out);
         CUDA_OK(cudaGetLastError());
         ++launches;
         return launches;
@@ -1013,7 +1018,9 @@ size_t factored_bytes_per_frame(const SpectrumJob& job) {
     const size_t beta = job.kernel == BGWX_KERNEL_MIXED
                             ? (size_t)job.n_cos * G.tiles_per_frame * G.nblk * 2 * kTcBlockFloats * sizeof(float)
                             : (size_t)job.n_cos * G.cols_pad * G.t_pad * real;
-    return beta + (size_t)G.tiles_per_frame * 2 * job.n_sets * job.n_w * sizeof(double2);
+    // partials: up to 16 row parts per column tile on the tensor-core path
+    const size_t parts = job.kernel == BGWX_KERNEL_MIXED ? 16 : 1;
+    return beta + (size_t)G.tiles_per_frame * parts * 2 * job.n_sets * job.n_w * sizeof(double2);
 }
 
 }  // namespace bgw

@@ -36,6 +36,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <string>
 #include <type_traits>
@@ -128,8 +130,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int wt = blockIdx.x;
     const int w0 = wt * kTcWT;
-    const int frame = blockIdx.y / A.tiles_per_frame;
-    const int tile = blockIdx.y % A.tiles_per_frame;
+    // blockIdx.y = (frame, tile, part): part p takes the rows [i0, i1)
+    const int part_ = blockIdx.y % A.row_parts;
+    const int frame = blockIdx.y / A.row_parts / A.tiles_per_frame;
+    const int tile = (blockIdx.y / A.row_parts) % A.tiles_per_frame;
+    const int i0 = A.n_cos * part_ / A.row_parts, i1 = A.n_cos * (part_ + 1) / A.row_parts;
     const D4* B = A.bub + (size_t)frame * A.n_tot;
 
     if (tid < 64) {
@@ -178,7 +183,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
         // ---------------- bulk-copy producer ----------------
         if (lane == 0 && active) {
             int it = 0;
-            for (int i = 0; i < A.n_cos && !failed; ++i) {
+            for (int i = i0; i < i1 && !failed; ++i) {
                 const float* arow = A.atab + ((size_t)(i * A.n_wt + wt) * nkb) * 2 * kTcBlockFloats;
                 const float* brow =
                     A.btab + ((((size_t)frame * A.n_cos + i) * A.tiles_per_frame + tile) * nkb) * 2 * kTcBlockFloats;
@@ -209,7 +214,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
         if (lane == 0 && active) {
             const uint32_t idesc = tc::idesc_tf32(kTcRows, kTcCols);
             int it = 0, seg = 0;
-            for (int i = 0; i < A.n_cos && !failed; ++i) {
+            for (int i = i0; i < i1 && !failed; ++i) {
                 uint32_t dcol = 0, accumulate = 0;
                 for (int kb = kb0; kb < nkb; ++kb, ++it) {
                     if ((kb - kb0) % kTcFoldKB == 0) {  // a new accumulation segment
@@ -280,7 +285,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
             constexpr int b_lo = c_lo / CPB, b_hi = (c_lo + kTcCols / 2 - 1) / CPB;
             constexpr int nb = b_hi - b_lo + 1;
             int seg = 0;
-            for (int i = 0; active && i < A.n_cos && !failed; ++i) {
+            for (int i = i0; active && i < i1 && !failed; ++i) {
                 // e^{i w (t_a c_i - z_a)} per (w, bubble) of this row; zero for empty columns.
                 // Each warp fills the entries it reads (its 16 frequencies, its bubbles).
                 const double ci = A.cos_t[i];
@@ -370,8 +375,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
                 const double os = __shfl_xor_sync(0xffffffffu, as, 1);
                 if (part == 0 && wi < A.n_w) {
                     const int s_ = sg >> 1, g = sg & 1;
-                    const size_t o =
-                        ((((size_t)frame * A.tiles_per_frame + tile) * 2 + g) * S + s_) * A.n_w + wi;
+                    const size_t o = (((((size_t)frame * A.tiles_per_frame + tile) * A.row_parts + part_) * 2 + g) * S +
+                                       s_) * A.n_w + wi;
                     A.partial[o] = make_double2(ac - os, oc + as);
                 }
             }
@@ -407,10 +412,27 @@ void launch_tc_phase_table(const double* w, const double* cos_t, const double* t
     CUDA_OK(cudaGetLastError());
 }
 
+int tc_row_parts(size_t n_ctas, int n_cos, int n_sm) {
+    int best = 1;
+    double best_eff = 0.0;
+    const int max_parts = std::max(1, std::min(16, n_cos / 8));
+    for (int p = 1; p <= max_parts; ++p) {
+        const double c = (double)n_ctas * p;
+        const double waves = std::ceil(c / n_sm);
+        const double eff = c / (waves * n_sm);
+        if (eff > best_eff + 0.01) {
+            best_eff = eff;
+            best = p;
+        }
+    }
+    return best;
+}
+
 void launch_gemm_tc(const TcArgs& A, size_t kn, cudaStream_t st) {
     if (A.bpt * 2 * A.S > kTcCols) throw Error{"tensor-core GEMM: too many columns per tile"};
+    if (A.row_parts < 1 || A.row_parts > A.n_cos) throw Error{"tensor-core GEMM: bad row split"};
     const size_t smem = SmemLayout::total + 1024;
-    const size_t gy = kn * (size_t)A.tiles_per_frame;
+    const size_t gy = kn * (size_t)A.tiles_per_frame * A.row_parts;
     if (gy > 65535) throw Error{"too many column tiles in one k-hat chunk"};
     dim3 grid((unsigned)A.n_wt, (unsigned)gy);
     switch (A.S) {

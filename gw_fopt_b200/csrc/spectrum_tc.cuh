@@ -28,7 +28,8 @@ struct TcArgs {
     int n_wt, nkb;
     int bpt;                // bubbles per 128-column tile
     int tiles_per_frame;
-    double2* partial;       // (kn, tiles_per_frame, 2, S, W)
+    int row_parts;          // CTAs per (frequency tile, column tile), each over a range of cos-theta rows
+    double2* partial;       // (kn, tiles_per_frame, row_parts, 2, S, W)
     unsigned int* err;      // set non-zero when a pipeline wait gave up
 };
 
@@ -39,5 +40,9 @@ void launch_tc_phase_table(const double* w, const double* cos_t, const double* t
 
 // Launches the GEMM + epilogue for kn frames on `st`.
 void launch_gemm_tc(const TcArgs& A, size_t kn, cudaStream_t st);
+
+// Row parts that make n_ctas x parts CTAs fill whole waves of one CTA per SM
+// best (at most n_cos / 8 parts).
+int tc_row_parts(size_t n_ctas, int n_cos, int n_sm);
 
 }  // namespace bgw
