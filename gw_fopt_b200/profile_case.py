@@ -1,6 +1,6 @@
 """One spectrum call of a synthetic workload, for profiling (ncu) and timing.
 
-    python -m gw_fopt_b200.profile_case --config 3 --kernel mixed --khat 1 --bubbles 512 [--reps 1]
+    python -m gw_fopt_b200.profile_case --config 3 --kernel mixed --khat 1 --bubbles 512 [--reps 1] [--n-t 256]
     python -m gw_fopt_b200.profile_case --config 4 --kernel mixed --khat 64 --realizations 256 [--compare 4]
     python -m gw_fopt_b200.profile_case --config 5 --kernel mixed --khat 32 --fit-steps 5
 
@@ -37,6 +37,7 @@ def main():
     ap.add_argument("--realizations", type=int, default=256)
     ap.add_argument("--compare", type=int, default=0)
     ap.add_argument("--fit-steps", type=int, default=3)
+    ap.add_argument("--n-t", type=int, default=0, help="override the configuration's time steps (smaller captures)")
     a = ap.parse_args()
     if a.config == 4:
         return run_ensemble(a)
@@ -50,12 +51,13 @@ def main():
     sel = np.arange(a.bubbles) if a.bubbles else None
     for r in range(a.reps):
         t0 = time.perf_counter()
-        out = g.compute_c_integral_khat(c.w, c.khat, t_begin=c.t_begin, t_end=c.t_end, n_t=c.n_t,
+        n_t = a.n_t or c.n_t
+        out = g.compute_c_integral_khat(c.w, c.khat, t_begin=c.t_begin, t_end=c.t_end, n_t=n_t,
                                         selected_bubbles=sel)
         wall = time.perf_counter() - t0
         t = g.last_timings()
         n_rad = a.bubbles or c.n
-        pte = c.khat.shape[0] * n_rad * c.n_cos * c.n_phi * c.n_t
+        pte = c.khat.shape[0] * n_rad * c.n_cos * c.n_phi * n_t
         print(json.dumps({"rep": r, "config": c.name, "kernel": a.kernel, "khat": int(c.khat.shape[0]),
                           "radiating": int(n_rad), "wall_s": wall, "masks_ms": t["masks_ms"],
                           "spectrum_ms": t["spectrum_ms"], "total_ms": t["total_ms"], "fallbacks": t["fallbacks"],
