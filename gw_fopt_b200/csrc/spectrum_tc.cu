@@ -302,6 +302,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
                     etab[eslot(l, b)] = e;
                 }
                 __syncwarp();
+                // this lane's phases for the whole row stay in registers
+                float2 evr[nb];
+#pragma unroll
+                for (int j = 0; j < nb; ++j) evr[j] = etab[eslot(wl, b_lo + j)];
                 const int nseg = (nkb - kb0 + kTcFoldKB - 1) / kTcFoldKB;
                 for (int g = 0; g < nseg; ++g, ++seg) {
                     const int buf = seg & 1;
@@ -313,11 +317,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
                     // columns [n0, n0 + 32) from y; the chunk's phases are loaded first
                     auto consume = [&](const uint32_t (&y)[32], auto n0_c) {
                         constexpr int n0 = decltype(n0_c)::value;
-                        constexpr int b_first = n0 / CPB;
-                        constexpr int NB = (n0 + 31) / CPB - b_first + 1;
-                        float2 ev[NB];
-#pragma unroll
-                        for (int j = 0; j < NB; ++j) ev[j] = etab[eslot(wl, b_first + j)];
                         float pc[2][CPB], ps[2][CPB];
 #pragma unroll
                         for (int c = 0; c < CPB; ++c) pc[0][c] = ps[0][c] = pc[1][c] = ps[1][c] = 0.f;
@@ -325,7 +324,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
                         for (int c = 0; c < 32; ++c) {
                             const int n = n0 + c;
                             const int b = n / CPB, sc = n % CPB, h2 = b & 1;
-                            const float2 e = ev[b - b_first];
+                            const float2 e = evr[b - b_lo];
                             const float yv = __uint_as_float(y[c]);
                             pc[h2][sc] = fmaf(e.x, yv, pc[h2][sc]);
                             ps[h2][sc] = fmaf(e.y, yv, ps[h2][sc]);
