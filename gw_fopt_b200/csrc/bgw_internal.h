@@ -110,6 +110,13 @@ void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_
 
 int device_count();
 
+// Energy spectrum per k-hat and its cos(theta_k) integral (postprocess.cu).
+// c: (K, 2, S, W) complex128, on the device or the host; w (W), set weights
+// (S) and x = sorted cos(theta_k) (K) on the host; spectra (K, W) may be null.
+void run_power_spectrum(Device* dev, const void* c, bool c_on_device, size_t K, size_t S, size_t W,
+                        const double* w, const double* a, const double* x_sorted, double* spectra, double* de,
+                        bool out_on_device);
+
 // Thread-local message of bgw_last_error_message (capi.cpp).
 void set_last_error(std::string message);
 void clear_last_error();

@@ -520,6 +520,57 @@ BgwStatus bgwx_generalized_bulk_flow_spectrum_vjp(bgw_generalized_bulk_flow* bul
     });
 }
 
+namespace {
+// Validates the post-processing arguments and returns x = sorted cos(theta_k)
+// (data_gw_bulkflow.py:23: np.sort of the rows' cos_theta_k).
+std::vector<double> power_spectrum_args(size_t n_khat, size_t n_sets, const double* w_arr, size_t n_w,
+                                        const double* set_weights, const double* cos_thetak) {
+    if (n_khat == 0) throw Error{"cos_thetak must hold at least one direction"};
+    if (n_sets == 0) throw Error{"n_sets must be > 0"};
+    slice(w_arr, n_w, "w_arr");
+    const double* a = slice(set_weights, n_sets, "set_weights");
+    const double* ck = slice(cos_thetak, n_khat, "cos_thetak");
+    checked_mul(checked_mul(checked_mul(n_khat, 2, "c"), n_sets, "c"), n_w, "c");
+    for (size_t s = 0; s < n_sets; ++s)
+        if (!std::isfinite(a[s])) throw Error{"set_weights must be finite"};
+    std::vector<double> x(ck, ck + n_khat);
+    for (double v : x)
+        if (std::isnan(v)) throw Error{"cos_thetak must not contain NaN"};
+    std::sort(x.begin(), x.end());
+    return x;
+}
+}  // namespace
+
+BgwStatus bgwx_generalized_bulk_flow_power_spectrum(bgw_generalized_bulk_flow* bulk_flow, const BgwComplex64* c,
+                                                    size_t n_khat, size_t n_sets, const double* w_arr, size_t n_w,
+                                                    const double* set_weights, const double* cos_thetak,
+                                                    double* spectra, double* de_dlogw) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        const std::vector<double> x = power_spectrum_args(n_khat, n_sets, w_arr, n_w, set_weights, cos_thetak);
+        if (n_w == 0) return;
+        const BgwComplex64* pc = slice(c, n_khat * 2 * n_sets * n_w, "c");
+        if (!de_dlogw) throw Error{"de_dlogw must not be null"};
+        bgw::run_power_spectrum(device(h), pc, false, n_khat, n_sets, n_w, w_arr, set_weights, x.data(), spectra,
+                                de_dlogw, false);
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_power_spectrum_device(bgw_generalized_bulk_flow* bulk_flow,
+                                                           const void* c_device, size_t n_khat, size_t n_sets,
+                                                           const double* w_arr, size_t n_w,
+                                                           const double* set_weights, const double* cos_thetak,
+                                                           void* spectra_device, void* de_dlogw_device) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        const std::vector<double> x = power_spectrum_args(n_khat, n_sets, w_arr, n_w, set_weights, cos_thetak);
+        if (n_w == 0) return;
+        if (!c_device || !de_dlogw_device) throw Error{"c_device and de_dlogw_device must not be null"};
+        bgw::run_power_spectrum(device(h), c_device, true, n_khat, n_sets, n_w, w_arr, set_weights, x.data(),
+                                static_cast<double*>(spectra_device), static_cast<double*>(de_dlogw_device), true);
+    });
+}
+
 BgwStatus bgwx_generalized_bulk_flow_set_bubbles(bgw_generalized_bulk_flow* bulk_flow, const double* interior,
                                                  size_t n_interior, const double* exterior, size_t n_exterior) {
     return run_ffi([&] {

@@ -79,6 +79,7 @@ struct Device {
     DevBuf tau, codes, partial, out, counters, nblists;
     DevBuf fact_D, fact_kfirst, beta, fact_partial;  // factored-kernel work arrays
     DevBuf ens_out;                                  // batched ensemble: all realizations' spectra
+    DevBuf pp_in, pp_small, pp_out;                  // spectrum post-processing: input, small tables, output
     DevBuf tc_atab;                                  // tensor-core GEMM: time-phase table
     std::vector<double> tc_key;                      // (n_w, n_cos, n_t, w, cos-theta, t) of tc_atab
     DevBuf adj_gbar, adj_scratch, adj_grad, adj_mtab; // adjoint: cotangents, work arrays, gradients, phases

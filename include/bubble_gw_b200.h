@@ -194,6 +194,33 @@ BgwStatus bgwx_generalized_bulk_flow_compute_c_integrand(bgw_generalized_bulk_fl
                                                          size_t n_selected_bubbles, BgwComplex64 *out,
                                                          size_t out_len);
 
+/* Energy spectrum of bulk-flow output, the post-processing the reference's
+ * consumer applies to compute_c_integral results
+ * (src/gw_fopt/bubble_dynamics/utils/data_gw_bulkflow.py:26-146,
+ * DataGwBulkFlow.de_dlogw_dcosthetak and de_dlogw), on this handle's GPU:
+ *   C_+/x(w) = sum_s set_weights[s] C_{+/x,s}(w)          (sets with weight 0 are skipped)
+ *   spectra[k, w] = 8 pi w^3 (|C_+|^2 + |C_x|^2)           per k-hat direction k
+ *   de_dlogw[w]   = 2 trapezoid(spectra[:, w], x = sorted(cos_thetak))
+ * The rows enter the trapezoid in the order given (the reference sorts only x).
+ * c: (n_khat, 2, n_sets, n_w) complex128 (the layout of
+ * bgwx_generalized_bulk_flow_compute_c_integral_khat); spectra: (n_khat, n_w)
+ * or NULL; de_dlogw: (n_w).  Host pointers.  Errors: CalculationError. */
+BgwStatus bgwx_generalized_bulk_flow_power_spectrum(bgw_generalized_bulk_flow *bulk_flow, const BgwComplex64 *c,
+                                                    size_t n_khat, size_t n_sets, const double *w_arr, size_t n_w,
+                                                    const double *set_weights, const double *cos_thetak,
+                                                    double *spectra, double *de_dlogw);
+
+/* The same with c, spectra and de_dlogw in device memory (for example the
+ * output of bgwx_generalized_bulk_flow_compute_c_integral_khat_device), so the
+ * spectrum never leaves the GPU; w_arr, set_weights and cos_thetak are host
+ * arrays.  Runs on the handle's stream and returns when the results are
+ * written.  No counterpart in the reference. */
+BgwStatus bgwx_generalized_bulk_flow_power_spectrum_device(bgw_generalized_bulk_flow *bulk_flow,
+                                                           const void *c_device, size_t n_khat, size_t n_sets,
+                                                           const double *w_arr, size_t n_w,
+                                                           const double *set_weights, const double *cos_thetak,
+                                                           void *spectra_device, void *de_dlogw_device);
+
 /* Runs this handle's device work on `stream` (a cudaStream_t created by the
  * caller; NULL selects the handle's own non-blocking stream, so the legacy
  * default stream cannot be chosen).  No counterpart in the reference. */
@@ -223,7 +250,7 @@ BgwStatus bgwx_measure_compute_peaks(double *fp64_flops, double *fp32_flops, dou
  *   d_delta_tab (n_selected, n_dirs) f64 out.
  * The work runs on `stream` (a cudaStream_t, NULL = legacy default stream) and
  * is left in flight.  The library's only work array, the per-bubble candidate
- * lists, is a fixed static device array of 512 entries (about 0.8 MB on every
+ * lists, is a fixed static device array of 512 entries (about 3.2 MB on every
  * GPU that loads the library, until exit); more than 512 selected bubbles is
  * rejected with an error.  The first call on each device looks up that array's
  * device address, so make the first call before any stream capture.  All calls
