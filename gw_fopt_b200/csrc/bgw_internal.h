@@ -110,6 +110,13 @@ void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_
 
 int device_count();
 
+// Exponential-rate nucleation of R realizations on the GPU (nucleation.cu).
+// interior (sum n, 4), exterior (6 sum n, 4), rows of realization r from the
+// running sum of n; attempts (R): prefactor doublings used + 1, or -1.
+void run_nucleation(const int64_t* n, const double* beta, const uint64_t* seed, size_t R, double L,
+                    double gamma_scale, int64_t max_rejections, int max_attempts, double* interior,
+                    double* exterior, int32_t* attempts);
+
 // Energy spectrum per k-hat and its cos(theta_k) integral (postprocess.cu).
 // c: (K, 2, S, W) complex128, on the device or the host; w (W), set weights
 // (S) and x = sorted cos(theta_k) (K) on the host; spectra (K, W) may be null.

@@ -571,6 +571,43 @@ BgwStatus bgwx_generalized_bulk_flow_power_spectrum_device(bgw_generalized_bulk_
     });
 }
 
+BgwStatus bgwx_nucleate_exponential(const int64_t* n_bubbles, const double* beta, const uint64_t* seeds,
+                                    size_t n_realizations, double box_side, double gamma_scale,
+                                    size_t max_rejections, double* interior, size_t interior_len, double* exterior,
+                                    size_t exterior_len, int32_t* attempts) {
+    return run_ffi([&] {
+        const size_t R = n_realizations;
+        const int64_t* n = slice(n_bubbles, R, "n_bubbles");
+        const double* b = slice(beta, R, "beta");
+        const uint64_t* sd = slice(seeds, R, "seeds");
+        if (!(box_side > 0.0) || !std::isfinite(box_side)) throw Error{"box_side must be positive and finite"};
+        if (!(gamma_scale > 0.0) || !std::isfinite(gamma_scale)) throw Error{"gamma_scale must be positive and finite"};
+        if (max_rejections == 0 || max_rejections > (size_t)INT64_MAX) throw Error{"max_rejections must be > 0"};
+        size_t rows = 0;
+        for (size_t r = 0; r < R; ++r) {
+            if (n[r] < 0) throw Error{"n_bubbles must be >= 0"};
+            if (!(b[r] > 0.0) || !std::isfinite(b[r])) throw Error{"beta must be positive and finite"};
+            rows += (size_t)n[r];
+        }
+        if (interior_len != checked_mul(rows, 4, "interior") || exterior_len != checked_mul(rows, 24, "exterior"))
+            throw Error{"interior_len / exterior_len must be 4 and 24 times the total bubble count " +
+                        std::to_string(rows)};
+        std::vector<int32_t> att(R, 0);
+        if (rows) {
+            slice(interior, interior_len, "interior");
+            slice(exterior, exterior_len, "exterior");
+        }
+        bgw::run_nucleation(n, b, sd, R, box_side, gamma_scale, (int64_t)max_rejections, 40, interior, exterior,
+                            att.data());
+        for (size_t r = 0; r < R; ++r)
+            if (att[r] < 0)
+                throw Error{"realization " + std::to_string(r) +
+                            ": the false vacuum ran out before every bubble was placed, after 40 doublings of "
+                            "the rate prefactor"};
+        if (attempts) std::memcpy(attempts, att.data(), R * sizeof(int32_t));
+    });
+}
+
 BgwStatus bgwx_generalized_bulk_flow_set_bubbles(bgw_generalized_bulk_flow* bulk_flow, const double* interior,
                                                  size_t n_interior, const double* exterior, size_t n_exterior) {
     return run_ffi([&] {

@@ -36,6 +36,8 @@ def main():
     ap.add_argument("--reps", type=int, default=1)
     ap.add_argument("--realizations", type=int, default=256)
     ap.add_argument("--compare", type=int, default=0)
+    ap.add_argument("--device-nucleation", action="store_true",
+                    help="config 4: draw the realizations on the GPU (gw_fopt_b200.nucleation)")
     ap.add_argument("--fit-steps", type=int, default=3)
     ap.add_argument("--n-t", type=int, default=0, help="override the configuration's time steps (smaller captures)")
     a = ap.parse_args()
@@ -67,8 +69,12 @@ def main():
 def run_ensemble(a):
     from .ensemble import BulkFlowEnsemble
     t0 = time.perf_counter()
-    c = W.ensemble_config(k_subset=a.khat)
-    c.realizations = c.realizations[:a.realizations]
+    if a.device_nucleation:
+        from .nucleation import ensemble_config_device
+        c = ensemble_config_device(n_real=a.realizations, k_subset=a.khat)
+    else:
+        c = W.ensemble_config(k_subset=a.khat)
+        c.realizations = c.realizations[:a.realizations]
     gen_s = time.perf_counter() - t0
 
     def make(kernel, reals):

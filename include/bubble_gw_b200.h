@@ -194,6 +194,25 @@ BgwStatus bgwx_generalized_bulk_flow_compute_c_integrand(bgw_generalized_bulk_fl
                                                          size_t n_selected_bubbles, BgwComplex64 *out,
                                                          size_t out_len);
 
+/* Draws the bubbles of n_realizations nucleation Monte Carlo realizations on
+ * the GPU (one block per realization): exponential-rate nucleation in a
+ * periodic cube of side box_side, candidates arriving as a Poisson process
+ * with rate Gamma0 V e^{beta t} (Gamma0 V / beta = gamma_scale n), rejected
+ * inside an accepted bubble's wall at the nearest periodic copy, the rejection
+ * against bubbles and images of the reference's
+ * rust/bubble-gw/src/many_bubbles/bubbles_nucleation/fixed_rate_nucleation.rs;
+ * after max_rejections rejections the prefactor doubles and the draw restarts
+ * (at most 40 times).  Random numbers: Philox4x32-10 keyed by seeds[r].
+ * interior: (sum n, 4) rows [t, x, y, z], times relative to each realization's
+ * first bubble; exterior: (6 sum n, 4), the +x, -x, +y, -y, +z, -z images of
+ * every bubble; attempts (n_realizations, may be NULL): prefactor attempts
+ * used.  The ensemble sampler of the benchmark configurations, moved to the
+ * device; no counterpart in the reference's C ABI. */
+BgwStatus bgwx_nucleate_exponential(const int64_t *n_bubbles, const double *beta, const uint64_t *seeds,
+                                    size_t n_realizations, double box_side, double gamma_scale,
+                                    size_t max_rejections, double *interior, size_t interior_len, double *exterior,
+                                    size_t exterior_len, int32_t *attempts);
+
 /* Energy spectrum of bulk-flow output, the post-processing the reference's
  * consumer applies to compute_c_integral results
  * (src/gw_fopt/bubble_dynamics/utils/data_gw_bulkflow.py:26-146,
