@@ -36,6 +36,9 @@ struct SpectrumJob {
     const double* dirs = nullptr;
     const double* sin2phi = nullptr;  // sin(2 phi_j)
     const double* cos2phi = nullptr;  // cos(2 phi_j)
+    const double* sinphi = nullptr;   // sin(phi_j), cos(phi_j): the tensor form
+    const double* cosphi = nullptr;
+    bool tensor = false;              // NewGeneralizedBulkFlow: (6, S, W) per k-hat, FP64 direct only
     // scaling functions
     size_t n_sets = 0, n_terms = 0;
     const double* coeffs = nullptr;

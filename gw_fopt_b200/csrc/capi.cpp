@@ -26,7 +26,7 @@ struct bgw_generalized_bulk_flow {
     bool has_res = false;
     bool precompute = false;
     size_t n_cos = 0, n_phi = 0;
-    std::vector<double> cos_thetax, phix, dirs, sin2phi, cos2phi;
+    std::vector<double> cos_thetax, phix, dirs, sin2phi, cos2phi, sinphi, cosphi;
     // generalized_bulk_flow.rs:98-99 defaults: coefficients [[1.0]], powers [[3.0]]
     size_t n_sets = 1, n_terms = 1;
     std::vector<double> coeffs{1.0}, powers{3.0};
@@ -158,6 +158,8 @@ bgw::SpectrumJob settings_job(const bgw_generalized_bulk_flow* h, const std::vec
     job.dirs = h->dirs.data();
     job.sin2phi = h->sin2phi.data();
     job.cos2phi = h->cos2phi.data();
+    job.sinphi = h->sinphi.data();
+    job.cosphi = h->cosphi.data();
     job.n_sets = h->n_sets;
     job.n_terms = h->n_terms;
     job.coeffs = h->coeffs.data();
@@ -321,6 +323,12 @@ BgwStatus bgw_generalized_bulk_flow_set_resolution(bgw_generalized_bulk_flow* bu
         }
         h->sin2phi.resize(n_phix);
         h->cos2phi.resize(n_phix);
+        h->sinphi.resize(n_phix);
+        h->cosphi.resize(n_phix);
+        for (size_t j = 0; j < n_phix; ++j) {  // new_generalized_bulk_flow.rs:640-644
+            h->sinphi[j] = std::sin(h->phix[j]);
+            h->cosphi[j] = std::cos(h->phix[j]);
+        }
         for (size_t j = 0; j < n_phix; ++j) {
             h->sin2phi[j] = std::sin(2.0 * h->phix[j]);
             h->cos2phi[j] = std::cos(2.0 * h->phix[j]);
@@ -568,6 +576,61 @@ BgwStatus bgwx_generalized_bulk_flow_power_spectrum_device(bgw_generalized_bulk_
         if (!c_device || !de_dlogw_device) throw Error{"c_device and de_dlogw_device must not be null"};
         bgw::run_power_spectrum(device(h), c_device, true, n_khat, n_sets, n_w, w_arr, set_weights, x.data(),
                                 static_cast<double*>(spectra_device), static_cast<double*>(de_dlogw_device), true);
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_compute_c_tensor_khat(bgw_generalized_bulk_flow* bulk_flow, const double* w_arr,
+                                                          size_t n_w, bool has_t_begin, double t_begin, double t_end,
+                                                          size_t n_t, const double* khat, size_t n_khat,
+                                                          const size_t* selected_bubbles, size_t n_selected_bubbles,
+                                                          BgwComplex64* out, size_t out_len) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        const double* w = slice(w_arr, n_w, "w_arr");
+        const size_t K = khat ? n_khat : 1;
+        if (khat && n_khat == 0) throw Error{"khat must hold at least one direction"};
+        std::vector<double> rot = khat ? khat_rotations(khat, n_khat) : std::vector<double>();
+        const size_t S = h->n_sets;
+        const size_t expected = checked_mul(checked_mul(checked_mul(K, 6, "out"), S, "out"), n_w, "out");
+        if (out_len != expected)
+            throw Error{"out_len=" + std::to_string(out_len) + " does not match expected length " +
+                        std::to_string(expected)};
+        if (n_t < 2) throw Error{"n_t must be >= 2 for integration"};
+        std::vector<uint32_t> ids;
+        if (selected_bubbles) {
+            const size_t* sel = slice(selected_bubbles, n_selected_bubbles, "selected_bubbles");
+            for (size_t q = 0; q < n_selected_bubbles; ++q) {
+                if (sel[q] >= h->n_int) {
+                    Error e{"Index " + std::to_string(sel[q]) + " out of bounds for max " + std::to_string(h->n_int)};
+                    e.index_error = true;
+                    throw e;
+                }
+                ids.push_back((uint32_t)sel[q]);
+            }
+        } else {
+            for (size_t a = 0; a < h->n_int; ++a) ids.push_back((uint32_t)a);
+        }
+        std::vector<double> result(2 * expected, 0.0);
+        h->timings = BgwxTimings{};
+        const double tb = has_t_begin ? t_begin : 0.0;
+        if (tb > t_end)
+            throw Error{"Invalid time range: t_begin=" + bgw::rust_f64(tb) + " > t_end=" + bgw::rust_f64(t_end)};
+        if (!ids.empty() && S > 0 && n_w > 0) {
+            require_resolution(h);
+            std::vector<double> t_arr = bgw::linspace(tb, t_end, n_t);
+            std::vector<double> cw(n_t, 1.0);  // the tensor form has no time cutoff
+            bgw::SpectrumJob job = settings_job(h, t_arr, cw, w, n_w, khat ? rot.data() : nullptr, K);
+            job.bubbles = h->bubbles.data();
+            job.n_int = h->n_int;
+            job.n_tot = h->n_int + h->n_ext;
+            job.sel = ids.data();
+            job.n_sel = ids.size();
+            job.tensor = true;
+            job.kernel = BGWX_KERNEL_FP64_DIRECT;
+            bgw::run_spectrum(device(h), job, result.data(), false, &h->timings);
+        }
+        BgwComplex64* o = const_cast<BgwComplex64*>(slice(out, out_len, "out"));
+        for (size_t q = 0; q < expected; ++q) o[q] = BgwComplex64{result[2 * q], result[2 * q + 1]};
     });
 }
 

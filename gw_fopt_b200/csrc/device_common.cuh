@@ -75,7 +75,7 @@ struct Device {
     cudaEvent_t ev[8] = {};
     std::vector<cudaEvent_t> chunk_ev;  // 3 per k-hat chunk
     std::vector<cudaEvent_t> fact_ev;   // 3 per k-hat chunk: before beta, before GEMM, after GEMM
-    DevBuf bub, bubrot, dirs, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, sel, rot;
+    DevBuf bub, bubrot, dirs, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, sel, rot, cosphi, sinphi;
     DevBuf tau, codes, partial, out, counters, nblists;
     DevBuf fact_D, fact_kfirst, beta, fact_partial;  // factored-kernel work arrays
     DevBuf ens_out;                                  // batched ensemble: all realizations' spectra

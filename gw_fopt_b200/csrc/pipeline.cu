@@ -63,7 +63,7 @@ void device_set_stream(Device* d, void* stream) {
 
 void device_drop_resident(Device* d) {
     for (DevBuf* b : {&d->bub, &d->dirs, &d->cos_t, &d->sin2, &d->cos2, &d->coeffs, &d->powers, &d->t_arr,
-                      &d->cutw, &d->w, &d->sel, &d->rot})
+                      &d->cutw, &d->w, &d->sel, &d->rot, &d->cosphi, &d->sinphi})
         b->shadow_valid = false;
 }
 
@@ -129,8 +129,10 @@ struct SpecArgs {
     double dt;
     const double* w;
     int n_w;
-    double2* partial;  // (K, n_sel, 2, S, W); with PER_T: (n_sel, 2, S, W, n_t)
+    double2* partial;  // (K, n_sel, 2, S, W); with PER_T: (n_sel, 2, S, W, n_t); tensor: (K, n_sel, 6, S, W)
     int tau_in_smem;
+    const double* cosphi;  // tensor form
+    const double* sinphi;
 };
 
 // Combination step of ndarray's unrolled_fold:
@@ -328,6 +330,160 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_direct(SpecArgs A) {
     }
 }
 
+// The tensor form of new_generalized_bulk_flow.rs (NGBF:592-1203): the phi
+// integral of x_i x_j (t - t_n)^3 f in six components (xx, xy, xz, yy, yz, zz,
+// NGBF:634-727), the same A and C stages with NGBF's factor placement
+// (NGBF:782-826, 1145-1168), no time cutoff; one coefficient set at a time.
+__global__ void __launch_bounds__(kSpecThreads) k_tensor_direct(SpecArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int NG = 6;
+    const int k = blockIdx.y;
+    const size_t slot = blockIdx.x;
+    const int nd = A.n_cos * A.n_phi;
+    const double* tau_g = A.tau + ((size_t)k * A.n_sel + slot) * nd;
+    double* tau_s = reinterpret_cast<double*>(smem_raw);
+    double* Bsm = tau_s + (A.tau_in_smem ? ((nd + 1) & ~1) : 0);                      // [n_cos][6]
+    double2* red = reinterpret_cast<double2*>(Bsm + (size_t)A.n_cos * NG);            // [256][6]
+    const double* tau = A.tau_in_smem ? tau_s : tau_g;
+    if (A.tau_in_smem)
+        for (int q = threadIdx.x; q < nd; q += kSpecThreads) tau_s[q] = tau_g[q];
+    __syncthreads();
+
+    const uint32_t a = A.sel[slot];
+    const D4 xa = A.bub[(size_t)k * A.n_tot + a];
+    const double ta = xa.t, za = xa.z;
+    const int W_eff = min(A.n_w, kSpecThreads);
+    const int n_ig = kSpecThreads / W_eff;
+    const int wl = threadIdx.x % W_eff;
+    const int ig = threadIdx.x / W_eff;
+    const bool wthread = ig < n_ig;
+    const double dphi = 2.0 * CUDART_PI / (double)A.n_phi;
+    const double dcos = A.n_cos > 1 ? 2.0 / (double)(A.n_cos - 1) : 1.0;
+    const double inv6pi = 1.0 / (6.0 * CUDART_PI);
+
+    for (int s = 0; s < A.n_sets; ++s) {
+        for (int wb = 0; wb < A.n_w; wb += W_eff) {
+            const int wi = wb + wl;
+            const bool wvalid = wthread && wi < A.n_w;
+            const double wv = wvalid ? A.w[wi] : 0.0;
+            double2 cacc[NG];
+#pragma unroll
+            for (int g = 0; g < NG; ++g) cacc[g] = make_double2(0.0, 0.0);
+            for (int kt = 0; kt < A.n_t; ++kt) {
+                const double t = A.t_arr[kt];
+                if (t <= ta) continue;  // NGBF:1130
+                const double dta = t - ta;
+                // ---- B stage (NGBF:592-727) ----
+                for (int i = threadIdx.x; i < A.n_cos; i += kSpecThreads) {
+                    const double c = A.cos_thetax[i];
+                    const double st = sqrt(fmax(__dsub_rn(1.0, __dmul_rn(c, c)), 0.0));
+                    const double s2 = __dmul_rn(st, st), c2 = __dmul_rn(c, c), scz = __dmul_rn(st, c);
+                    const double cubed = __dmul_rn(__dmul_rn(dta, dta), dta);
+                    const double* trow = tau + (size_t)i * A.n_phi;
+                    const int sidx = s * A.n_terms;
+                    auto factor = [&](int j) {
+                        const double tj = trow[j];
+                        double f = 1.0;
+                        if (tj > 0.0 && dta >= tj) {
+                            const double ratio = tj / dta;
+                            f = 0.0;
+                            for (int m = 0; m < A.n_terms; ++m) f += A.coeffs[sidx + m] * pow(ratio, A.powers[sidx + m]);
+                            if (A.has_damping) f *= exp(-dta * (1.0 - ratio) / A.damping);
+                        }
+                        return f;
+                    };
+                    auto basis = [&](int j, int g) {
+                        const double cp = A.cosphi[j], sp = A.sinphi[j];
+                        switch (g) {
+                            case 0: return __dmul_rn(__dmul_rn(cp, cp), s2);
+                            case 1: return __dmul_rn(__dmul_rn(cp, sp), s2);
+                            case 2: return __dmul_rn(cp, scz);
+                            case 3: return __dmul_rn(__dmul_rn(sp, sp), s2);
+                            case 4: return __dmul_rn(sp, scz);
+                            default: return c2;
+                        }
+                    };
+                    // ndarray's eight-way unrolled sum over phi, per component
+                    double p8[NG][8];
+#pragma unroll
+                    for (int g = 0; g < NG; ++g)
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) p8[g][u] = 0.0;
+                    const int nfull = A.n_phi & ~7;
+                    for (int j0 = 0; j0 < nfull; j0 += 8) {
+#pragma unroll
+                        for (int u = 0; u < 8; ++u) {
+                            const int j = j0 + u;
+                            const double f = factor(j);
+                            const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
+#pragma unroll
+                            for (int g = 0; g < NG; ++g) p8[g][u] = __dadd_rn(p8[g][u], __dmul_rn(__dmul_rn(basis(j, g), f), wj));
+                        }
+                    }
+                    double sums[NG];
+#pragma unroll
+                    for (int g = 0; g < NG; ++g) sums[g] = unrolled_sum8(p8[g], 0.0);
+                    for (int j = nfull; j < A.n_phi; ++j) {
+                        const double f = factor(j);
+                        const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
+#pragma unroll
+                        for (int g = 0; g < NG; ++g) sums[g] = __dadd_rn(sums[g], __dmul_rn(__dmul_rn(basis(j, g), f), wj));
+                    }
+#pragma unroll
+                    for (int g = 0; g < NG; ++g) Bsm[(size_t)i * NG + g] = __dmul_rn(__dmul_rn(sums[g], dphi), cubed);
+                }
+                __syncthreads();
+                // ---- A stage (NGBF:782-826): phase e^{-i w dt c_i} (dcos w_theta) ----
+                double2 aacc[NG];
+#pragma unroll
+                for (int g = 0; g < NG; ++g) aacc[g] = make_double2(0.0, 0.0);
+                if (wvalid) {
+                    for (int i = ig; i < A.n_cos; i += n_ig) {
+                        double sn, cs;
+                        sincos(wv * (-dta * A.cos_thetax[i]), &sn, &cs);
+                        const double vi = A.n_cos == 1 ? 1.0 : ((i == 0 || i == A.n_cos - 1) ? 0.5 : 1.0);
+                        const double pfs = dcos * vi;
+                        const double pr = cs * pfs, pim = sn * pfs;
+#pragma unroll
+                        for (int g = 0; g < NG; ++g) {
+                            const double b = Bsm[(size_t)i * NG + g];
+                            aacc[g].x += b * pr;
+                            aacc[g].y += b * pim;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int g = 0; g < NG; ++g) red[(size_t)threadIdx.x * NG + g] = aacc[g];
+                __syncthreads();
+                // ---- C stage (NGBF:1145-1168): A e^{i w (t - z_a)} (dt w_t) ----
+                if (wvalid && ig == 0) {
+                    double sn, cs;
+                    sincos(wv * (t - za), &sn, &cs);
+                    const double dtw = A.dt * ((kt == 0 || kt == A.n_t - 1) ? 0.5 : 1.0);
+                    const double fr = cs * dtw, fi = sn * dtw;
+                    for (int g = 0; g < NG; ++g) {
+                        double2 at = make_double2(0.0, 0.0);
+                        for (int q = 0; q < n_ig; ++q) {
+                            const double2 v = red[(size_t)(q * W_eff + wl) * NG + g];
+                            at.x += v.x;
+                            at.y += v.y;
+                        }
+                        cacc[g].x += at.x * fr - at.y * fi;
+                        cacc[g].y += at.x * fi + at.y * fr;
+                    }
+                }
+                __syncthreads();
+            }
+            if (wvalid && ig == 0) {
+                for (int g = 0; g < NG; ++g) {
+                    const size_t o = ((((size_t)k * A.n_sel + slot) * NG + g) * A.n_sets + s) * A.n_w + wi;
+                    A.partial[o] = make_double2(cacc[g].x * inv6pi, cacc[g].y * inv6pi);
+                }
+            }
+        }
+    }
+}
+
 // Sum over radiating bubbles in index order (GBF:971-981).
 __global__ void k_reduce(const double2* __restrict__ partial, size_t n_sel, size_t per, size_t kc,
                          double2* __restrict__ out) {
@@ -416,7 +572,9 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     CUDA_OK(cudaSetDevice(dev->id));
     const size_t nd = job.n_cos * job.n_phi;
     const size_t S = job.n_sets, W = job.n_w, K = job.n_k;
-    const size_t per = 2 * S * W;
+    const size_t per = (job.tensor ? 6 : 2) * S * W;
+    if (job.tensor && job.kernel != BGWX_KERNEL_FP64_DIRECT)
+        throw Error{"the tensor form runs only on the FP64 direct kernel"};
     if (job.n_cos > 4096 || job.n_phi > 65536) throw Error{"angular resolution too large for the GPU kernels"};
     if (job.n_t > (size_t)0x7fffffff || W > (size_t)0x7fffffff) throw Error{"n_t or n_w too large"};
 
@@ -432,6 +590,8 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     double* w = upload(dev, dev->w, job.w, W, tm);
     uint32_t* sel = upload(dev, dev->sel, job.sel, job.n_sel, tm);
     double* rot = job.rot ? upload(dev, dev->rot, job.rot, 9 * K, tm) : nullptr;
+    double* cosphi = job.tensor ? upload(dev, dev->cosphi, job.cosphi, job.n_phi, tm) : nullptr;
+    double* sinphi = job.tensor ? upload(dev, dev->sinphi, job.sinphi, job.n_phi, tm) : nullptr;
 
     // frames per chunk: bounded by the mask buffer budget
     const size_t per_k = job.n_sel * nd * sizeof(double) +
@@ -462,8 +622,9 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
 
     // shared memory of the direct kernel
-    size_t smem_fixed = (size_t)job.n_cos * kSetChunk * 2 * sizeof(double) +
-                        (size_t)kSpecThreads * kSetChunk * 2 * sizeof(double2);
+    size_t smem_fixed = job.tensor ? (size_t)job.n_cos * 6 * sizeof(double) + (size_t)kSpecThreads * 6 * sizeof(double2)
+                                   : (size_t)job.n_cos * kSetChunk * 2 * sizeof(double) +
+                                         (size_t)kSpecThreads * kSetChunk * 2 * sizeof(double2);
     size_t smem_tau = ((nd + 1) & ~(size_t)1) * sizeof(double);
     int max_optin = 0;
     CUDA_OK(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev->id));
@@ -471,6 +632,8 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     size_t smem = smem_fixed + (tau_in_smem ? smem_tau : 0);
     if (smem > (size_t)max_optin) throw Error{"n_cos_thetax too large for the shared-memory layout"};
     CUDA_OK(cudaFuncSetAttribute(k_spec_direct<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (job.tensor)
+        CUDA_OK(cudaFuncSetAttribute(k_tensor_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
     uint64_t launches = 0;
     CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
@@ -515,9 +678,14 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             A.n_w = (int)W;
             A.partial = (double2*)dev->partial.p;
             A.tau_in_smem = tau_in_smem;
+            A.cosphi = cosphi;
+            A.sinphi = sinphi;
             if (job.n_sel > 0x7fffffffULL) throw Error{"too many radiating bubbles"};
             dim3 g((unsigned)job.n_sel, (unsigned)kn);
-            k_spec_direct<false><<<g, kSpecThreads, smem, dev->stream>>>(A);
+            if (job.tensor)
+                k_tensor_direct<<<g, kSpecThreads, smem, dev->stream>>>(A);
+            else
+                k_spec_direct<false><<<g, kSpecThreads, smem, dev->stream>>>(A);
             CUDA_OK(cudaGetLastError());
             ++launches;
             dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);

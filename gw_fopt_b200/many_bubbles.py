@@ -21,7 +21,7 @@ from . import _lib as L
 
 __all__ = [
     "Isometry3", "ParallelepipedLattice", "CartesianLattice", "SphericalLattice", "EmptyLattice",
-    "LatticeBubbles", "ExponentialTimeCutoff", "GeneralizedBulkFlow",
+    "LatticeBubbles", "ExponentialTimeCutoff", "GeneralizedBulkFlow", "NewGeneralizedBulkFlow",
 ]
 
 
@@ -748,6 +748,82 @@ class GeneralizedBulkFlow:
         t = L.BgwxTimings()
         _call(L.lib().bgwx_generalized_bulk_flow_last_timings(self._h, C.byref(t)))
         return {f: getattr(t, f) for f, _ in L.BgwxTimings._fields_}
+
+
+class NewGeneralizedBulkFlow(GeneralizedBulkFlow):
+    """The tensor form (the reference's NewGeneralizedBulkFlow,
+    rust/py-bubble-gw/src/py_many_bubbles/py_new_generalized_bulk_flow.rs and
+    rust/bubble-gw/src/many_bubbles/new_generalized_bulk_flow.rs): C_ij(w) in six
+    components xx, xy, xz, yy, yz, zz, from the phi integral of x_i x_j (t - t_n)^3 f
+    instead of the cos 2phi / sin 2phi projections.  Configuration and geometry
+    methods are those of GeneralizedBulkFlow; the spectrum runs in plain FP64 on
+    the GPU (the direct kernel), with no time cutoff (the tensor form has none)."""
+
+    def _compute_tensor(self, w_arr, t_begin, t_end, n_t, selected, khat=None):
+        self._push_params()
+        w = np.ascontiguousarray(np.asarray(w_arr, dtype=np.float64).ravel())
+        S = self._coefficients.shape[0]
+        kh = None if khat is None else np.ascontiguousarray(np.asarray(khat, dtype=np.float64).reshape(-1, 3))
+        K = 1 if kh is None else kh.shape[0]
+        out = np.zeros((K, 6, S, w.size), dtype=np.complex128)
+        if selected is not None:
+            sel = np.ascontiguousarray(selected, dtype=np.uint64)
+            psel, nsel = sel.ctypes.data_as(C.POINTER(C.c_size_t)), sel.size
+        else:
+            psel, nsel = None, 0
+        _call(L.lib().bgwx_generalized_bulk_flow_compute_c_tensor_khat(
+            self._h, L.ptr(w), w.size, t_begin is not None, 0.0 if t_begin is None else float(t_begin),
+            float(t_end), int(n_t), L.ptr(kh) if kh is not None else None, 0 if kh is None else K, psel, nsel,
+            out.ctypes.data_as(C.POINTER(L.BgwComplex64)), out.size))
+        return out if khat is not None else out[0]
+
+    def compute_c_tensor(self, w_arr, *, t_begin=None, t_end, n_t, selected_bubbles=None):
+        """(6, n_sets, n_w) complex128, summed over the selected bubbles (new_generalized_bulk_flow.rs:1205-1275)."""
+        if int(n_t) < 2:
+            raise ValueError("Invalid resolution: n_t must be >= 2 for integration")
+        sel = self._selected(selected_bubbles)
+        if sel is not None and sel.size == 0:
+            return np.zeros((6, self._coefficients.shape[0], np.asarray(w_arr).size), dtype=np.complex128)
+        return self._compute_tensor(w_arr, t_begin, t_end, n_t, sel)
+
+    def compute_c_tensor_fixed_bubble(self, a_idx, w_arr, t_begin, t_end, n_t):
+        """One bubble's (6, n_sets, n_w) contribution (new_generalized_bulk_flow.rs:1067-1203)."""
+        self._check_a(int(a_idx))
+        tb = 0.0 if t_begin is None else float(t_begin)
+        if tb > float(t_end):
+            raise ValueError(f"Invalid time range: t_begin={_rust_f64(tb)} > t_end={_rust_f64(float(t_end))}")
+        if int(n_t) < 2:
+            return np.zeros((6, self._coefficients.shape[0], np.asarray(w_arr).size), dtype=np.complex128)
+        return self._compute_tensor(w_arr, t_begin, t_end, n_t, np.array([int(a_idx)], dtype=np.uint64))
+
+    def compute_c_tensor_khat(self, w_arr, khat, *, t_begin=None, t_end, n_t, selected_bubbles=None):
+        """(K, 6, n_sets, n_w): the tensor of each k-hat row's rotated configuration (B200 extension)."""
+        if int(n_t) < 2:
+            raise ValueError("Invalid resolution: n_t must be >= 2 for integration")
+        sel = self._selected(selected_bubbles)
+        kh = np.asarray(khat, dtype=np.float64).reshape(-1, 3)
+        if sel is not None and sel.size == 0:
+            return np.zeros((kh.shape[0], 6, self._coefficients.shape[0], np.asarray(w_arr).size),
+                            dtype=np.complex128)
+        return self._compute_tensor(w_arr, t_begin, t_end, n_t, sel, khat=kh)
+
+
+def tt_energy(c_tensor, khat=(0.0, 0.0, 1.0)):
+    """Lambda_ij,lm(k) C*_ij C_lm = Tr[P C* P C] - |Tr[P C]|^2 / 2, P = 1 - k k^T
+    (docs/generalized_bulkflow.md:8-17), for c_tensor (6, ...) in the order
+    xx, xy, xz, yy, yz, zz; the energy per ln w and solid angle is 2 G w^3 times
+    this (with T = kappa rho v^3 C).  For k = z it is 2 (|C_+|^2 + |C_x|^2) with
+    C_+ = (C_xx - C_yy) / 2, C_x = C_xy."""
+    c = np.asarray(c_tensor)
+    k = np.asarray(khat, dtype=np.float64)
+    k = k / np.linalg.norm(k)
+    idx = [[0, 1, 2], [1, 3, 4], [2, 4, 5]]
+    T = np.stack([np.stack([c[idx[i][j]] for j in range(3)]) for i in range(3)])  # (3, 3, ...)
+    P = np.eye(3) - np.outer(k, k)
+    PT = np.einsum("ij,jl...->il...", P, T)
+    tr_pc = np.einsum("ii...->...", PT)
+    tr_pcpc = np.einsum("ij...,ji...->...", np.conj(PT), PT)
+    return np.real(tr_pcpc) - 0.5 * np.abs(tr_pc) ** 2
 
 
 def _rust_f64(x: float) -> str:

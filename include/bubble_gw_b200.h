@@ -194,6 +194,23 @@ BgwStatus bgwx_generalized_bulk_flow_compute_c_integrand(bgw_generalized_bulk_fl
                                                          size_t n_selected_bubbles, BgwComplex64 *out,
                                                          size_t out_len);
 
+/* The tensor form of the reference's NewGeneralizedBulkFlow::compute_c_tensor
+ * (rust/bubble-gw/src/many_bubbles/new_generalized_bulk_flow.rs:1205-1275,
+ * Python rust/py-bubble-gw/src/py_many_bubbles/py_new_generalized_bulk_flow.rs:265-313):
+ * C_ij(w) = 1/(6 pi) sum_n int dt e^{i w (t - z_n)} A_n,ij with the phi
+ * integral of x_i x_j (t - t_n)^3 f in six components, out (K, 6, S, W) in the
+ * order xx, xy, xz, yy, yz, zz, for each k-hat row of `khat` (its rotated
+ * configuration, the convention of ..._compute_c_integral_khat) or, with
+ * khat NULL, the configuration as given (K = 1, the reference's call).  No
+ * time cutoff (the tensor form has none); plain FP64 (the direct kernel) for
+ * every kernel selection.  The handle's bubbles, resolution and scaling
+ * parameters are those of the scalar form. */
+BgwStatus bgwx_generalized_bulk_flow_compute_c_tensor_khat(bgw_generalized_bulk_flow *bulk_flow, const double *w_arr,
+                                                          size_t n_w, bool has_t_begin, double t_begin, double t_end,
+                                                          size_t n_t, const double *khat, size_t n_khat,
+                                                          const size_t *selected_bubbles, size_t n_selected_bubbles,
+                                                          BgwComplex64 *out, size_t out_len);
+
 /* Draws the bubbles of n_realizations nucleation Monte Carlo realizations on
  * the GPU (one block per realization): exponential-rate nucleation in a
  * periodic cube of side box_side, candidates arriving as a Poisson process

@@ -347,6 +347,108 @@ void c_increment(const Problem& P, size_t a, const int32_t* first, const double*
         }
 }
 
+// ---- tensor form: new_generalized_bulk_flow.rs (NGBF) ----
+// NGBF:592-727 (compute_b_tensor) for one cos(theta) row: the six components
+// xx, xy, xz, yy, yz, zz of the phi integral of x_i x_j (t - t_n)^3 f.
+void b_tensor(const Problem& P, size_t i, const int32_t* first, const double* dtab, double delta_ta, double* b6,
+              std::vector<double>& scratch) {
+    size_t nf = P.n_phi, S = P.n_sets, M = P.n_terms;
+    double c = P.cos_thetax[i];
+    double st = std::sqrt(std::max(1.0 - c * c, 0.0));
+    double s2 = st * st, c2 = c * c, sc = st * c;
+    double dphi = 2.0 * M_PI / (double)nf;
+    double cubed = delta_ta > 0.0 ? (delta_ta * delta_ta) * delta_ta : 0.0;
+    scratch.resize(7 * nf);
+    double* factors = scratch.data();
+    double* wk = factors + nf;  // 6 weighted rows
+    for (size_t s = 0; s < S; ++s) {
+        for (size_t j = 0; j < nf; ++j) {
+            size_t k = i * nf + j;
+            bool collided = false;  // NGBF:480-530: AlreadyCollided iff tau > 0 and delta_ta >= tau
+            if (first[k] != kNone) {
+                double dt = dtab[k];
+                collided = dt > 0.0 && delta_ta >= dt;
+            }
+            if (!collided) {
+                factors[j] = 1.0;
+            } else {
+                double ratio = dtab[k] / delta_ta;
+                double f = 0.0;
+                for (size_t m = 0; m < M; ++m) f += P.coeffs[s * M + m] * std::pow(ratio, P.powers[s * M + m]);
+                if (P.has_damping) f *= std::exp(-delta_ta * (1.0 - ratio) / P.damping);
+                factors[j] = f;
+            }
+        }
+        for (size_t j = 0; j < nf; ++j) {
+            double cp = std::cos(P.phix[j]), sp = std::sin(P.phix[j]);
+            double w = (nf > 1 && (j == 0 || j == nf - 1)) ? 0.5 : 1.0;
+            double basis[6] = {(cp * cp) * s2, (cp * sp) * s2, cp * sc, (sp * sp) * s2, sp * sc, c2};
+            for (int q = 0; q < 6; ++q) wk[q * nf + j] = (basis[q] * factors[j]) * w;
+        }
+        for (int q = 0; q < 6; ++q) b6[q * S + s] = (unrolled_sum(wk + q * nf, nf) * dphi) * cubed;
+    }
+}
+
+// NGBF:729-830 (compute_a_tensor) and the per-t increment of NGBF:1130-1168:
+// inc (6, S, W) = A(t) e^{i w (t - z_a)} (dt weight).
+void c_tensor_increment(const Problem& P, size_t a, const int32_t* first, const double* dtab, const double* w,
+                        size_t W, double t, size_t t_idx, size_t n_t, double dt, Cplx* inc,
+                        std::vector<double>& scratch) {
+    size_t S = P.n_sets, nc = P.n_cos;
+    double ta = P.interior[a].t, za = P.interior[a].z;
+    double delta_ta = t - ta;
+    std::vector<Cplx> acc(6 * S * W, Cplx{0, 0});
+    std::vector<double> b6(6 * S);
+    std::vector<Cplx> ph(W);
+    double dcos = nc > 1 ? 2.0 / (double)(nc - 1) : 1.0;
+    for (size_t i = 0; i < nc; ++i) {
+        b_tensor(P, i, first, dtab, delta_ta, b6.data(), scratch);
+        double base_im = -delta_ta * P.cos_thetax[i];
+        double wt = nc == 1 ? 1.0 : ((i == 0 || i == nc - 1) ? 0.5 : 1.0);
+        double pfs = dcos * wt;
+        for (size_t k = 0; k < W; ++k) ph[k] = cscale(cexp_i(w[k] * base_im), pfs);
+        for (int q = 0; q < 6; ++q)
+            for (size_t s = 0; s < S; ++s) {
+                Cplx bv{b6[q * S + s], 0.0};
+                for (size_t k = 0; k < W; ++k)
+                    acc[(q * S + s) * W + k] = cadd(acc[(q * S + s) * W + k], cmul(bv, ph[k]));
+            }
+    }
+    double uw = (t_idx == 0 || t_idx == n_t - 1) ? 0.5 : 1.0;
+    Cplx dtc{dt * uw, 0.0};
+    for (size_t k = 0; k < W; ++k) {
+        Cplx factor = cmul(cexp_i(w[k] * (t - za)), dtc);
+        for (size_t q = 0; q < 6 * S; ++q) inc[q * W + k] = cmul(acc[q * W + k], factor);
+    }
+}
+
+// NGBF:1067-1203 (compute_c_tensor_fixed_bubble), t reduced in index order; adds into acc (6, S, W).
+void c_tensor_fixed_bubble(const Problem& P, size_t a, const int32_t* first, const double* w, size_t W,
+                           double t_begin, double t_end, size_t n_t, Cplx* acc, int threads) {
+    size_t S = P.n_sets;
+    std::vector<double> dtab(P.n_cos * P.n_phi);
+    delta_tab(P, a, first, dtab.data());
+    std::vector<double> t_arr = linspace(t_begin, t_end, n_t);
+    double dt = n_t > 1 ? t_arr[1] - t_arr[0] : 0.0;
+    size_t per = 6 * S * W;
+    std::vector<Cplx> incs(n_t * per, Cplx{0, 0});
+    std::vector<char> active(n_t, 0);
+    double tn = P.interior[a].t;
+    parallel_for<std::vector<double>>(n_t, threads, [&](size_t ti, std::vector<double>& scratch) {
+        double t = t_arr[ti];
+        if (t > tn) {  // NGBF:1130: t <= t_nucleation contributes nothing
+            active[ti] = 1;
+            c_tensor_increment(P, a, first, dtab.data(), w, W, t, ti, n_t, dt, &incs[ti * per], scratch);
+        }
+    });
+    std::vector<Cplx> c(per, Cplx{0, 0});
+    for (size_t ti = 0; ti < n_t; ++ti)
+        if (active[ti])
+            for (size_t q = 0; q < per; ++q) c[q] = cadd(c[q], incs[ti * per + q]);
+    Cplx f{1.0 / (6.0 * M_PI), 0.0};
+    for (size_t q = 0; q < per; ++q) acc[q] = cadd(acc[q], cmul(c[q], f));
+}
+
 thread_local std::string g_err;
 
 int fail(const std::string& m) {
@@ -634,6 +736,44 @@ int orc_compute_c_integral_khat(const double* interior, size_t n_int, const doub
                                         n_terms, damping, w, n_w, 1, t_begin, t_end, n_t, nullptr, 0, cutoff_kind,
                                         smax, ratio_t_cut, ratio_t_0, out + 2 * k * per, nullptr, threads);
         if (rc) return rc;
+    }
+    return 0;
+}
+
+// NGBF:1205-1275 (compute_c_tensor): out (6, S, W) complex as interleaved
+// doubles, the sum over the selected bubbles (NULL = all) in selection order.
+int orc_compute_c_tensor(const double* interior, size_t n_int, const double* exterior, size_t n_ext, size_t n_cos,
+                         size_t n_phi, const double* coeffs, const double* powers, size_t n_sets, size_t n_terms,
+                         double damping, const double* w, size_t n_w, int has_t_begin, double t_begin, double t_end,
+                         size_t n_t, const size_t* selected, size_t n_sel, double* out, int threads) {
+    if (n_cos < 2 || n_phi < 2) return fail("Invalid resolution: Angular resolutions must be greater than one");
+    if (n_t < 2) return fail("Invalid resolution: n_t must be >= 2 for integration");
+    Problem P;
+    load(P, interior, n_int, exterior, n_ext);
+    set_resolution(P, n_cos, n_phi);
+    set_params(P, coeffs, powers, n_sets, n_terms, damping);
+    size_t per = 6 * n_sets * n_w;
+    std::vector<Cplx> acc(per, Cplx{0, 0});
+    std::vector<size_t> ids;
+    if (selected) {
+        for (size_t q = 0; q < n_sel; ++q) {
+            if (selected[q] >= n_int)
+                return fail("Index " + std::to_string(selected[q]) + " out of bounds for max " + std::to_string(n_int));
+            ids.push_back(selected[q]);
+        }
+    } else {
+        for (size_t a = 0; a < n_int; ++a) ids.push_back(a);
+    }
+    double tb = has_t_begin ? t_begin : 0.0;
+    if (tb > t_end) return fail("Invalid time range");
+    std::vector<int32_t> first(n_cos * n_phi);
+    for (size_t a : ids) {
+        masks_for(P, a, first.data(), threads);
+        c_tensor_fixed_bubble(P, a, first.data(), w, n_w, tb, t_end, n_t, acc.data(), threads);
+    }
+    for (size_t q = 0; q < per; ++q) {
+        out[2 * q] = acc[q].re;
+        out[2 * q + 1] = acc[q].im;
     }
     return 0;
 }

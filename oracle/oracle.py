@@ -55,6 +55,9 @@ def lib():
         L.orc_compute_c_integrand.argtypes = [
             _dp, C.c_size_t, _dp, C.c_size_t, C.c_size_t, C.c_size_t, _dp, _dp, C.c_size_t, C.c_size_t,
             C.c_double, _dp, C.c_size_t, C.c_int, C.c_double, C.c_double, C.c_size_t, _szp, C.c_size_t, _dp, C.c_int]
+        L.orc_compute_c_tensor.argtypes = [
+            _dp, C.c_size_t, _dp, C.c_size_t, C.c_size_t, C.c_size_t, _dp, _dp, C.c_size_t, C.c_size_t,
+            C.c_double, _dp, C.c_size_t, C.c_int, C.c_double, C.c_double, C.c_size_t, _szp, C.c_size_t, _dp, C.c_int]
         L.orc_rotation_for_khat.argtypes = [C.c_double, C.c_double, C.c_double, _dp]
         L.orc_rotate.argtypes = [_dp, _dp, C.c_size_t, _dp]
         L.orc_time_cutoff.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double, _dp, C.c_size_t, _dp]
@@ -206,3 +209,37 @@ def time_cutoff(t, smax, ratio_t_cut=None, ratio_t_0=None):
     lib().orc_time_cutoff(1, float(smax), np.nan if ratio_t_cut is None else ratio_t_cut,
                           np.nan if ratio_t_0 is None else ratio_t_0, pt, t.size, out.ctypes.data_as(_dp))
     return out
+
+
+def compute_c_tensor(interior, exterior, n_cos, n_phi, w, t_end, n_t, t_begin=None, coefficients=((1.0,),),
+                     powers=((3.0,),), damping=None, selected=None, threads=None):
+    """(6, n_sets, n_w) complex128 in the order xx, xy, xz, yy, yz, zz: the reference's
+    NewGeneralizedBulkFlow.compute_c_tensor (new_generalized_bulk_flow.rs:1205-1275)."""
+    ai, pi, ni = _bubbles(interior)
+    ae, pe, ne = _bubbles(np.zeros((0, 4)) if exterior is None else exterior)
+    co = np.ascontiguousarray(np.asarray(coefficients, dtype=np.float64))
+    po = np.ascontiguousarray(np.asarray(powers, dtype=np.float64))
+    S, M = co.shape
+    w, pw = _d(np.asarray(w, dtype=np.float64).ravel())
+    out = np.zeros((6, S, w.size), dtype=np.complex128)
+    sel = None if selected is None else np.ascontiguousarray(selected, dtype=np.uintp)
+    _check(lib().orc_compute_c_tensor(
+        pi, ni, pe, ne, n_cos, n_phi, co.ctypes.data_as(_dp), po.ctypes.data_as(_dp), S, M,
+        float("nan") if damping is None else float(damping), pw, w.size, 0 if t_begin is None else 1,
+        0.0 if t_begin is None else float(t_begin), float(t_end), n_t,
+        sel.ctypes.data_as(_szp) if sel is not None else None, 0 if sel is None else sel.size,
+        out.ctypes.data_as(_dp), threads or max_threads()))
+    return out
+
+
+def compute_c_tensor_khat(interior, exterior, khat, n_cos, n_phi, w, t_end, n_t, t_begin=None,
+                          coefficients=((1.0,),), powers=((3.0,),), damping=None, threads=None):
+    """(K, 6, n_sets, n_w): compute_c_tensor on each k-hat's rotated configuration."""
+    kh = np.asarray(khat, dtype=np.float64).reshape(-1, 3)
+    outs = []
+    for k in kh:
+        R = rotation_for_khat(k)
+        outs.append(compute_c_tensor(rotate(R, interior), rotate(R, np.zeros((0, 4)) if exterior is None else exterior),
+                                     n_cos, n_phi, w, t_end, n_t, t_begin, coefficients, powers, damping,
+                                     threads=threads))
+    return np.stack(outs)
