@@ -83,6 +83,9 @@ SIGNATURES = {
     "bgwx_generalized_bulk_flow_compute_c_tensor_khat": (
         C.c_int, [_hp, _dp, C.c_size_t, C.c_bool, C.c_double, C.c_double, C.c_size_t, _dp, C.c_size_t, _szp,
                   C.c_size_t, C.POINTER(BgwComplex64), C.c_size_t]),
+    "bgwx_generalized_bulk_flow_compute_c_tensor_integrand": (
+        C.c_int, [_hp, _dp, C.c_size_t, C.c_bool, C.c_double, C.c_double, C.c_size_t, _szp, C.c_size_t,
+                  C.POINTER(BgwComplex64), C.c_size_t]),
     "bgwx_nucleate_exponential": (
         C.c_int, [C.POINTER(C.c_int64), _dp, C.POINTER(C.c_uint64), C.c_size_t, C.c_double, C.c_double, C.c_size_t,
                   _dp, C.c_size_t, _dp, C.c_size_t, C.POINTER(C.c_int32)]),

@@ -687,16 +687,17 @@ BgwStatus bgwx_generalized_bulk_flow_set_bubbles(bgw_generalized_bulk_flow* bulk
     });
 }
 
-BgwStatus bgwx_generalized_bulk_flow_compute_c_integrand(bgw_generalized_bulk_flow* bulk_flow, const double* w_arr,
-                                                         size_t n_w, bool has_t_begin, double t_begin, double t_end,
-                                                         size_t n_t, const size_t* selected_bubbles,
-                                                         size_t n_selected_bubbles, BgwComplex64* out,
-                                                         size_t out_len) {
-    return run_ffi([&] {
+namespace {
+// compute_c_integrand (GBF:875-920) and its tensor form (NGBF:993-1065): out
+// (NG, S, W, n_t) with NG = 2 (C_+, C_x) or 6 (xx, xy, xz, yy, yz, zz).
+void integrand_common(bgw_generalized_bulk_flow* bulk_flow, const double* w_arr, size_t n_w, bool has_t_begin,
+                      double t_begin, double t_end, size_t n_t, const size_t* selected_bubbles,
+                      size_t n_selected_bubbles, BgwComplex64* out, size_t out_len, bool tensor) {
+    {
         auto* h = handle(bulk_flow);
         const size_t S = h->n_sets;
         const size_t expected =
-            checked_mul(checked_mul(checked_mul(2, S, "out"), n_w, "out"), n_t, "out");
+            checked_mul(checked_mul(checked_mul(tensor ? 6 : 2, S, "out"), n_w, "out"), n_t, "out");
         // generalized_bulk_flow.rs:883-906: n_t, then the selection
         if (n_t < 2) throw Error{"Invalid resolution: n_t must be >= 2"};
         std::vector<uint32_t> ids;
@@ -736,10 +737,35 @@ BgwStatus bgwx_generalized_bulk_flow_compute_c_integrand(bgw_generalized_bulk_fl
         job.n_tot = h->n_int + h->n_ext;
         job.sel = live.data();
         job.n_sel = live.size();
+        job.tensor = tensor;
         std::vector<double> result(2 * expected);
         h->timings = BgwxTimings{};
         bgw::run_integrand(device(h), job, result.data(), &h->timings);
         for (size_t q = 0; q < expected; ++q) o[q] = BgwComplex64{result[2 * q], result[2 * q + 1]};
+    }
+}
+}  // namespace
+
+BgwStatus bgwx_generalized_bulk_flow_compute_c_integrand(bgw_generalized_bulk_flow* bulk_flow, const double* w_arr,
+                                                         size_t n_w, bool has_t_begin, double t_begin, double t_end,
+                                                         size_t n_t, const size_t* selected_bubbles,
+                                                         size_t n_selected_bubbles, BgwComplex64* out,
+                                                         size_t out_len) {
+    return run_ffi([&] {
+        integrand_common(bulk_flow, w_arr, n_w, has_t_begin, t_begin, t_end, n_t, selected_bubbles,
+                         n_selected_bubbles, out, out_len, false);
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_compute_c_tensor_integrand(bgw_generalized_bulk_flow* bulk_flow,
+                                                                const double* w_arr, size_t n_w, bool has_t_begin,
+                                                                double t_begin, double t_end, size_t n_t,
+                                                                const size_t* selected_bubbles,
+                                                                size_t n_selected_bubbles, BgwComplex64* out,
+                                                                size_t out_len) {
+    return run_ffi([&] {
+        integrand_common(bulk_flow, w_arr, n_w, has_t_begin, t_begin, t_end, n_t, selected_bubbles,
+                         n_selected_bubbles, out, out_len, true);
     });
 }
 

@@ -334,6 +334,9 @@ __global__ void __launch_bounds__(kSpecThreads) k_spec_direct(SpecArgs A) {
 // integral of x_i x_j (t - t_n)^3 f in six components (xx, xy, xz, yy, yz, zz,
 // NGBF:634-727), the same A and C stages with NGBF's factor placement
 // (NGBF:782-826, 1145-1168), no time cutoff; one coefficient set at a time.
+// PER_T: the time-resolved integrand (NGBF:832-991), each step's
+// A e^{i w (t - z_a)} (dt w_t) / (6 pi), partial (n_sel, 6, S, W, n_t).
+template <bool PER_T>
 __global__ void __launch_bounds__(kSpecThreads) k_tensor_direct(SpecArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int NG = 6;
@@ -456,7 +459,23 @@ __global__ void __launch_bounds__(kSpecThreads) k_tensor_direct(SpecArgs A) {
                 for (int g = 0; g < NG; ++g) red[(size_t)threadIdx.x * NG + g] = aacc[g];
                 __syncthreads();
                 // ---- C stage (NGBF:1145-1168): A e^{i w (t - z_a)} (dt w_t) ----
-                if (wvalid && ig == 0) {
+                if (PER_T && wvalid && ig == 0) {
+                    double sn, cs;
+                    sincos(wv * (t - za), &sn, &cs);
+                    const double dtw = A.dt * ((kt == 0 || kt == A.n_t - 1) ? 0.5 : 1.0);
+                    const double fr = cs * dtw, fi = sn * dtw;
+                    for (int g = 0; g < NG; ++g) {
+                        double2 at = make_double2(0.0, 0.0);
+                        for (int q = 0; q < n_ig; ++q) {
+                            const double2 v = red[(size_t)(q * W_eff + wl) * NG + g];
+                            at.x += v.x;
+                            at.y += v.y;
+                        }
+                        const size_t o = ((((size_t)slot * NG + g) * A.n_sets + s) * A.n_w + wi) * A.n_t + kt;
+                        A.partial[o] = make_double2((at.x * fr - at.y * fi) * inv6pi, (at.x * fi + at.y * fr) * inv6pi);
+                    }
+                }
+                if (!PER_T && wvalid && ig == 0) {
                     double sn, cs;
                     sincos(wv * (t - za), &sn, &cs);
                     const double dtw = A.dt * ((kt == 0 || kt == A.n_t - 1) ? 0.5 : 1.0);
@@ -474,7 +493,7 @@ __global__ void __launch_bounds__(kSpecThreads) k_tensor_direct(SpecArgs A) {
                 }
                 __syncthreads();
             }
-            if (wvalid && ig == 0) {
+            if (!PER_T && wvalid && ig == 0) {
                 for (int g = 0; g < NG; ++g) {
                     const size_t o = ((((size_t)k * A.n_sel + slot) * NG + g) * A.n_sets + s) * A.n_w + wi;
                     A.partial[o] = make_double2(cacc[g].x * inv6pi, cacc[g].y * inv6pi);
@@ -633,7 +652,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     if (smem > (size_t)max_optin) throw Error{"n_cos_thetax too large for the shared-memory layout"};
     CUDA_OK(cudaFuncSetAttribute(k_spec_direct<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (job.tensor)
-        CUDA_OK(cudaFuncSetAttribute(k_tensor_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        CUDA_OK(cudaFuncSetAttribute(k_tensor_direct<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
     uint64_t launches = 0;
     CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
@@ -683,7 +702,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             if (job.n_sel > 0x7fffffffULL) throw Error{"too many radiating bubbles"};
             dim3 g((unsigned)job.n_sel, (unsigned)kn);
             if (job.tensor)
-                k_tensor_direct<<<g, kSpecThreads, smem, dev->stream>>>(A);
+                k_tensor_direct<false><<<g, kSpecThreads, smem, dev->stream>>>(A);
             else
                 k_spec_direct<false><<<g, kSpecThreads, smem, dev->stream>>>(A);
             CUDA_OK(cudaGetLastError());
@@ -871,7 +890,7 @@ void run_integrand(Device* dev, const SpectrumJob& job, double* out, BgwxTimings
     CUDA_OK(cudaSetDevice(dev->id));
     const size_t nd = job.n_cos * job.n_phi;
     const size_t S = job.n_sets, W = job.n_w, T = job.n_t;
-    const size_t per = 2 * S * W * T;  // complex values of one bubble's integrand
+    const size_t per = (job.tensor ? 6 : 2) * S * W * T;  // complex values of one bubble's integrand
     if (job.n_cos > 4096 || job.n_phi > 65536) throw Error{"angular resolution too large for the GPU kernels"};
     D4* bub = reinterpret_cast<D4*>(upload(dev, dev->bub, job.bubbles, 4 * job.n_tot, tm));
     D4* dirs = reinterpret_cast<D4*>(upload(dev, dev->dirs, job.dirs, 4 * nd, tm));
@@ -884,6 +903,8 @@ void run_integrand(Device* dev, const SpectrumJob& job, double* out, BgwxTimings
     double* cutw = upload(dev, dev->cutw, job.cutoff, T, tm);
     double* w = upload(dev, dev->w, job.w, W, tm);
     uint32_t* sel = upload(dev, dev->sel, job.sel, job.n_sel, tm);
+    double* cosphi = job.tensor ? upload(dev, dev->cosphi, job.cosphi, job.n_phi, tm) : nullptr;
+    double* sinphi = job.tensor ? upload(dev, dev->sinphi, job.sinphi, job.n_phi, tm) : nullptr;
     // bubbles per chunk: bounded by the per-bubble integrand buffer
     const size_t budget = mask_budget_bytes();
     size_t chunk = std::max<size_t>(1, std::min(job.n_sel, budget / std::max<size_t>(per * sizeof(double2), 1)));
@@ -894,8 +915,9 @@ void run_integrand(Device* dev, const SpectrumJob& job, double* out, BgwxTimings
     dev->counters.ensure(64);
     CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
     CUDA_OK(cudaMemsetAsync(dev->out.p, 0, per * sizeof(double2), dev->stream));
-    size_t smem = (size_t)job.n_cos * kSetChunk * 2 * sizeof(double) +
-                  (size_t)kSpecThreads * kSetChunk * 2 * sizeof(double2);
+    size_t smem = job.tensor ? (size_t)job.n_cos * 6 * sizeof(double) + (size_t)kSpecThreads * 6 * sizeof(double2)
+                             : (size_t)job.n_cos * kSetChunk * 2 * sizeof(double) +
+                                   (size_t)kSpecThreads * kSetChunk * 2 * sizeof(double2);
     const size_t smem_tau = ((nd + 1) & ~(size_t)1) * sizeof(double);
     int max_optin = 0;
     CUDA_OK(cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev->id));
@@ -903,6 +925,8 @@ void run_integrand(Device* dev, const SpectrumJob& job, double* out, BgwxTimings
     if (tau_in_smem) smem += smem_tau;
     if (smem > (size_t)max_optin) throw Error{"n_cos_thetax too large for the shared-memory layout"};
     CUDA_OK(cudaFuncSetAttribute(k_spec_direct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (job.tensor)
+        CUDA_OK(cudaFuncSetAttribute(k_tensor_direct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     uint64_t launches = 0;
     CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
     launch_mask_pipeline(dev, bub, bub, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, 1, (double*)dev->tau.p,
@@ -935,7 +959,12 @@ void run_integrand(Device* dev, const SpectrumJob& job, double* out, BgwxTimings
         A.n_w = (int)W;
         A.partial = (double2*)dev->partial.p;
         A.tau_in_smem = tau_in_smem;
-        k_spec_direct<true><<<dim3((unsigned)n, 1), kSpecThreads, smem, dev->stream>>>(A);
+        A.cosphi = cosphi;
+        A.sinphi = sinphi;
+        if (job.tensor)
+            k_tensor_direct<true><<<dim3((unsigned)n, 1), kSpecThreads, smem, dev->stream>>>(A);
+        else
+            k_spec_direct<true><<<dim3((unsigned)n, 1), kSpecThreads, smem, dev->stream>>>(A);
         CUDA_OK(cudaGetLastError());
         k_reduce_integrand<<<(unsigned)((per + 255) / 256), 256, 0, dev->stream>>>((const double2*)dev->partial.p, n,
                                                                                    per, (double2*)dev->out.p);

@@ -808,6 +808,39 @@ class NewGeneralizedBulkFlow(GeneralizedBulkFlow):
         return self._compute_tensor(w_arr, t_begin, t_end, n_t, sel, khat=kh)
 
 
+    def compute_c_tensor_integrand(self, w_arr, *, t_begin=None, t_end, n_t, selected_bubbles=None):
+        """(6, n_sets, n_w, n_t): the time-resolved tensor integrand summed over the selected
+        bubbles (new_generalized_bulk_flow.rs:993-1065), computed on the GPU."""
+        self._push_params()
+        w = np.ascontiguousarray(np.asarray(w_arr, dtype=np.float64).ravel())
+        S = self._coefficients.shape[0]
+        if int(n_t) < 0:
+            raise OverflowError("can't convert negative int to unsigned")
+        out = np.zeros((6, S, w.size, int(n_t)), dtype=np.complex128)
+        sel = self._selected(selected_bubbles)
+        psel = sel.ctypes.data_as(C.POINTER(C.c_size_t)) if sel is not None else None
+        _call(L.lib().bgwx_generalized_bulk_flow_compute_c_tensor_integrand(
+            self._h, L.ptr(w), w.size, t_begin is not None, 0.0 if t_begin is None else float(t_begin),
+            float(t_end), int(n_t), psel, 0 if sel is None else sel.size,
+            out.ctypes.data_as(C.POINTER(L.BgwComplex64)), out.size))
+        return out
+
+    def compute_c_tensor_integrand_fixed_bubble(self, a_idx, w_arr, t_begin, t_end, n_t):
+        """(6, n_sets, n_w, n_t): bubble a_idx's time-resolved tensor integrand
+        (new_generalized_bulk_flow.rs:832-991)."""
+        self._check_a(int(a_idx))
+        n_t = int(n_t)
+        S = self._coefficients.shape[0]
+        w = np.ascontiguousarray(np.asarray(w_arr, dtype=np.float64).ravel())
+        if float(self._interior[int(a_idx), 0]) >= float(t_end) or n_t < 2:
+            tb = 0.0 if t_begin is None else float(t_begin)
+            if float(self._interior[int(a_idx), 0]) < float(t_end) and tb > float(t_end):
+                raise ValueError(f"Invalid time range: t_begin={_rust_f64(tb)} > t_end={_rust_f64(float(t_end))}")
+            return np.zeros((6, S, w.size, max(n_t, 0)), dtype=np.complex128)
+        return self.compute_c_tensor_integrand(w, t_begin=t_begin, t_end=t_end, n_t=n_t,
+                                               selected_bubbles=np.array([int(a_idx)]))
+
+
 def tt_energy(c_tensor, khat=(0.0, 0.0, 1.0)):
     """Lambda_ij,lm(k) C*_ij C_lm = Tr[P C* P C] - |Tr[P C]|^2 / 2, P = 1 - k k^T
     (docs/generalized_bulkflow.md:8-17), for c_tensor (6, ...) in the order

@@ -211,6 +211,18 @@ BgwStatus bgwx_generalized_bulk_flow_compute_c_tensor_khat(bgw_generalized_bulk_
                                                           const size_t *selected_bubbles, size_t n_selected_bubbles,
                                                           BgwComplex64 *out, size_t out_len);
 
+/* The time-resolved tensor integrand (the reference's
+ * NewGeneralizedBulkFlow::compute_c_tensor_integrand,
+ * new_generalized_bulk_flow.rs:832-1065): out (6, S, W, n_t), each step's
+ * A_ij e^{i w (t - z_a)} (trapezoid dt weight) / (6 pi) summed over the
+ * selected bubbles (NULL = all); plain FP64, unrotated configuration. */
+BgwStatus bgwx_generalized_bulk_flow_compute_c_tensor_integrand(bgw_generalized_bulk_flow *bulk_flow,
+                                                                const double *w_arr, size_t n_w, bool has_t_begin,
+                                                                double t_begin, double t_end, size_t n_t,
+                                                                const size_t *selected_bubbles,
+                                                                size_t n_selected_bubbles, BgwComplex64 *out,
+                                                                size_t out_len);
+
 /* Draws the bubbles of n_realizations nucleation Monte Carlo realizations on
  * the GPU (one block per realization): exponential-rate nucleation in a
  * periodic cube of side box_side, candidates arriving as a Poisson process

@@ -89,3 +89,17 @@ def test_gpu_tensor_khat_and_scalar_consistency(gpu_available):
     assert err_per_w(got[:, 1], sc[:, 1]) < TOL
     assert np.array_equal(g.compute_c_tensor(c.w, t_end=1.5, n_t=48, selected_bubbles=np.array([], dtype=int)),
                           np.zeros((6, 1, c.w.size), dtype=complex))
+
+
+@pytest.mark.gpu
+def test_gpu_tensor_integrand_sums_to_the_tensor(gpu_available):
+    c = W.config(1)
+    g = make(c, [[1.0], [0.5]], [[5.0], [2.5]], 0.7)
+    tot = g.compute_c_tensor(c.w, t_end=1.5, n_t=40)
+    integ = g.compute_c_tensor_integrand(c.w, t_end=1.5, n_t=40)
+    assert integ.shape == (6, 2, c.w.size, 40)
+    assert err_per_w(integ.sum(axis=-1), tot) < TOL
+    one = g.compute_c_tensor_integrand_fixed_bubble(2, c.w, None, 1.5, 40)
+    ref1 = O.compute_c_tensor(c.interior, c.exterior, 16, 16, c.w, 1.5, 40, coefficients=[[1.0], [0.5]],
+                              powers=[[5.0], [2.5]], damping=0.7, selected=[2])
+    assert err_per_w(one.sum(axis=-1), ref1) < TOL
