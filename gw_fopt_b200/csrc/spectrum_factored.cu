@@ -401,17 +401,50 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             double dq[NQ];
 #pragma unroll
             for (int q = 0; q < NQ; ++q) dq[q] = 0.0;
-            const uint32_t pat = 0x01010101u * (uint32_t)lane;
-            for (int e4 = e0 & ~3; e4 < e1; e4 += 4) {
-                uint32_t eq = __vcmpeq4(*reinterpret_cast<const uint32_t*>(evs + e4), pat);
-                if (e4 < e0) eq &= 0xffffffffu << (8 * (e0 - e4));
-                if (e1 - e4 < 4) eq &= (1u << (8 * (e1 - e4))) - 1u;
-                while (eq) {
-                    const int by = (__ffs(eq) - 1) >> 3;
-                    eq &= ~(0xffu << (8 * by));
-                    const double* qe = evq + (size_t)(e4 + by) * NQ;
+            if (NB >= 32 && e1 - e0 > 32) {
+                // Many events: lanes take 32 events at a time; the events of one step
+                // (a __match_any group) are added by the group's lowest lane in event
+                // order and the group sum is added to that step's row of a table in the
+                // (by now unused) block-total array, rounds in event order.
+                double* D = btot;  // [32 steps][NQ]
 #pragma unroll
-                    for (int q = 0; q < NQ; ++q) dq[q] += qe[q];
+                for (int q = 0; q < NQ; ++q) D[lane * NQ + q] = 0.0;
+                __syncwarp();
+                for (int r0 = e0; r0 < e1; r0 += 32) {
+                    const int e = r0 + lane;
+                    const bool valid = e < e1;
+                    const int se = valid ? (int)evs[e] : 32 + lane;
+                    const unsigned m = __match_any_sync(full, se);
+                    if (valid && lane == __ffs(m) - 1) {
+                        double g[NQ];
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) g[q] = 0.0;
+                        for (unsigned mm = m; mm; mm &= mm - 1) {
+                            const double* qe = evq + (size_t)(r0 + __ffs(mm) - 1) * NQ;
+#pragma unroll
+                            for (int q = 0; q < NQ; ++q) g[q] += qe[q];
+                        }
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) D[se * NQ + q] += g[q];
+                    }
+                    __syncwarp();
+                }
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) dq[q] = D[lane * NQ + q];
+                __syncwarp();
+            } else {
+                const uint32_t pat = 0x01010101u * (uint32_t)lane;
+                for (int e4 = e0 & ~3; e4 < e1; e4 += 4) {
+                    uint32_t eq = __vcmpeq4(*reinterpret_cast<const uint32_t*>(evs + e4), pat);
+                    if (e4 < e0) eq &= 0xffffffffu << (8 * (e0 - e4));
+                    if (e1 - e4 < 4) eq &= (1u << (8 * (e1 - e4))) - 1u;
+                    while (eq) {
+                        const int by = (__ffs(eq) - 1) >> 3;
+                        eq &= ~(0xffu << (8 * by));
+                        const double* qe = evq + (size_t)(e4 + by) * NQ;
+#pragma unroll
+                        for (int q = 0; q < NQ; ++q) dq[q] += qe[q];
+                    }
                 }
             }
             // collided sums through this step (inclusive scan), uncollided after it (suffix scan)

@@ -222,6 +222,28 @@ def test_config2_subset(gpu_available, kernel):
     check(kernel, out, ref, "config2 subset")
 
 
+@pytest.mark.parametrize("kernel", ["fp64_factored", "mixed"])
+def test_dense_collision_blocks(gpu_available, kernel):
+    """Config 2 geometry with 192 phi patches and 1056 steps (33 blocks of 32): a row's
+    collisions crowd into a few step blocks with more than 32 events each, the case
+    in which k_beta sums each step's events by match groups."""
+    c = W.config(2)
+    sel = np.array([5, 300])
+    n_cos, n_phi, n_t, w = 16, 192, 1056, c.w[::16]
+    g = make_flow(c.interior, c.exterior, n_cos, n_phi, c.coefficients, c.powers, kernel=kernel)
+    out = g.compute_c_integral(w, t_begin=0.0, t_end=c.t_end, n_t=n_t, selected_bubbles=sel)
+    ref = O.compute_c_integral(c.interior, c.exterior, n_cos, n_phi, w, c.t_end, n_t, t_begin=0.0,
+                               coefficients=c.coefficients, powers=c.powers, selected=sel)
+    # the case under test occurs: some row has a 32-step block holding more than 32 collisions
+    codes, tau = O.first_colliding(c.interior, c.exterior, n_cos, n_phi, 5, 6, with_delta_tab=True)
+    t_arr = np.linspace(0.0, c.t_end, n_t)
+    ta = c.interior[5, 0]
+    k = np.searchsorted(t_arr - ta, tau[0], side="left")
+    busiest = max(np.bincount(k[i][(tau[0][i] > 0) & (k[i] < n_t)] // 32, minlength=33).max() for i in range(n_cos))
+    assert busiest > 32
+    check(kernel, out, ref, "dense collision blocks")
+
+
 def test_python_fixed_bubble_and_masks(gpu_available):
     p = golden_cases()["bench5"]
     g = make_flow(p["interior"], p["exterior"], int(p["n_cos"]), int(p["n_phi"]), p["coeffs"], p["powers"])
