@@ -51,6 +51,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="CPU-baseline sample budget")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="automatic launch shape instead of the measured one")
     return ap.parse_args()
 
 
@@ -197,6 +198,8 @@ def run_b200(args):
     K = cfg.khat.shape[0]
     cfg.khat = khat_shard(K, rank, world)
     g = make_flow(cfg, args.kernel)
+    if not args.no_autotune:
+        g.set_autotune(True)  # the first warm-up step measures the launch shape
     lib = L.lib()
     S, Wn = cfg.coefficients.shape[0], cfg.w.size
     # a created stream: handle 0 (torch's legacy default stream) would mean "library's own stream"
@@ -235,6 +238,7 @@ def run_b200(args):
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
+    launch_shape = g.last_launch_shape()
     ms = max_over_ranks(e0.elapsed_time(e1), device="cuda")
     ms_step = ms / args.steps
     pte_total = cfg.pte * world
@@ -328,7 +332,9 @@ def run_b200(args):
             "config": {"workload": cfg.name, "bubbles": int(cfg.n), "colliders": int(cfg.n + cfg.exterior.shape[0]),
                        "n_cos": cfg.n_cos, "n_phi": cfg.n_phi, "n_t": cfg.n_t, "n_w": int(Wn),
                        "n_khat_per_gpu": int(K), "kernel": args.kernel, "pte_per_step": pte_total,
-                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"khat-shard x{world}"},
+                       "l2": "flushed between steps (256 MiB write)", "parallelism": f"khat-shard x{world}",
+                       "launch_shape": dict(zip(("frames_per_launch", "row_parts"), launch_shape),
+                                            autotuned=not args.no_autotune)},
             "roofline": roofline, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
             "compare": compare}
     if compare:

@@ -57,6 +57,10 @@ SIGNATURES = {
     "bgwx_check_causality": (C.c_int, [_dp, C.c_size_t, _dp, C.c_size_t]),
     "bgwx_generalized_bulk_flow_new_unchecked": (C.c_int, [C.POINTER(_hp), _dp, C.c_size_t, _dp, C.c_size_t]),
     "bgwx_generalized_bulk_flow_set_kernel": (C.c_int, [_hp, C.c_int]),
+    "bgwx_generalized_bulk_flow_set_launch_shape": (C.c_int, [_hp, C.c_size_t, C.c_size_t]),
+    "bgwx_generalized_bulk_flow_set_autotune": (C.c_int, [_hp, C.c_bool]),
+    "bgwx_generalized_bulk_flow_last_launch_shape": (C.c_int, [_hp, C.POINTER(C.c_size_t),
+                                                                C.POINTER(C.c_size_t)]),
     "bgwx_generalized_bulk_flow_first_colliding": (
         C.c_int, [_hp, C.c_size_t, C.c_size_t, C.POINTER(C.c_int32), _dp]),
     "bgwx_generalized_bulk_flow_compute_c_integral_khat": (

@@ -1,0 +1,171 @@
+// Measured launch shape of the factored spectrum kernels.
+//
+// Two knobs set how a spectrum call is cut into launches: the number of k-hat
+// frames per launch (each launch runs masks, beta and the GEMM over that many
+// frames; the memory budget gives the largest) and, for the tensor-core GEMM,
+// the number of cos-theta row parts each (frequency tile, column tile) is
+// split into (the wave-fill model picks one).  The tuner times a few
+// candidates around the automatic choice on a sample of the job's own frames
+// and keeps the fastest per frame.  Every candidate computes the same spectrum:
+// frames are independent and the row parts only regroup FP64 partial sums.
+//
+// Choices are keyed by the device (name, multiprocessor count) and every size
+// the launch shapes depend on; they live for the process and, when
+// BGWX_AUTOTUNE_CACHE names a file, are read from and appended to that file
+// (one "key frames row_parts" line per shape).
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "bgw_internal.h"
+#include "device_common.cuh"
+
+namespace bgw {
+
+namespace {
+
+std::mutex g_mu;
+std::map<std::string, LaunchShape> g_cache;
+bool g_loaded = false;
+
+const char* cache_file() {
+    const char* p = std::getenv("BGWX_AUTOTUNE_CACHE");
+    return (p && *p) ? p : nullptr;
+}
+
+void load_locked() {
+    if (g_loaded) return;
+    g_loaded = true;
+    const char* path = cache_file();
+    if (!path) return;
+    std::ifstream in(path);
+    std::string line;
+    while (std::getline(in, line)) {
+        std::istringstream ls(line);
+        std::string key;
+        long long f = 0, r = 0;
+        if (!(ls >> key >> f >> r) || f < 1 || r < 1 || r > 16) continue;  // malformed lines are skipped
+        g_cache[key] = LaunchShape{(size_t)f, (int)r};
+    }
+}
+
+void append_locked(const std::string& key, const LaunchShape& s) {
+    const char* path = cache_file();
+    if (!path) return;
+    std::ofstream out(path, std::ios::app);
+    if (out) out << key << ' ' << s.frames_per_launch << ' ' << s.row_parts << '\n';
+}
+
+std::string shape_key(const Device* dev, const SpectrumJob& job) {
+    cudaDeviceProp prop{};
+    CUDA_OK(cudaGetDeviceProperties(&prop, dev->id));
+    std::string name = prop.name;
+    for (auto& ch : name)
+        if (ch == ' ' || ch == '\t') ch = '_';
+    std::ostringstream k;
+    k << name << ':' << dev->n_sm << ":k" << (int)job.kernel << ":int" << job.n_int << ":tot" << job.n_tot << ":sel"
+      << job.n_sel << ":c" << job.n_cos << ":p" << job.n_phi << ":t" << job.n_t << ":w" << job.n_w << ":s"
+      << job.n_sets << ":m" << job.n_terms << ":d" << (job.has_damping ? 1 : 0) << ":K" << job.n_k;
+    return k.str();
+}
+
+// Device time of one spectrum run of `job` into the device array `out`.
+float time_run(Device* dev, const SpectrumJob& job, double* out) {
+    CUDA_OK(cudaEventRecord(dev->ev[6], dev->stream));
+    run_spectrum(dev, job, out, true, nullptr);  // enqueued on dev->stream, not synchronised
+    CUDA_OK(cudaEventRecord(dev->ev[7], dev->stream));
+    CUDA_OK(cudaEventSynchronize(dev->ev[7]));
+    float ms = 0.0f;
+    CUDA_OK(cudaEventElapsedTime(&ms, dev->ev[6], dev->ev[7]));
+    return ms;
+}
+
+}  // namespace
+
+LaunchShape autotune_launch_shape(Device* dev, const SpectrumJob& job) {
+    LaunchShape automatic;
+    if (job.kernel == BGWX_KERNEL_FP64_DIRECT || job.n_sel == 0 || job.n_k == 0 || job.n_w == 0 || job.n_sets == 0)
+        return automatic;
+    CUDA_OK(cudaSetDevice(dev->id));
+    const std::string key = shape_key(dev, job);
+    {
+        std::lock_guard<std::mutex> lk(g_mu);
+        load_locked();
+        auto it = g_cache.find(key);
+        if (it != g_cache.end()) return it->second;
+    }
+    const size_t kc_max = std::min(job.n_k, spectrum_max_frames_per_launch(job));
+    // the sample: one launch of the largest frame count (all frames if fewer)
+    const size_t n_s = kc_max;
+    std::vector<size_t> frames;
+    for (size_t f = kc_max; f >= 1 && frames.size() < 3; f /= 2) {
+        frames.push_back(f);
+        if (f == 1) break;
+    }
+    struct Cand {
+        size_t f;
+        int r;
+    };
+    std::vector<Cand> cands;
+    const int r_max = std::max(1, std::min(16, (int)job.n_cos / 8));
+    for (size_t f : frames) {
+        const int r0 = factored_auto_row_parts(dev, job, f);
+        if (job.kernel != BGWX_KERNEL_MIXED) {
+            cands.push_back({f, 1});
+            continue;
+        }
+        for (int r : {r0, r0 - 1, r0 + 1})
+            if (r >= 1 && r <= r_max) {
+                bool dup = false;
+                for (const Cand& c : cands) dup |= (c.f == f && c.r == r);
+                if (!dup) cands.push_back({f, r});
+            }
+    }
+    SpectrumJob sub = job;
+    sub.n_k = n_s;  // the first n_s frames (rot rows are frame-major)
+    if (!job.rot) sub.n_k = 1;
+    const size_t out_bytes = sub.n_k * 2 * job.n_sets * job.n_w * sizeof(double2);
+    double* out = nullptr;
+    CUDA_OK(cudaMalloc(&out, out_bytes));
+    LaunchShape best;
+    float best_ms = 0.0f;
+    try {
+        // untimed first run: work arrays grow to the largest candidate, tables are built
+        sub.frames_per_launch = cands.front().f;
+        sub.row_parts = cands.front().r;
+        run_spectrum(dev, sub, out, true, nullptr);
+        for (const Cand& c : cands) {
+            sub.frames_per_launch = c.f;
+            sub.row_parts = c.r;
+            const float ms = time_run(dev, sub, out);
+            if (best.frames_per_launch == 0 || ms < best_ms) {
+                best_ms = ms;
+                best.frames_per_launch = c.f;
+                best.row_parts = c.r;
+            }
+        }
+    } catch (...) {
+        cudaStreamSynchronize(dev->stream);
+        cudaFree(out);
+        throw;
+    }
+    CUDA_OK(cudaStreamSynchronize(dev->stream));
+    CUDA_OK(cudaFree(out));
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_cache.find(key) == g_cache.end()) {
+        g_cache[key] = best;
+        append_locked(key, best);
+    }
+    return g_cache[key];
+}
+
+}  // namespace bgw

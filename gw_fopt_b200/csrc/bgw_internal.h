@@ -60,6 +60,17 @@ struct SpectrumJob {
     const double* rot = nullptr;
     size_t n_k = 1;
     BgwxKernel kernel = BGWX_KERNEL_FP64_DIRECT;
+    // launch shape; 0 = automatic (frames per launch from the memory budget,
+    // row parts from the wave-fill model).  frames_per_launch is capped by the
+    // budget; row_parts applies to the tensor-core GEMM only (at most 16).
+    size_t frames_per_launch = 0;
+    int row_parts = 0;
+};
+
+// The launch shape a spectrum call used (or is to use).
+struct LaunchShape {
+    size_t frames_per_launch = 0;
+    int row_parts = 0;
 };
 
 struct MaskJob {
@@ -81,6 +92,25 @@ void device_destroy(Device*);
 // the call returns without synchronising (timings are then not filled).
 // Throws Error.
 void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_device, BgwxTimings* timings);
+
+// The launch shape of the last run_spectrum on this device (frames per launch
+// and GEMM row parts actually used).
+LaunchShape last_launch_shape(const Device* dev);
+
+// Frames per launch that the memory budget allows for this job.
+size_t spectrum_max_frames_per_launch(const SpectrumJob& job);
+
+// Row parts the wave-fill model picks for kn frames per launch (1 unless the
+// job runs the tensor-core GEMM).
+int factored_auto_row_parts(const Device* dev, const SpectrumJob& job, size_t kn);
+
+// Measured launch shape for a factored-kernel spectrum job: candidate frame
+// counts per launch and GEMM row splits are timed on the device on a sample of
+// the job's frames, once per (device, problem shape); the choice is kept for
+// the process and, when the environment variable BGWX_AUTOTUNE_CACHE names a
+// file, in that file.  The FP64 direct kernel has no tunable shape and gets
+// the automatic one.  Throws Error.
+LaunchShape autotune_launch_shape(Device* dev, const SpectrumJob& job);
 
 // Runs one job per realization back to back on the handle's stream (largest
 // first, so the grow-only work arrays are sized once) into one device array

@@ -34,6 +34,9 @@ struct bgw_generalized_bulk_flow {
     double damping = 0.0;
     size_t num_threads = 1;
     BgwxKernel kernel = BGWX_KERNEL_FP64_DIRECT;
+    // launch shape of spectrum calls: fixed (non-zero), measured (autotune) or automatic
+    size_t frames_per_launch = 0, row_parts = 0;
+    bool autotune = false;
     bgw::Device* dev = nullptr;
     BgwxTimings timings{};
     ~bgw_generalized_bulk_flow() {
@@ -178,6 +181,19 @@ bgw::SpectrumJob settings_job(const bgw_generalized_bulk_flow* h, const std::vec
     return job;
 }
 
+// The handle's launch shape into a spectrum job: a fixed shape when one is
+// set, else the measured one when autotuning is on, else automatic.
+void apply_launch_shape(bgw_generalized_bulk_flow* h, bgw::SpectrumJob& job) {
+    if (h->frames_per_launch || h->row_parts) {
+        job.frames_per_launch = h->frames_per_launch;
+        job.row_parts = (int)h->row_parts;
+    } else if (h->autotune) {
+        const bgw::LaunchShape s = bgw::autotune_launch_shape(device(h), job);
+        job.frames_per_launch = s.frames_per_launch;
+        job.row_parts = s.row_parts;
+    }
+}
+
 // Rotations R(k) of the (n_khat, 3) unit rows.
 std::vector<double> khat_rotations(const double* khat, size_t n_khat) {
     const double* k = slice(khat, checked_mul(n_khat, 3, "khat"), "khat");
@@ -237,6 +253,7 @@ void compute_common(bgw_generalized_bulk_flow* h, const double* w_arr, size_t n_
             job.n_tot = h->n_int + h->n_ext;
             job.sel = ids.data();
             job.n_sel = ids.size();
+            apply_launch_shape(h, job);
             if (out_device) {
                 bgw::run_spectrum(device(h), job, static_cast<double*>(out_device), true, &h->timings);
                 device_written = true;
@@ -787,6 +804,36 @@ BgwStatus bgwx_generalized_bulk_flow_set_kernel(bgw_generalized_bulk_flow* bulk_
             kernel != BGWX_KERNEL_MIXED_SIMT)
             throw Error{"unknown kernel " + std::to_string((int)kernel)};
         h->kernel = kernel;
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_set_launch_shape(bgw_generalized_bulk_flow* bulk_flow, size_t frames_per_launch,
+                                                      size_t row_parts) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        if (row_parts > 16) throw Error{"row_parts must be at most 16"};
+        h->frames_per_launch = frames_per_launch;
+        h->row_parts = row_parts;
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_set_autotune(bgw_generalized_bulk_flow* bulk_flow, bool enabled) {
+    return run_ffi([&] { handle(bulk_flow)->autotune = enabled; });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_last_launch_shape(const bgw_generalized_bulk_flow* bulk_flow,
+                                                       size_t* out_frames_per_launch, size_t* out_row_parts) {
+    return run_ffi([&] {
+        if (!bulk_flow) throw Error{"bulk_flow must not be null"};
+        if (!out_frames_per_launch || !out_row_parts) throw Error{"outputs must not be null"};
+        const bgw_generalized_bulk_flow* h = bulk_flow;
+        *out_frames_per_launch = 0;
+        *out_row_parts = 0;
+        if (h->dev) {
+            const bgw::LaunchShape s = bgw::last_launch_shape(h->dev);
+            *out_frames_per_launch = s.frames_per_launch;
+            *out_row_parts = (size_t)s.row_parts;
+        }
     });
 }
 

@@ -83,6 +83,8 @@ struct Device {
     DevBuf tc_atab;                                  // tensor-core GEMM: time-phase table
     std::vector<double> tc_key;                      // (n_w, n_cos, n_t, w, cos-theta, t) of tc_atab
     DevBuf adj_gbar, adj_scratch, adj_grad, adj_mtab; // adjoint: cotangents, work arrays, gradients, phases
+    size_t last_frames_per_launch = 0;               // launch shape of the last spectrum call
+    int last_row_parts = 0;
     ~Device();
 };
 

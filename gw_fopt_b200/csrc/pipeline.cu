@@ -552,6 +552,23 @@ size_t mask_budget_bytes() {
 
 }  // namespace
 
+size_t spectrum_max_frames_per_launch(const SpectrumJob& job) {
+    const size_t nd = job.n_cos * job.n_phi;
+    const size_t per = (job.tensor ? 6 : 2) * job.n_sets * job.n_w;
+    const size_t per_k = job.n_sel * nd * sizeof(double) +
+                         (job.kernel == BGWX_KERNEL_FP64_DIRECT ? job.n_sel * per * sizeof(double2)
+                                                                : factored_bytes_per_frame(job));
+    const size_t kc = std::max<size_t>(1, mask_budget_bytes() / std::max<size_t>(per_k, 1));
+    return std::min<size_t>(kc, 65535);
+}
+
+LaunchShape last_launch_shape(const Device* dev) {
+    LaunchShape s;
+    s.frames_per_launch = dev->last_frames_per_launch;
+    s.row_parts = dev->last_row_parts;
+    return s;
+}
+
 void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_tau, BgwxTimings* tm) {
     CUDA_OK(cudaSetDevice(dev->id));
     const size_t nd = job.n_cos * job.n_phi;
@@ -612,12 +629,11 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     double* cosphi = job.tensor ? upload(dev, dev->cosphi, job.cosphi, job.n_phi, tm) : nullptr;
     double* sinphi = job.tensor ? upload(dev, dev->sinphi, job.sinphi, job.n_phi, tm) : nullptr;
 
-    // frames per chunk: bounded by the mask buffer budget
-    const size_t per_k = job.n_sel * nd * sizeof(double) +
-                         (job.kernel == BGWX_KERNEL_FP64_DIRECT ? job.n_sel * per * sizeof(double2)
-                                                                : factored_bytes_per_frame(job));
-    size_t kc = std::max<size_t>(1, std::min(K, mask_budget_bytes() / std::max<size_t>(per_k, 1)));
-    kc = std::min<size_t>(kc, 65535);
+    // frames per chunk: bounded by the mask buffer budget (and by the job's launch shape)
+    size_t kc = std::min(K, spectrum_max_frames_per_launch(job));
+    if (job.frames_per_launch) kc = std::min(kc, job.frames_per_launch);
+    dev->last_frames_per_launch = kc;
+    dev->last_row_parts = job.kernel == BGWX_KERNEL_FP64_DIRECT ? 1 : 0;  // the factored launch records its own
     dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
     if (job.kernel == BGWX_KERNEL_FP64_DIRECT) dev->partial.ensure(kc * job.n_sel * per * sizeof(double2));
     double2* final_out = out_is_device ? reinterpret_cast<double2*>(out) : nullptr;

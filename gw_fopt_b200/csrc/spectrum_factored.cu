@@ -963,7 +963,10 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     // tensor-core path: each column tile's CTAs split the cos-theta rows so that
     // the grid fills whole waves of one CTA per SM
     const int row_parts =
-        tc ? tc_row_parts((size_t)((n_w + 63) / 64) * kn * G.tiles_per_frame, n_cos, dev->n_sm) : 1;
+        !tc ? 1
+            : job.row_parts > 0 ? std::min(std::min(job.row_parts, 16), n_cos)
+                                : tc_row_parts((size_t)((n_w + 63) / 64) * kn * G.tiles_per_frame, n_cos, dev->n_sm);
+    dev->last_row_parts = row_parts;
     dev->fact_partial.ensure((size_t)kn * G.tiles_per_frame * row_parts * per * sizeof(double2));
     A.partial = (double2*)dev->fact_partial.p;
     if (tc) {
@@ -1042,6 +1045,12 @@ uint64_t launch_factored(Device* dev, const SpectrumJob& job, const D4* bub_fram
                                    kn, out, ev3);
     return launch_typed<double>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, kn,
                                 out, ev3);
+}
+
+int factored_auto_row_parts(const Device* dev, const SpectrumJob& job, size_t kn) {
+    if (job.kernel != BGWX_KERNEL_MIXED) return 1;
+    const FactGeom G = fact_geom(job, sizeof(float));
+    return tc_row_parts((size_t)((job.n_w + 63) / 64) * kn * G.tiles_per_frame, (int)job.n_cos, dev->n_sm);
 }
 
 size_t factored_bytes_per_frame(const SpectrumJob& job) {

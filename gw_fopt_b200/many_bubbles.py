@@ -542,6 +542,26 @@ class GeneralizedBulkFlow:
              "mixed": L.KERNEL_MIXED, "mixed_simt": L.KERNEL_MIXED_SIMT}[kernel]
         _call(L.lib().bgwx_generalized_bulk_flow_set_kernel(self._h, k))
 
+    def set_launch_shape(self, frames_per_launch: int = 0, row_parts: int = 0) -> None:
+        """Fixes how spectrum calls are cut into launches (B200 extension): at most
+        ``frames_per_launch`` k-hat frames per launch and ``row_parts`` cos-theta row
+        parts per tensor-core GEMM tile; 0 keeps the automatic choice of either."""
+        if frames_per_launch < 0 or row_parts < 0:
+            raise ValueError("frames_per_launch and row_parts must be >= 0")
+        _call(L.lib().bgwx_generalized_bulk_flow_set_launch_shape(self._h, int(frames_per_launch), int(row_parts)))
+
+    def set_autotune(self, enabled: bool = True) -> None:
+        """Measured launch shapes (B200 extension): the first spectrum call of each problem
+        shape on a factored kernel times candidate shapes on its own first frames and keeps
+        the fastest; ``BGWX_AUTOTUNE_CACHE`` may name a file that keeps the choices."""
+        _call(L.lib().bgwx_generalized_bulk_flow_set_autotune(self._h, bool(enabled)))
+
+    def last_launch_shape(self) -> tuple[int, int]:
+        """(frames per launch, GEMM row parts) of the last spectrum call; (0, 0) before one."""
+        f, r = C.c_size_t(0), C.c_size_t(0)
+        _call(L.lib().bgwx_generalized_bulk_flow_last_launch_shape(self._h, C.byref(f), C.byref(r)))
+        return int(f.value), int(r.value)
+
     # --- geometry -------------------------------------------------------------
     def _require_res(self, name="n_cos_thetax"):
         if self._n_cos is None:

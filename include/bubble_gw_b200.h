@@ -99,6 +99,30 @@ BgwStatus bgwx_generalized_bulk_flow_new_unchecked(bgw_generalized_bulk_flow **o
  * No counterpart in the reference (it has one f64 CPU path). */
 BgwStatus bgwx_generalized_bulk_flow_set_kernel(bgw_generalized_bulk_flow *bulk_flow, BgwxKernel kernel);
 
+/* Launch shape of the spectrum calls on this handle (compute_c_integral and
+ * the k-hat forms; not the ensemble or the adjoint): at most frames_per_launch
+ * k-hat frames per launch (0 = as many as the memory budget allows) and
+ * row_parts cos-theta row parts per tensor-core GEMM tile (0 = the wave-fill
+ * model's choice; at most 16; the mixed kernel only).  A non-zero value here
+ * takes precedence over autotuning.  The spectrum does not depend on the shape
+ * beyond the order of FP64 partial sums.  No counterpart in the reference. */
+BgwStatus bgwx_generalized_bulk_flow_set_launch_shape(bgw_generalized_bulk_flow *bulk_flow, size_t frames_per_launch,
+                                                      size_t row_parts);
+
+/* Measured launch shapes: with enabled, the first spectrum call of each problem
+ * shape (device, kernel, bubble counts, grids, coefficient sets) on a factored
+ * kernel times candidate shapes around the automatic one on its own first
+ * frames and keeps the fastest for the process; with the environment variable
+ * BGWX_AUTOTUNE_CACHE naming a file, choices are also read from and appended
+ * to it.  The FP64 direct kernel has no tunable shape.  Off by default.
+ * No counterpart in the reference. */
+BgwStatus bgwx_generalized_bulk_flow_set_autotune(bgw_generalized_bulk_flow *bulk_flow, bool enabled);
+
+/* The launch shape the last spectrum call on this handle used (frames per
+ * launch, GEMM row parts; zeros before the first call).  No counterpart. */
+BgwStatus bgwx_generalized_bulk_flow_last_launch_shape(const bgw_generalized_bulk_flow *bulk_flow,
+                                                       size_t *out_frames_per_launch, size_t *out_row_parts);
+
 /* First-collider codes (-1 None, i Interior(i), -(i+2) Exterior(i)) and the
  * collision delays of compute_delta_tab for interior bubbles [a_begin, a_end)
  * at k-hat = z, computed on the GPU.  out_codes: (a_end-a_begin, n_cos, n_phi)

@@ -240,3 +240,20 @@ def test_python_surface_errors_without_gpu():
     assert st[1, 3] == 2
     cut = mb.ExponentialTimeCutoff(2.0, 0.5)
     assert cut.t_cut == 1.0 and cut.t_0 == 0.25
+
+
+def test_launch_shape_settings_without_gpu():
+    from gw_fopt_b200 import many_bubbles as mb
+    lb = mb.LatticeBubbles(mb.EmptyLattice(), np.array([[0.0, 0, 10, 0], [0.0, 0, 0, 0]]))
+    g = mb.GeneralizedBulkFlow(lb)
+    assert g.last_launch_shape() == (0, 0)
+    g.set_launch_shape(2, 3)
+    g.set_launch_shape()
+    g.set_autotune(True)
+    g.set_autotune(False)
+    with pytest.raises(ValueError, match="row_parts must be at most 16"):
+        g.set_launch_shape(1, 17)
+    with pytest.raises(ValueError, match=">= 0"):
+        g.set_launch_shape(-1, 0)
+    f, r = C.c_size_t(7), C.c_size_t(7)
+    assert L.lib().bgwx_generalized_bulk_flow_last_launch_shape(None, C.byref(f), C.byref(r)) != 0
