@@ -150,9 +150,10 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
     const long row = (long)blockIdx.x * (blockDim.x >> 5) + warp;
     if (row >= A.n_rows) return;
     const int NB = A.nblk;
+    const int EV = A.n_phi;  // event capacity: one event per patch at most
     unsigned char* base = sm_b + (size_t)warp * A.per_warp_bytes;
-    double* evq = reinterpret_cast<double*>(base);             // [n_phi][NQ]
-    double* btot = evq + (size_t)A.n_phi * NQ;                  // [NB][NQ] block totals
+    double* evq = reinterpret_cast<double*>(base);             // [NQ][n_phi]: weight q of event e at q * n_phi + e
+    double* btot = evq + (size_t)A.n_phi * NQ;                  // [NQ][NB] block totals
     double* uend = btot + (size_t)NQ * NB;                      // [NB][2] uncollided after block
     double* pbeg = uend + 2 * NB;                               // [NB][2 SMC] collided before block
     int* evk = reinterpret_cast<int*>(pbeg + (size_t)2 * SMC * NB);  // [n_phi]
@@ -240,15 +241,15 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             const double tj = trow[j];
             const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
             const double qc = wj * A.cos2[j], qs = wj * A.sin2[j];
-            double* q = evq + (size_t)pos * NQ;
+            double* q = evq + pos;
             q[0] = qc;
-            q[1] = qs;
+            q[EV] = qs;
             const double ed = A.has_damp ? exp(tj / A.damp) : 1.0;
 #pragma unroll
             for (int t = 0; t < SMC; ++t) {
                 const double f = tpow(tj, A.powers[t]) * ed;
-                q[2 + 2 * t] = qc * f;
-                q[3 + 2 * t] = qs * f;
+                q[(2 + 2 * t) * EV] = qc * f;
+                q[(3 + 2 * t) * EV] = qs * f;
             }
         }
     };
@@ -271,7 +272,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
     for (int b = lane; b < NB; b += 32)
         if (boff[b] == boff[b + 1]) {
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) btot[(size_t)b * NQ + q] = 0.0;
+            for (int q = 0; q < NQ; ++q) btot[(size_t)q * NB + b] = 0.0;
         }
     for (int bc = 0; bc < NB; bc += 32) {
         const int bl = bc + lane;
@@ -282,7 +283,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             for (int q = 0; q < NQ; ++q) t[q] = 0.0;
             for (int e = boff[b] + lane; e < boff[b + 1]; e += 32) {
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) t[q] += evq[(size_t)e * NQ + q];
+                for (int q = 0; q < NQ; ++q) t[q] += evq[(size_t)q * EV + e];
             }
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
@@ -291,7 +292,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             }
             if (lane == 0) {
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) btot[(size_t)b * NQ + q] = t[q];
+                for (int q = 0; q < NQ; ++q) btot[(size_t)q * NB + b] = t[q];
             }
         }
     }
@@ -304,7 +305,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             const int b = bc + lane;
             double v[2 * SMC];
 #pragma unroll
-            for (int q = 0; q < 2 * SMC; ++q) v[q] = b < NB ? btot[(size_t)b * NQ + 2 + q] : 0.0;
+            for (int q = 0; q < 2 * SMC; ++q) v[q] = b < NB ? btot[(size_t)(2 + q) * NB + b] : 0.0;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
 #pragma unroll
@@ -325,7 +326,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         double cc = __shfl_sync(full, nc, 0), cs = __shfl_sync(full, ns, 0);
         for (int bc = ((NB - 1) >> 5) << 5; bc >= 0; bc -= 32) {
             const int b = bc + lane;
-            double vc = b < NB ? btot[(size_t)b * NQ] : 0.0, vs = b < NB ? btot[(size_t)b * NQ + 1] : 0.0;
+            double vc = b < NB ? btot[b] : 0.0, vs = b < NB ? btot[(size_t)NB + b] : 0.0;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const double uc = __shfl_down_sync(full, vc, o), us = __shfl_down_sync(full, vs, o);
@@ -406,9 +407,9 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
                 // (a __match_any group) are added by the group's lowest lane in event
                 // order and the group sum is added to that step's row of a table in the
                 // (by now unused) block-total array, rounds in event order.
-                double* D = btot;  // [32 steps][NQ]
+                double* D = btot;  // [NQ][32 steps]
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) D[lane * NQ + q] = 0.0;
+                for (int q = 0; q < NQ; ++q) D[q * 32 + lane] = 0.0;
                 __syncwarp();
                 for (int r0 = e0; r0 < e1; r0 += 32) {
                     const int e = r0 + lane;
@@ -420,17 +421,17 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
 #pragma unroll
                         for (int q = 0; q < NQ; ++q) g[q] = 0.0;
                         for (unsigned mm = m; mm; mm &= mm - 1) {
-                            const double* qe = evq + (size_t)(r0 + __ffs(mm) - 1) * NQ;
+                            const double* qe = evq + (r0 + __ffs(mm) - 1);
 #pragma unroll
-                            for (int q = 0; q < NQ; ++q) g[q] += qe[q];
+                            for (int q = 0; q < NQ; ++q) g[q] += qe[(size_t)q * EV];
                         }
 #pragma unroll
-                        for (int q = 0; q < NQ; ++q) D[se * NQ + q] += g[q];
+                        for (int q = 0; q < NQ; ++q) D[q * 32 + se] += g[q];
                     }
                     __syncwarp();
                 }
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) dq[q] = D[lane * NQ + q];
+                for (int q = 0; q < NQ; ++q) dq[q] = D[q * 32 + lane];
                 __syncwarp();
             } else {
                 const uint32_t pat = 0x01010101u * (uint32_t)lane;
@@ -441,9 +442,9 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
                     while (eq) {
                         const int by = (__ffs(eq) - 1) >> 3;
                         eq &= ~(0xffu << (8 * by));
-                        const double* qe = evq + (size_t)(e4 + by) * NQ;
+                        const double* qe = evq + (e4 + by);
 #pragma unroll
-                        for (int q = 0; q < NQ; ++q) dq[q] += qe[q];
+                        for (int q = 0; q < NQ; ++q) dq[q] += qe[(size_t)q * EV];
                     }
                 }
             }
