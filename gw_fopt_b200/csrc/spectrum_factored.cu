@@ -156,8 +156,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
     double* btot = evq + (size_t)A.n_phi * NQ;                  // [NQ][NB] block totals
     double* uend = btot + (size_t)NQ * NB;                      // [NB][2] uncollided after block
     double* pbeg = uend + 2 * NB;                               // [NB][2 SMC] collided before block
-    int* evk = reinterpret_cast<int*>(pbeg + (size_t)2 * SMC * NB);  // [n_phi]
-    int* boff = evk + A.n_phi;                                  // [NB+1]
+    int* boff = reinterpret_cast<int*>(pbeg + (size_t)2 * SMC * NB);  // [NB+1]
     int* brun = boff + NB + 1;                                  // [NB]
     uint8_t* evs = reinterpret_cast<uint8_t*>(brun + NB);       // [n_phi + 4] step of each event within its block
     const int slot = (int)((row / A.n_cos) % A.n_sel);
@@ -236,7 +235,6 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         if (b >= 0 && lane == __ffs(m) - 1) brun[b] += __popc(m);
         __syncwarp();
         if (b >= 0) {
-            evk[pos] = kj;
             evs[pos] = (uint8_t)(kj & 31);
             const double tj = trow[j];
             const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
@@ -926,7 +924,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         B.t_pad = G.t_pad;
         const int NQ = 2 + 2 * SM;
         size_t pw = (size_t)n_phi * NQ * sizeof(double) + 2 * (size_t)NQ * G.nblk * sizeof(double) +
-                    ((size_t)n_phi + 2 * G.nblk + 1) * sizeof(int) + ((size_t)n_phi + 4);
+                    (2 * (size_t)G.nblk + 1) * sizeof(int) + ((size_t)n_phi + 4);
         pw = (pw + 15) & ~(size_t)15;
         B.per_warp_bytes = (int)pw;
         B.tc_layout = tc ? 1 : 0;
