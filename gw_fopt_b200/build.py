@@ -45,20 +45,35 @@ def needs_build() -> bool:
 
 
 def build(force: bool = False, ptxas_info: bool = False, verbose: bool = False) -> str:
+    """Compiles every source to an object (in parallel, under _build/) and links the library."""
     if not force and not needs_build() and not ptxas_info:
         return LIB_PATH
-    cmd = [_nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo",
-           "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math", "-shared",
-           "-I", os.path.join(ROOT, "include"), "-o", LIB_PATH, *sources()]
+    from concurrent.futures import ThreadPoolExecutor
+    obj_dir = os.path.join(ROOT, "_build", "obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    flags = ["-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off,-fno-fast-math",
+             "-I", os.path.join(ROOT, "include")]
     if ptxas_info:
-        cmd.insert(1, "-Xptxas=-v")
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
+        flags.insert(0, "-Xptxas=-v")
+
+    def compile_one(src):
+        obj = os.path.join(obj_dir, os.path.basename(src) + ".o")
+        cmd = [_nvcc(), *flags, "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        return obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 4)) as ex:
+        results = list(ex.map(compile_one, sources()))
+    for obj, res in results:
+        if res.returncode != 0:
+            raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
+        if ptxas_info:
+            sys.stderr.write(res.stderr)
+    cmd = [_nvcc(), *ARCH, "-shared", "-o", LIB_PATH, *[o for o, _ in results]]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
-    if ptxas_info:
-        sys.stderr.write(res.stderr)
+        raise RuntimeError("nvcc link failed:\n" + res.stdout + res.stderr)
     return LIB_PATH
 
 

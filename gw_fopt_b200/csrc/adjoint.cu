@@ -26,9 +26,10 @@
 //   k_adj_mtab    the time-phase table M_i(w, k), once per call
 //   k_adj_pq      per (frame, row): Re P and Im Q as two real products of depth W
 //   k_adj_rows    one warp per (frame, bubble, row): the patch sums above, dL/dtau per patch
-//   k_adj_geom    per (frame, bubble, patch): dL/dtau -> both bubbles of the collision (one atomic
-//                 per run of equal bubbles in a warp)
-//   k_adj_bubble  per (frame, bubble): the row partials of t_a and z_a (atomics)
+//   k_adj_bubble  per (frame, bubble): the row partials of t_a and z_a
+//   k_adj_geom    per (frame, bubble, patch): dL/dtau -> both bubbles of the collision, and the
+//                 bubble parts above, summed as fixed-point integers (deterministic; two passes:
+//                 exponent bound, then sums) and added to the gradients by k_adj_fixout
 //   k_adj_params  per parameter: fixed-order sum of the row partials
 
 #include <cuda_runtime.h>
@@ -358,46 +359,21 @@ __device__ __forceinline__ void rotate_back(const double* R, double& gx, double&
     gz = uz;
 }
 
-// Adds each lane's 4-vector to g_bub[key] (key < 0: nothing) with one atomic
-// per run of equal keys in consecutive lanes: neighbouring patches mostly share
-// their radiating bubble and their first collider.  Call with the full warp.
-__device__ __forceinline__ void warp_runs_add(double* g_bub, long key, double v0, double v1, double v2, double v3) {
-    const int lane = threadIdx.x & 31;
-    const long prev = __shfl_up_sync(0xffffffffu, key, 1);
-    const bool head = lane == 0 || prev != key;
-    const unsigned heads = __ballot_sync(0xffffffffu, head);
-    const int run = __popc(heads & (0xffffffffu >> (31 - lane)));  // runs started at or before this lane
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) {
-        const int r_up = __shfl_up_sync(0xffffffffu, run, off);
-        const double u0 = __shfl_up_sync(0xffffffffu, v0, off);
-        const double u1 = __shfl_up_sync(0xffffffffu, v1, off);
-        const double u2 = __shfl_up_sync(0xffffffffu, v2, off);
-        const double u3 = __shfl_up_sync(0xffffffffu, v3, off);
-        if (lane >= off && r_up == run) {
-            v0 += u0;
-            v1 += u1;
-            v2 += u2;
-            v3 += u3;
-        }
-    }
-    const int r_dn = __shfl_down_sync(0xffffffffu, run, 1);
-    const bool tail = lane == 31 || r_dn != run;
-    if (tail && key >= 0) {
-        double* g = g_bub + 4 * key;
-        atomicAdd(g + 0, v0);
-        atomicAdd(g + 1, v1);
-        atomicAdd(g + 2, v2);
-        atomicAdd(g + 3, v3);
-    }
-}
+// Bubble gradients are summed deterministically (the same bits on every run,
+// whatever the order in which blocks run): every contribution v becomes the
+// integer X = rint(v 2^(61 - E)), E the chunk's exponent bound (|v| < 2^E),
+// split as X = H 2^31 + L with 0 <= L < 2^31, and H and L are added with
+// 64-bit integer atomics, which are exact and so order-independent.  X keeps
+// v to double precision relative to the chunk's largest contribution; the
+// sums cannot overflow while a chunk has fewer than 2^31 contributions.
 
-__global__ void k_adj_geom(AdjArgs A) {
-    const int nd = A.n_cos * A.n_phi;
-    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int f = blockIdx.y;
-    long ka = -1, kb = -1;
-    double gt = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+// Contribution of item q of frame f: q < n_sel*nd is a patch whose dL/dtau
+// moves onto its first collider (kb, +g) and its radiating bubble (ka, -g);
+// q = n_sel*nd + slot is the radiating bubble's own (t, x, y, z) part.
+__device__ __forceinline__ void geom_item(const AdjArgs& A, int f, size_t q, long& ka, long& kb, double (&g)[4]) {
+    const size_t nd = (size_t)A.n_cos * A.n_phi;
+    ka = kb = -1;
+    g[0] = g[1] = g[2] = g[3] = 0.0;
     if (q < (size_t)A.n_sel * nd) {
         const int slot = (int)(q / nd), d = (int)(q % nd);
         const size_t o = ((size_t)f * A.n_sel + slot) * nd + d;
@@ -416,18 +392,134 @@ __global__ void k_adj_geom(AdjArgs A) {
                 const double D2 = -Dt * Dt + Dx * Dx + Dy * Dy + Dz * Dz;
                 const double inv = 1.0 / dot;
                 const double h = 0.5 * D2 * inv * inv;
-                gt = tb * (-Dt * inv + h);
-                gx = tb * (Dx * inv - h * n.x);
-                gy = tb * (Dy * inv - h * n.y);
-                gz = tb * (Dz * inv - h * n.z);
-                rotate_back(A.rot ? A.rot + 9 * f : nullptr, gx, gy, gz);
+                g[0] = tb * (-Dt * inv + h);
+                g[1] = tb * (Dx * inv - h * n.x);
+                g[2] = tb * (Dy * inv - h * n.y);
+                g[3] = tb * (Dz * inv - h * n.z);
+                rotate_back(A.rot ? A.rot + 9 * f : nullptr, g[1], g[2], g[3]);
                 ka = (long)a;
                 kb = (long)b;
             }
         }
+    } else if (q < (size_t)A.n_sel * nd + A.n_sel) {
+        const int slot = (int)(q - (size_t)A.n_sel * nd);
+        const double* bp = A.s.bubpart + ((size_t)f * A.n_sel + slot) * 4;
+        g[0] = bp[0];
+        g[1] = bp[1];
+        g[2] = bp[2];
+        g[3] = bp[3];
+        ka = (long)A.sel[slot];
     }
-    warp_runs_add(A.g_bub, kb, gt, gx, gy, gz);
-    warp_runs_add(A.g_bub, ka, -gt, -gx, -gy, -gz);
+}
+
+// Adds each lane's fixed-point 4-vector (high and low parts) to gfix[key]
+// (key < 0: nothing) with one atomic per run of equal keys in consecutive
+// lanes: neighbouring patches mostly share their radiating bubble and their
+// first collider.  Integer sums: exact in any order.  Call with the full warp.
+__device__ __forceinline__ void warp_runs_add(long long* gfix, long key, const long long (&h_in)[4],
+                                              const long long (&l_in)[4]) {
+    const int lane = threadIdx.x & 31;
+    long long h[4], l[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        h[c] = h_in[c];
+        l[c] = l_in[c];
+    }
+    const long prev = __shfl_up_sync(0xffffffffu, key, 1);
+    const bool head = lane == 0 || prev != key;
+    const unsigned heads = __ballot_sync(0xffffffffu, head);
+    const int run = __popc(heads & (0xffffffffu >> (31 - lane)));  // runs started at or before this lane
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const int r_up = __shfl_up_sync(0xffffffffu, run, off);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const long long uh = __shfl_up_sync(0xffffffffu, h[c], off);
+            const long long ul = __shfl_up_sync(0xffffffffu, l[c], off);
+            if (lane >= off && r_up == run) {
+                h[c] += uh;
+                l[c] += ul;
+            }
+        }
+    }
+    const int r_dn = __shfl_down_sync(0xffffffffu, run, 1);
+    const bool tail = lane == 31 || r_dn != run;
+    if (tail && key >= 0) {
+        unsigned long long* g = reinterpret_cast<unsigned long long*>(gfix + 8 * key);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            atomicAdd(g + 2 * c, (unsigned long long)h[c]);
+            atomicAdd(g + 2 * c + 1, (unsigned long long)l[c]);
+        }
+    }
+}
+
+__global__ void k_adj_gexp_init(int* gexp) { *gexp = -2000; }
+
+// PASS 0: the exponent bound of the chunk's contributions; PASS 1: their fixed-point sums.
+template <int PASS>
+__global__ void k_adj_geom(AdjArgs A) {
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int f = blockIdx.y;
+    long ka, kb;
+    double g[4];
+    geom_item(A, f, q, ka, kb, g);
+    if constexpr (PASS == 0) {
+        int e = -2000;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            int ex;
+            if (g[c] != 0.0 && isfinite(g[c])) {
+                frexp(g[c], &ex);  // |g| < 2^ex
+                e = max(e, ex);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
+        if ((threadIdx.x & 31) == 0 && e > -2000) atomicMax(A.s.gexp, e);
+    } else {
+        const int sh = 61 - *A.s.gexp;
+        long long h[4], l[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            long long X = 0;
+            if (isfinite(g[c])) {
+                X = __double2ll_rn(ldexp(g[c], sh));
+            } else if (kb >= 0 || ka >= 0) {
+                // a non-finite gradient is passed on as it is
+                if (kb >= 0) atomicAdd(A.g_bub + 4 * kb + c, g[c]);
+                if (ka >= 0 && kb >= 0) atomicAdd(A.g_bub + 4 * ka + c, -g[c]);
+                else if (ka >= 0) atomicAdd(A.g_bub + 4 * ka + c, g[c]);
+            }
+            h[c] = X >> 31;
+            l[c] = X & 0x7fffffffLL;
+        }
+        // a patch adds +g to its collider and -g to its radiating bubble; a bubble part adds +g
+        const bool patch = kb >= 0;
+        warp_runs_add(A.s.gfix, kb, h, l);
+        if (patch) {
+            // -X = (-H - 1) 2^31 + (2^31 - L) for L > 0, and -H 2^31 for L = 0
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const long long X = h[c] * (1LL << 31) + l[c];
+                h[c] = (-X) >> 31;
+                l[c] = (-X) & 0x7fffffffLL;
+            }
+        }
+        warp_runs_add(A.s.gfix, ka, h, l);
+    }
+}
+
+// g_bub += the chunk's fixed-point sums; the accumulators are cleared for the next chunk.
+__global__ void k_adj_fixout(AdjArgs A) {
+    const size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= 4 * A.n_tot) return;
+    const int sh = 61 - *A.s.gexp;
+    long long* p = A.s.gfix + 2 * c;
+    const long long H = p[0], L = p[1];
+    if (H != 0 || L != 0) A.g_bub[c] += ldexp((double)H, 31 - sh) + ldexp((double)L, -sh);
+    p[0] = 0;
+    p[1] = 0;
 }
 
 template <int SMC>
@@ -444,11 +536,11 @@ __global__ void k_adj_bubble(AdjArgs A) {
     // z' = R[2,:] . x  =>  dL/dx += dL/dz' R[2,:]
     double gx = 0.0, gy = 0.0, gz = sz;
     rotate_back(A.rot ? A.rot + 9 * f : nullptr, gx, gy, gz);
-    double* g = A.g_bub + 4 * (size_t)A.sel[slot];
-    atomicAdd(g + 0, st);
-    atomicAdd(g + 1, gx);
-    atomicAdd(g + 2, gy);
-    atomicAdd(g + 3, gz);
+    double* bp = A.s.bubpart + ((size_t)f * A.n_sel + slot) * 4;
+    bp[0] = st;
+    bp[1] = gx;
+    bp[2] = gy;
+    bp[3] = gz;
 }
 
 template <int SMC>
@@ -493,15 +585,18 @@ static uint64_t launch_typed(const AdjArgs& A, size_t kn, cudaStream_t st, const
         else launch_rows<S, SMC, 8>(A, rows, st, tt);
         CUDA_OK(cudaGetLastError());
         ++launches;
-        const size_t per = (size_t)A.n_sel * A.n_cos * A.n_phi;
-        dim3 gg((unsigned)((per + 255) / 256), (unsigned)kn);
-        k_adj_geom<<<gg, 256, 0, st>>>(A);
-        CUDA_OK(cudaGetLastError());
-        ++launches;
         dim3 gb((unsigned)((A.n_sel + 127) / 128), (unsigned)kn);
         k_adj_bubble<SMC><<<gb, 128, 0, st>>>(A);
         CUDA_OK(cudaGetLastError());
-        ++launches;
+        // every bubble gradient of the chunk: fixed-point sums (deterministic)
+        const size_t per = (size_t)A.n_sel * A.n_cos * A.n_phi + A.n_sel;
+        dim3 gg((unsigned)((per + 255) / 256), (unsigned)kn);
+        k_adj_gexp_init<<<1, 1, 0, st>>>(A.s.gexp);
+        k_adj_geom<0><<<gg, 256, 0, st>>>(A);
+        k_adj_geom<1><<<gg, 256, 0, st>>>(A);
+        k_adj_fixout<<<(unsigned)((4 * A.n_tot + 255) / 256), 256, 0, st>>>(A);
+        CUDA_OK(cudaGetLastError());
+        launches += 5;
         k_adj_params<SMC><<<2 * SMC, kAdjThreads, 0, st>>>(A, rows);
         CUDA_OK(cudaGetLastError());
         ++launches;

@@ -11,6 +11,9 @@ struct AdjointScratch {
     double* imq;      // (kn, n_sel, n_cos, n_t, 2S)  Im sum_w w conj(G) e^{i phi}
     double* taubar;   // (kn, n_sel, n_cos*n_phi)     dL/dtau
     double* rowpart;  // (kn, n_sel, n_cos, 2 + 2 S M) per-row partial sums
+    double* bubpart;  // (kn, n_sel, 4) gradient of each radiating bubble's own terms (t, x, y, z)
+    long long* gfix;  // (n_tot, 4, 2) bubble gradients of the chunk as fixed-point (high, low) integer sums
+    int* gexp;        // every contribution of the chunk is below 2^gexp in magnitude
 };
 
 // Launches the adjoint kernels of kn frames whose rotated bubbles, masks

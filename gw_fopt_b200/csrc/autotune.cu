@@ -78,14 +78,13 @@ std::string shape_key(const Device* dev, const SpectrumJob& job) {
     return k.str();
 }
 
-// Device time of one spectrum run of `job` into the device array `out`.
+// Device time of one spectrum run of `job` into the device array `out`
+// (run_spectrum's own events around its launches).  Throws Error when a
+// kernel of the run reported a failed wait.
 float time_run(Device* dev, const SpectrumJob& job, double* out) {
-    CUDA_OK(cudaEventRecord(dev->ev[6], dev->stream));
-    run_spectrum(dev, job, out, true, nullptr);  // enqueued on dev->stream, not synchronised
-    CUDA_OK(cudaEventRecord(dev->ev[7], dev->stream));
-    CUDA_OK(cudaEventSynchronize(dev->ev[7]));
+    run_spectrum(dev, job, out, true, nullptr);  // waits for the run and checks its error counters
     float ms = 0.0f;
-    CUDA_OK(cudaEventElapsedTime(&ms, dev->ev[6], dev->ev[7]));
+    CUDA_OK(cudaEventElapsedTime(&ms, dev->ev[4], dev->ev[5]));
     return ms;
 }
 
@@ -143,16 +142,24 @@ LaunchShape autotune_launch_shape(Device* dev, const SpectrumJob& job) {
         sub.frames_per_launch = cands.front().f;
         sub.row_parts = cands.front().r;
         run_spectrum(dev, sub, out, true, nullptr);
+        std::string last_err;
         for (const Cand& c : cands) {
             sub.frames_per_launch = c.f;
             sub.row_parts = c.r;
-            const float ms = time_run(dev, sub, out);
+            float ms = 0.0f;
+            try {
+                ms = time_run(dev, sub, out);
+            } catch (const Error& e) {  // a shape whose run failed is never chosen
+                last_err = e.msg;
+                continue;
+            }
             if (best.frames_per_launch == 0 || ms < best_ms) {
                 best_ms = ms;
                 best.frames_per_launch = c.f;
                 best.row_parts = c.r;
             }
         }
+        if (best.frames_per_launch == 0) throw Error{"autotune: every candidate launch shape failed: " + last_err};
     } catch (...) {
         cudaStreamSynchronize(dev->stream);
         cudaFree(out);

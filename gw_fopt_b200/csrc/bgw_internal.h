@@ -89,9 +89,13 @@ void device_destroy(Device*);
 
 // Runs the spectrum; out: (n_k, 2, n_sets, n_w) complex as interleaved
 // doubles.  With out_is_device the result is written to device memory and
-// the call returns without synchronising (timings are then not filled).
-// Throws Error.
-void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_device, BgwxTimings* timings);
+// only the device's error counters are read back (timings are then not
+// filled).  A call waits for its work and throws Error when a kernel reported
+// a failed wait.  `nested` calls (the batched ensemble) neither clear nor read
+// the error counters and return without synchronising: their caller does
+// both once.
+void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_device, BgwxTimings* timings,
+                  bool nested = false);
 
 // The launch shape of the last run_spectrum on this device (frames per launch
 // and GEMM row parts actually used).

@@ -80,8 +80,10 @@ struct Device {
     DevBuf fact_D, fact_kfirst, beta, fact_partial;  // factored-kernel work arrays
     DevBuf ens_out;                                  // batched ensemble: all realizations' spectra
     DevBuf pp_in, pp_small, pp_out;                  // spectrum post-processing: input, small tables, output
-    DevBuf tc_atab;                                  // tensor-core GEMM: time-phase table
+    DevBuf beta_scale;                               // int8 tensor-core GEMM: per-(bubble, row) beta scales
+    DevBuf tc_atab;                                  // int8 tensor-core GEMM: time-phase digits
     std::vector<double> tc_key;                      // (n_w, n_cos, n_t, w, cos-theta, t) of tc_atab
+    bool tc_key_reuse = false;                       // set by the batched ensemble: one grid for all calls
     DevBuf adj_gbar, adj_scratch, adj_grad, adj_mtab; // adjoint: cotangents, work arrays, gradients, phases
     size_t last_frames_per_launch = 0;               // launch shape of the last spectrum call
     int last_row_parts = 0;

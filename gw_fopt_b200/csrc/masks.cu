@@ -33,6 +33,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 
@@ -340,7 +341,7 @@ __global__ void __launch_bounds__(kNbThreads)
 __global__ void __launch_bounds__(kMaskListThreads)
     k_masks_list(const D4* __restrict__ bub, size_t n_int, size_t n_tot, const uint32_t* __restrict__ sel,
                  size_t n_sel, const NbList* __restrict__ lists, const D4* __restrict__ dirs, size_t nd,
-                 unsigned n_split, double* __restrict__ tau_out, int32_t* __restrict__ code_out,
+                 size_t row_len, unsigned n_split, double* __restrict__ tau_out, int32_t* __restrict__ code_out,
                  unsigned long long* __restrict__ counters) {
     // per listed collider: Delta = x_c - x_a and its Minkowski norm, computed once
     // per block with the reference's operations (direction independent)
@@ -355,22 +356,30 @@ __global__ void __launch_bounds__(kMaskListThreads)
     const int k = blockIdx.y;
     const size_t slot = blockIdx.x / n_split;
     const unsigned part = blockIdx.x % n_split;
-    const size_t chunks = (nd + 31) / 32;
-    const size_t c_begin = chunks * part / n_split, c_end = chunks * (part + 1) / n_split;
+    // the block's directions: whole rows [r_begin, r_end) of row_len directions (one cos-theta row)
+    const size_t n_rows = nd / row_len;
+    const size_t rpb = (n_rows + n_split - 1) / n_split;
+    const size_t r_begin = min(n_rows, rpb * part), r_end = min(n_rows, rpb * (part + 1));
+    const size_t d_begin = r_begin * row_len, d_end = r_end * row_len;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     constexpr int kWarps = kMaskListThreads / 32;
     constexpr int kBatch = 2;
+    constexpr int kRowsPerItem = 8;  // rows walked by a warp in one strip item
     const D4* B = bub + (size_t)k * n_tot;
     const uint32_t a = sel[slot];
     const NbList* L = lists + slot;
     const int n = L->count;
     __shared__ bool s_big;  // a listed Delta too large for the candidate filter's margin
-    if (threadIdx.x == 0) s_big = false;
+    __shared__ unsigned s_next;  // the block's work queue of strip items
+    if (threadIdx.x == 0) {
+        s_big = false;
+        s_next = 0;
+    }
     __syncthreads();
     double* tau_row = tau_out + ((size_t)k * n_sel + slot) * nd;
     int32_t* code_row = code_out ? code_out + ((size_t)k * n_sel + slot) * nd : nullptr;
     if (a >= n_int || n < 0) {  // invalid radiating bubble: sentinel outputs
-        for (size_t d = c_begin * 32 + threadIdx.x; d < min(c_end * 32, nd); d += kMaskListThreads) {
+        for (size_t d = d_begin + threadIdx.x; d < d_end; d += kMaskListThreads) {
             tau_row[d] = CUDART_NAN;
             if (code_row) code_row[d] = INT32_MIN;
         }
@@ -398,15 +407,31 @@ __global__ void __launch_bounds__(kMaskListThreads)
     const double kmax = L->kmax, rho1 = L->rho1, rho2 = L->rho2;
     const double u64 = 64.0 * 1.1102230246251565e-16;
     unsigned long long n_full = 0;
-
-    for (size_t ch = c_begin + warp; ch < c_end; ch += kWarps) {
-        // the whole warp takes the same chunks; the barrier at the end of each
-        // chunk reconverges lanes whose searches ended at different steps
+    // Work items: 32 consecutive directions of a row (a strip) over up to kRowsPerItem
+    // consecutive rows.  A lane walks its column down the rows; each result, when it came
+    // from the list, seeds the next row's candidate (the neighbouring patch in cos theta
+    // most often has the same first collider).  Warps take items from a shared counter.
+    const size_t n_strips = (row_len + 31) / 32;
+    const size_t n_groups = (r_end - r_begin + kRowsPerItem - 1) / kRowsPerItem;
+    const size_t n_items = n_strips * n_groups;
+    for (;;) {
+      unsigned item = 0;
+      if (lane == 0) item = atomicAdd(&s_next, 1u);
+      item = __shfl_sync(0xffffffffu, item, 0);
+      if (item >= n_items) break;
+      const size_t strip = item % n_strips, group = item / n_strips;
+      const size_t col = strip * 32 + lane;
+      int seed = -1;
+      for (int rr = 0; rr < kRowsPerItem; ++rr) {
+        const size_t rw = r_begin + group * kRowsPerItem + rr;
+        if (rw >= r_end) break;  // warp-uniform
+        // the barrier reconverges lanes whose searches ended at different steps
         __syncwarp();
-        const size_t d = min(ch * 32 + lane, nd - 1);
-        const bool live = ch * 32 + lane < nd;
+        const bool live = col < row_len;
+        const size_t d = rw * row_len + (live ? col : 0);
         const D4 x = dirs[d];
         long result = -1;
+        int res_pos = -1;      // list position of the result, when it came from the list
         double res_tau = 0.0;  // tau of the result when it came from the list (same operations)
         bool full = no < 0 || s_big;
 
@@ -483,7 +508,30 @@ __global__ void __launch_bounds__(kMaskListThreads)
             return tau * (1.0 + 1e-12) + u64 * (A * rho1 + Q * rho2) / dot;
         };
 
-        if (!full) {
+        // 0. the previous row's result at this column (the neighbouring patch in cos theta
+        //    most often has the same first collider): checked against every listed collider up
+        //    to its bound and the outliers, stopping at the first failure.  If it passes it is
+        //    the exact answer (the passer is unique); otherwise the direction takes steps 1-3.
+        bool seeded = false;
+        if (!full && seed >= 0) {
+            const D4 ds_ = s_pos[seed];
+            const double ds = mdot(ds_, x);
+            if (ds > 1e-10) {
+                const double ts = __ddiv_rn(s_nrm[seed], dmul(2.0, ds));
+                if (ts > 0.0) {
+                    const double th = theta_of(ds_, ts, ds);
+                    int dummy = 0;
+                    if (th < kmax && verify(s_idx[seed], ds_, s_nrm[seed], th, nullptr, dummy)) {
+                        result = s_idx[seed];
+                        res_pos = seed;
+                        res_tau = ts;
+                        seeded = true;
+                    }
+                }
+            }
+        }
+
+        if (!full && !seeded) {
             // 1. a candidate: the approximate argmin of tau = nrm / (2 dot) in key order
             //    (quotients compared by cross-multiplication), stopping once key exceeds
             //    the best quotient with a margin.  Any candidate serves: steps 2-3 decide
@@ -537,6 +585,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
                     int nfail = 0;
                     if (verify(s_idx[bi], dm, nm, th, fails, nfail)) {
                         result = s_idx[bi];
+                        res_pos = bi;
                         res_tau = best;
                     } else if (nfail > kMaxFail) {
                         full = true;
@@ -558,6 +607,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
                             int dummy = 0;
                             if (verify(s_idx[e], dc, nc, thf, nullptr, dummy)) {
                                 result = s_idx[e];
+                                res_pos = e;
                                 res_tau = tau;
                             }
                         }
@@ -593,19 +643,22 @@ __global__ void __launch_bounds__(kMaskListThreads)
                 code_row[d] =
                     result < 0 ? -1 : ((size_t)result < n_int ? (int32_t)result : -((int32_t)(result - n_int) + 2));
         }
+        seed = full ? -1 : res_pos;
+      }
     }
     if (n_full) atomicAdd(counters, n_full);
 }
 
-// Blocks per radiating bubble and frame: a few thousand directions per block
-// amortise the list gather; ranges shrink when there are too few blocks to
-// fill the GPU.
-static unsigned mask_split(size_t nd, size_t n_pairs) {
-    const size_t chunks = (nd + 31) / 32;
-    size_t split = (nd + 4095) / 4096;
+// Blocks per radiating bubble and frame: whole rows of about four thousand
+// directions per block amortise the list gather; ranges shrink (to one row at
+// least) when there are too few blocks to fill the GPU.
+static unsigned mask_split(size_t nd, size_t row_len, size_t n_pairs) {
+    const size_t n_rows = nd / row_len;
+    size_t rpb = std::max<size_t>(1, 4096 / row_len);
+    size_t split = (n_rows + rpb - 1) / rpb;
     const size_t want = 148 * 16;  // blocks for about four waves of resident blocks
-    while (split * n_pairs < want && split * 4 <= chunks) split *= 2;
-    if (split > chunks) split = chunks;
+    while (split * n_pairs < want && split * 2 <= n_rows) split *= 2;
+    if (split > n_rows) split = n_rows;
     return (unsigned)(split < 1 ? 1 : split);
 }
 
@@ -621,17 +674,20 @@ void launch_masks_with_lists(cudaStream_t stream, const D4* bub, size_t n_int, s
     if (n_sel > 0x7fffffffULL) throw Error{"too many radiating bubbles"};
     k_neighbors<<<(unsigned)n_sel, kNbThreads, 0, stream>>>(bub, n_int, n_tot, sel, lists);
     CUDA_OK(cudaGetLastError());
-    const unsigned n_split = mask_split(nd, n_sel);
+    // the directions' row structure is not known here: one row of nd directions
+    const unsigned n_split = mask_split(nd, nd, n_sel);
     const size_t gx = (size_t)n_split * n_sel;
     if (gx > 0x7fffffffULL) throw Error{"too many (bubble, patch) pairs for one launch"};
     k_masks_list<<<dim3((unsigned)gx, 1), kMaskListThreads, 0, stream>>>(bub, n_int, n_tot, sel, n_sel, lists, dirs,
-                                                                        nd, n_split, tau, codes, counters);
+                                                                        nd, nd, n_split, tau, codes, counters);
     CUDA_OK(cudaGetLastError());
 }
 
 void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames, size_t n_int, size_t n_tot,
-                          const uint32_t* sel, size_t n_sel, const D4* dirs, size_t nd, size_t kn, double* tau,
-                          int32_t* codes, unsigned long long* counters, bool build_lists, uint64_t* launches) {
+                          const uint32_t* sel, size_t n_sel, const D4* dirs, size_t nd, size_t row_len, size_t kn,
+                          double* tau, int32_t* codes, unsigned long long* counters, bool build_lists,
+                          uint64_t* launches) {
+    if (row_len == 0 || nd % row_len != 0) row_len = nd;
     if (n_tot < 2) {
         // a lone bubble has no collider: every direction is None
         CUDA_OK(cudaMemsetAsync(tau, 0, kn * n_sel * nd * sizeof(double), dev->stream));
@@ -646,12 +702,12 @@ void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames
         CUDA_OK(cudaGetLastError());
         if (launches) ++*launches;
     }
-    const unsigned n_split = mask_split(nd, n_sel * kn);
+    const unsigned n_split = mask_split(nd, row_len, n_sel * kn);
     const size_t gx = (size_t)n_split * n_sel;
     if (gx > 0x7fffffffULL || kn > 65535) throw Error{"too many (bubble, patch) pairs for one launch"};
     dim3 grid((unsigned)gx, (unsigned)kn);
     k_masks_list<<<grid, kMaskListThreads, 0, dev->stream>>>(bub_frames, n_int, n_tot, sel, n_sel,
-                                                             (const NbList*)dev->nblists.p, dirs, nd, n_split, tau,
+                                                             (const NbList*)dev->nblists.p, dirs, nd, row_len, n_split, tau,
                                                              codes, counters);
     CUDA_OK(cudaGetLastError());
     if (launches) ++*launches;

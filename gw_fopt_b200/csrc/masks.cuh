@@ -29,9 +29,11 @@ void launch_masks_with_lists(cudaStream_t stream, const D4* bub, size_t n_int, s
                              unsigned long long* counters);
 
 // Builds the lists (when build_lists) from the unrotated bubbles and runs the
-// list-based exact search for kn frames.  tau/codes: (kn, n_sel, nd).
+// list-based exact search for kn frames.  tau/codes: (kn, n_sel, nd); the
+// directions are rows of row_len (n_phi) consecutive patches.
 void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames, size_t n_int, size_t n_tot,
-                          const uint32_t* sel, size_t n_sel, const D4* dirs, size_t nd, size_t kn, double* tau,
-                          int32_t* codes, unsigned long long* counters, bool build_lists, uint64_t* launches);
+                          const uint32_t* sel, size_t n_sel, const D4* dirs, size_t nd, size_t row_len, size_t kn,
+                          double* tau, int32_t* codes, unsigned long long* counters, bool build_lists,
+                          uint64_t* launches);
 
 }  // namespace bgw

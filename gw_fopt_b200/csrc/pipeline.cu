@@ -581,7 +581,7 @@ void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_
     CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
     CUDA_OK(cudaEventRecord(dev->ev[0], dev->stream));
     uint64_t nl = 0;
-    launch_mask_pipeline(dev, bub, bub, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, 1, (double*)dev->tau.p,
+    launch_mask_pipeline(dev, bub, bub, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, job.n_phi, 1, (double*)dev->tau.p,
                          (int32_t*)dev->codes.p, (unsigned long long*)dev->counters.p, true, &nl);
     CUDA_OK(cudaEventRecord(dev->ev[1], dev->stream));
     CUDA_OK(cudaMemcpyAsync(out_codes, dev->codes.p, job.n_sel * nd * sizeof(int32_t), cudaMemcpyDeviceToHost,
@@ -604,7 +604,18 @@ void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_
     }
 }
 
-void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_device, BgwxTimings* tm) {
+// Error counters of a call: [0] mask fallbacks (u64), [1] non-zero when a
+// tensor-core pipeline wait gave up.
+static void check_counters(Device* dev, unsigned long long* fallbacks) {
+    unsigned long long cnt[2] = {0, 0};
+    CUDA_OK(cudaMemcpyAsync(cnt, dev->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, dev->stream));
+    CUDA_OK(cudaStreamSynchronize(dev->stream));
+    if (cnt[1] != 0) throw Error{"tensor-core GEMM: a pipeline wait gave up; the result is invalid"};
+    if (fallbacks) *fallbacks = cnt[0];
+}
+
+void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_device, BgwxTimings* tm,
+                  bool nested) {
     CUDA_OK(cudaSetDevice(dev->id));
     const size_t nd = job.n_cos * job.n_phi;
     const size_t S = job.n_sets, W = job.n_w, K = job.n_k;
@@ -653,8 +664,10 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
         dev->fact_ev.push_back(e);
     }
     if (rot) dev->bubrot.ensure(kc * job.n_tot * sizeof(D4));
-    dev->counters.ensure(64);
-    CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
+    if (!nested) {
+        dev->counters.ensure(64);
+        CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
+    }
 
     // shared memory of the direct kernel
     size_t smem_fixed = job.tensor ? (size_t)job.n_cos * 6 * sizeof(double) + (size_t)kSpecThreads * 6 * sizeof(double2)
@@ -684,7 +697,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             fb = (const D4*)dev->bubrot.p;
         }
         CUDA_OK(cudaEventRecord(cev[0], dev->stream));
-        launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, kn, (double*)dev->tau.p,
+        launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, job.n_phi, kn, (double*)dev->tau.p,
                              nullptr, (unsigned long long*)dev->counters.p, k0 == 0, &launches);
         CUDA_OK(cudaEventRecord(cev[1], dev->stream));
         if (job.kernel == BGWX_KERNEL_FP64_DIRECT) {
@@ -737,14 +750,12 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     CUDA_OK(cudaEventRecord(dev->ev[5], dev->stream));
     if (out_is_device) {
         if (tm) tm->launches += launches;
+        if (!nested) check_counters(dev, nullptr);
         return;
     }
     CUDA_OK(cudaMemcpyAsync(out, final_out, K * per * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
-    unsigned long long cnt[2] = {0, 0};
-    CUDA_OK(cudaMemcpyAsync(cnt, dev->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, dev->stream));
-    CUDA_OK(cudaStreamSynchronize(dev->stream));
-    const unsigned long long fbk = cnt[0];
-    if (cnt[1] != 0) throw Error{"tensor-core GEMM: a pipeline wait gave up; the result is invalid"};
+    unsigned long long fbk = 0;
+    check_counters(dev, &fbk);
     float total = 0, ms_masks = 0, ms_spec = 0;
     CUDA_OK(cudaEventElapsedTime(&total, dev->ev[4], dev->ev[5]));
     float ms_beta = 0, ms_gemm = 0;
@@ -789,14 +800,25 @@ void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out
         return jobs[a].n_sel * jobs[a].n_tot > jobs[b].n_sel * jobs[b].n_tot;
     });
     BgwxTimings local{};
+    dev->counters.ensure(64);
+    CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
     CUDA_OK(cudaEventRecord(dev->ev[6], dev->stream));
+    // every realization shares the (w, cos-theta, t) grid: the time-phase
+    // digits are built by the first call and reused by the others
+    struct Reuse {
+        Device* d;
+        explicit Reuse(Device* d_) : d(d_) { d->tc_key_reuse = false; }
+        void on() { d->tc_key_reuse = true; }
+        ~Reuse() { d->tc_key_reuse = false; }
+    } reuse(dev);
     for (size_t r : order) {
         if (jobs[r].n_sel == 0) continue;
-        run_spectrum(dev, jobs[r], reinterpret_cast<double*>(eo + r * per_r), true, &local);
+        run_spectrum(dev, jobs[r], reinterpret_cast<double*>(eo + r * per_r), true, &local, true);
+        reuse.on();
     }
     CUDA_OK(cudaEventRecord(dev->ev[7], dev->stream));
     CUDA_OK(cudaMemcpyAsync(out, eo, R * per_r * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
-    CUDA_OK(cudaStreamSynchronize(dev->stream));
+    check_counters(dev, nullptr);
     float total = 0;
     CUDA_OK(cudaEventElapsedTime(&total, dev->ev[6], dev->ev[7]));
     if (tm) {
@@ -836,13 +858,21 @@ void run_adjoint(Device* dev, const SpectrumJob& job, const double* gbar, double
     const size_t rows = job.n_sel * job.n_cos;
     dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
     dev->codes.ensure(kc * job.n_sel * nd * sizeof(int32_t));
-    dev->adj_scratch.ensure(kc * (2 * rows * job.n_t * 2 * S + job.n_sel * nd + rows * (2 + 2 * SM)) *
-                            sizeof(double));
+    // the fixed-point gradient sums of a chunk hold fewer than 2^31 contributions
+    const size_t per_frame_contrib = 2 * job.n_sel * nd + job.n_sel;
+    kc = std::max<size_t>(1, std::min(kc, ((size_t)1 << 31) / std::max<size_t>(per_frame_contrib, 1)));
+    if (per_frame_contrib >= ((size_t)1 << 31)) throw Error{"adjoint: too many (bubble, patch) pairs per frame"};
+    const size_t n_dbl = kc * (2 * rows * job.n_t * 2 * S + job.n_sel * nd + rows * (2 + 2 * SM) + job.n_sel * 4);
+    dev->adj_scratch.ensure(n_dbl * sizeof(double) + job.n_tot * 8 * sizeof(long long) + 64);
     AdjointScratch sc;
     sc.bbar = (double*)dev->adj_scratch.p;
     sc.imq = sc.bbar + kc * rows * job.n_t * 2 * S;
     sc.taubar = sc.imq + kc * rows * job.n_t * 2 * S;
     sc.rowpart = sc.taubar + kc * job.n_sel * nd;
+    sc.bubpart = sc.rowpart + kc * rows * (2 + 2 * SM);
+    sc.gfix = reinterpret_cast<long long*>(sc.bubpart + kc * job.n_sel * 4);
+    sc.gexp = reinterpret_cast<int*>(sc.gfix + job.n_tot * 8);
+    CUDA_OK(cudaMemsetAsync(sc.gfix, 0, job.n_tot * 8 * sizeof(long long), dev->stream));
     dev->adj_grad.ensure((4 * job.n_tot + 2 * SM) * sizeof(double));
     double* d_gbub = (double*)dev->adj_grad.p;
     double* d_gpar = d_gbub + 4 * job.n_tot;
@@ -868,7 +898,7 @@ void run_adjoint(Device* dev, const SpectrumJob& job, const double* gbar, double
             ++launches;
             fb = (const D4*)dev->bubrot.p;
         }
-        launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, kn, (double*)dev->tau.p,
+        launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, job.n_phi, kn, (double*)dev->tau.p,
                              (int32_t*)dev->codes.p, (unsigned long long*)dev->counters.p, k0 == 0, &launches);
         launches += launch_adjoint_chunk(dev, job, fb, sel, (const double*)dev->tau.p, (const int32_t*)dev->codes.p,
                                          dirs, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w,
@@ -945,7 +975,7 @@ void run_integrand(Device* dev, const SpectrumJob& job, double* out, BgwxTimings
         CUDA_OK(cudaFuncSetAttribute(k_tensor_direct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     uint64_t launches = 0;
     CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
-    launch_mask_pipeline(dev, bub, bub, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, 1, (double*)dev->tau.p,
+    launch_mask_pipeline(dev, bub, bub, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, job.n_phi, 1, (double*)dev->tau.p,
                          nullptr, (unsigned long long*)dev->counters.p, true, &launches);
     for (size_t s0 = 0; s0 < job.n_sel; s0 += chunk) {
         const size_t n = std::min(chunk, job.n_sel - s0);

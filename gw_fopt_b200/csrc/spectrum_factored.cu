@@ -112,8 +112,8 @@ struct BetaArgs {
     int bpt;               // bubbles per tile
     int t_pad;             // row length of beta
     int per_warp_bytes;
-    int tc_layout;         // beta as pre-split, pre-swizzled blocks of the tensor-core GEMM (Real = float)
-    int tiles;             // column tiles per frame (tc_layout)
+    int tiles;             // column tiles per frame (int8 digit layout)
+    double* scale;         // int8 digit layout: (kn, n_sel, n_cos) row scales, max |beta| of the row
 };
 
 // x^p: binary powering for integral |p| <= 32 (a few ulp), pow() otherwise.
@@ -130,16 +130,6 @@ __device__ __forceinline__ double tpow(double x, double p) {
         return r < 0.0 ? 1.0 / acc : acc;
     }
     return pow(x, p);
-}
-
-// One beta value into the tensor-core GEMM's block layout: the hi and lo TF32
-// parts at (column n, step kk) of the block pair at `blk`.
-__device__ __forceinline__ void tc_store(float* blk, int n, int kk, float x) {
-    uint32_t hi, lo;
-    tc::split_tf32_fast(x, hi, lo);
-    const size_t o = tc_swz(n, kk);
-    blk[o] = __uint_as_float(hi);
-    blk[kTcBlockFloats + o] = __uint_as_float(lo);
 }
 
 template <class Real, int SMC>
@@ -349,18 +339,22 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
     // offsets are compared four at a time as bytes), then warp scans give the
     // collided sums up to and the uncollided sums after every step.  Blocks
     // without events have constant sums: each lane forms 4 consecutive steps,
-    // 8 lanes a block, 4 such blocks at a time.
+    // 8 lanes a block, 4 such blocks at a time (int8 digits: 16 steps, 2 lanes
+    // a block, 16 blocks at a time).  The int8 digit layout needs the row's
+    // scale, max |beta| over its steps and columns, before any digit: a first
+    // sweep forms every value and keeps only the maximum.
+    constexpr bool kI8 = std::is_same<Real, int8_t>::value;
     const double ci = A.cos_t[i];
     const double vi = (i == 0 || i == A.n_cos - 1) ? 0.5 : 1.0;
     const double rf = (0.5 * (1.0 - ci * ci) * A.dphi) * (A.dcos * vi) * A.dt * (1.0 / (6.0 * CUDART_PI));
     const long col = (long)(slot / A.bpt) * A.tile_cols + (long)(slot % A.bpt) * 2 * A.S;
-    Real* brow = beta + (((size_t)frame * A.n_cos + i) * A.cols_pad + col) * A.t_pad;
+    Real* brow = kI8 ? nullptr : beta + (((size_t)frame * A.n_cos + i) * A.cols_pad + col) * A.t_pad;
     const double* Dslot = A.D + (size_t)slot * A.n_t * (1 + SMC);
     const int nbase = (slot % A.bpt) * 2 * A.S;
-    float* blk_row = A.tc_layout ? reinterpret_cast<float*>(beta) +
-                                       (((size_t)frame * A.n_cos + i) * A.tiles + slot / A.bpt) * NB * 2 *
-                                           kTcBlockFloats
-                                 : nullptr;
+    int8_t* blk_row =
+        kI8 ? reinterpret_cast<int8_t*>(beta) +
+                  (((size_t)frame * A.n_cos + i) * A.tiles + slot / A.bpt) * (size_t)NB * kI8BlockSet
+            : nullptr;
     // beta of coefficient set s at step k from the sums there: the table row
     // holds the step weight times dt^3 and times a_m dt^{3-p_m} e^{-dt/w}
     auto value = [&](int k, int s, const double* P, double Uc, double Us, double& xc, double& xs) {
@@ -388,130 +382,170 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         xc = r * vc;
         xs = r * vs;
     };
-    for (int bc = 0; bc < NB; bc += 32) {
-        const int bl = bc + lane;
-        const bool has = bl < NB && boff[bl] != boff[bl + 1];
-        const unsigned ev_blocks = __ballot_sync(full, has);
-        unsigned quiet = __ballot_sync(full, bl < NB && !has);
-        // ---- event blocks, lane = step
-        for (unsigned h = ev_blocks; h; h &= h - 1) {
-            const int b = bc + __ffs(h) - 1;
-            const int e0 = boff[b], e1 = boff[b + 1];
-            double dq[NQ];
+    // Collided sums through step (b << 5) + lane and uncollided sums after it, for
+    // block b, lane = step (the whole warp calls it with the same b).
+    auto step_sums = [&](int b, double (&P)[2 * SMC], double& Uc, double& Us) {
+        const int e0 = boff[b], e1 = boff[b + 1];
+        if (e0 == e1) {  // a block without events: constant sums
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) dq[q] = 0.0;
-            if (NB >= 32 && e1 - e0 > 32) {
-                // Many events: lanes take 32 events at a time; the events of one step
-                // (a __match_any group) are added by the group's lowest lane in event
-                // order and the group sum is added to that step's row of a table in the
-                // (by now unused) block-total array, rounds in event order.
-                double* D = btot;  // [NQ][32 steps]
+            for (int q = 0; q < 2 * SMC; ++q) P[q] = pbeg[(size_t)b * 2 * SMC + q];
+            Uc = uend[2 * b];
+            Us = uend[2 * b + 1];
+            return;
+        }
+        double dq[NQ];
 #pragma unroll
-                for (int q = 0; q < NQ; ++q) D[q * 32 + lane] = 0.0;
-                __syncwarp();
-                for (int r0 = e0; r0 < e1; r0 += 32) {
-                    const int e = r0 + lane;
-                    const bool valid = e < e1;
-                    const int se = valid ? (int)evs[e] : 32 + lane;
-                    const unsigned m = __match_any_sync(full, se);
-                    if (valid && lane == __ffs(m) - 1) {
-                        double g[NQ];
+        for (int q = 0; q < NQ; ++q) dq[q] = 0.0;
+        if (NB >= 32 && e1 - e0 > 32) {
+            // Many events: lanes take 32 events at a time; the events of one step
+            // (a __match_any group) are added by the group's lowest lane in event
+            // order and the group sum is added to that step's row of a table in the
+            // (by now unused) block-total array, rounds in event order.
+            double* D = btot;  // [NQ][32 steps]
 #pragma unroll
-                        for (int q = 0; q < NQ; ++q) g[q] = 0.0;
-                        for (unsigned mm = m; mm; mm &= mm - 1) {
-                            const double* qe = evq + (r0 + __ffs(mm) - 1);
+            for (int q = 0; q < NQ; ++q) D[q * 32 + lane] = 0.0;
+            __syncwarp();
+            for (int r0 = e0; r0 < e1; r0 += 32) {
+                const int e = r0 + lane;
+                const bool valid = e < e1;
+                const int se = valid ? (int)evs[e] : 32 + lane;
+                const unsigned m = __match_any_sync(full, se);
+                if (valid && lane == __ffs(m) - 1) {
+                    double g[NQ];
 #pragma unroll
-                            for (int q = 0; q < NQ; ++q) g[q] += qe[(size_t)q * EV];
-                        }
+                    for (int q = 0; q < NQ; ++q) g[q] = 0.0;
+                    for (unsigned mm = m; mm; mm &= mm - 1) {
+                        const double* qe = evq + (r0 + __ffs(mm) - 1);
 #pragma unroll
-                        for (int q = 0; q < NQ; ++q) D[q * 32 + se] += g[q];
+                        for (int q = 0; q < NQ; ++q) g[q] += qe[(size_t)q * EV];
                     }
-                    __syncwarp();
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) D[q * 32 + se] += g[q];
                 }
-#pragma unroll
-                for (int q = 0; q < NQ; ++q) dq[q] = D[q * 32 + lane];
                 __syncwarp();
-            } else {
-                const uint32_t pat = 0x01010101u * (uint32_t)lane;
-                for (int e4 = e0 & ~3; e4 < e1; e4 += 4) {
-                    uint32_t eq = __vcmpeq4(*reinterpret_cast<const uint32_t*>(evs + e4), pat);
-                    if (e4 < e0) eq &= 0xffffffffu << (8 * (e0 - e4));
-                    if (e1 - e4 < 4) eq &= (1u << (8 * (e1 - e4))) - 1u;
-                    while (eq) {
-                        const int by = (__ffs(eq) - 1) >> 3;
-                        eq &= ~(0xffu << (8 * by));
-                        const double* qe = evq + (e4 + by);
+            }
 #pragma unroll
-                        for (int q = 0; q < NQ; ++q) dq[q] += qe[(size_t)q * EV];
-                    }
+            for (int q = 0; q < NQ; ++q) dq[q] = D[q * 32 + lane];
+            __syncwarp();
+        } else {
+            const uint32_t pat = 0x01010101u * (uint32_t)lane;
+            for (int e4 = e0 & ~3; e4 < e1; e4 += 4) {
+                uint32_t eq = __vcmpeq4(*reinterpret_cast<const uint32_t*>(evs + e4), pat);
+                if (e4 < e0) eq &= 0xffffffffu << (8 * (e0 - e4));
+                if (e1 - e4 < 4) eq &= (1u << (8 * (e1 - e4))) - 1u;
+                while (eq) {
+                    const int by = (__ffs(eq) - 1) >> 3;
+                    eq &= ~(0xffu << (8 * by));
+                    const double* qe = evq + (e4 + by);
+#pragma unroll
+                    for (int q = 0; q < NQ; ++q) dq[q] += qe[(size_t)q * EV];
                 }
             }
-            // collided sums through this step (inclusive scan), uncollided after it (suffix scan)
-            double P[2 * SMC], uc = dq[0], us = dq[1];
+        }
+        // collided sums through this step (inclusive scan), uncollided after it (suffix scan)
+        double uc = dq[0], us = dq[1];
 #pragma unroll
-            for (int q = 0; q < 2 * SMC; ++q) P[q] = dq[2 + q];
+        for (int q = 0; q < 2 * SMC; ++q) P[q] = dq[2 + q];
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
+        for (int o = 1; o < 32; o <<= 1) {
 #pragma unroll
-                for (int q = 0; q < 2 * SMC; ++q) {
-                    const double v = __shfl_up_sync(full, P[q], o);
-                    if (lane >= o) P[q] += v;
-                }
-                const double vc = __shfl_down_sync(full, uc, o), vs = __shfl_down_sync(full, us, o);
-                if (lane + o < 32) {
-                    uc += vc;
-                    us += vs;
-                }
+            for (int q = 0; q < 2 * SMC; ++q) {
+                const double v = __shfl_up_sync(full, P[q], o);
+                if (lane >= o) P[q] += v;
             }
-            // uncollided after this step: the next step's inclusive suffix sum
-            double Uc = __shfl_down_sync(full, uc, 1), Us = __shfl_down_sync(full, us, 1);
-            if (lane == 31) Uc = Us = 0.0;
-            Uc += uend[2 * b];
-            Us += uend[2 * b + 1];
+            const double vc = __shfl_down_sync(full, uc, o), vs = __shfl_down_sync(full, us, o);
+            if (lane + o < 32) {
+                uc += vc;
+                us += vs;
+            }
+        }
+        // uncollided after this step: the next step's inclusive suffix sum
+        Uc = __shfl_down_sync(full, uc, 1);
+        Us = __shfl_down_sync(full, us, 1);
+        if (lane == 31) Uc = Us = 0.0;
+        Uc += uend[2 * b];
+        Us += uend[2 * b + 1];
 #pragma unroll
-            for (int q = 0; q < 2 * SMC; ++q) P[q] = pbeg[(size_t)b * 2 * SMC + q] + P[q];
+        for (int q = 0; q < 2 * SMC; ++q) P[q] = pbeg[(size_t)b * 2 * SMC + q] + P[q];
+    };
+    if constexpr (kI8) {
+        // lane = step for every block.  Sweep 0: the row's scale, max |beta|.  Sweep 1: the
+        // digits.  A quad of lanes (4 steps) transposes its four packed digit words so that
+        // lane 4q + d holds digit d of steps 4q .. 4q + 3; one store instruction then fills
+        // 32 contiguous bytes of each of the four digit blocks.
+        double vmax = 0.0;
+        for (int b = 0; b < NB; ++b) {
+            double P[2 * SMC], Uc, Us;
+            step_sums(b, P, Uc, Us);
             const int k = (b << 5) + lane;
             for (int s2 = 0; s2 < A.S; ++s2) {
                 double xc, xs;
                 value(k, s2, P, Uc, Us, xc, xs);
-                if (A.tc_layout) {
-                    float* blk = blk_row + (size_t)b * 2 * kTcBlockFloats;
-                    tc_store(blk, nbase + 2 * s2, lane, (float)(Real)xc);
-                    tc_store(blk, nbase + 2 * s2 + 1, lane, (float)(Real)xs);
-                } else if (k < A.t_pad) {
-                    brow[(size_t)(2 * s2) * A.t_pad + k] = (Real)xc;
-                    brow[(size_t)(2 * s2 + 1) * A.t_pad + k] = (Real)xs;
-                }
+                vmax = fmax(vmax, fmax(fabs(xc), fabs(xs)));
             }
         }
-        // ---- blocks without events, 4 steps per lane
-        const int sub = lane >> 3, s0 = (lane & 7) * 4;
-        while (quiet) {
-            unsigned t = quiet;
-            for (int g = 0; g < sub && t; ++g) t &= t - 1;
-            const int b = t ? bc + __ffs(t) - 1 : -1;
-            for (int g = 0; g < 4 && quiet; ++g) quiet &= quiet - 1;
-            if (b < 0) continue;
-            const double* P = pbeg + (size_t)b * 2 * SMC;
-            const double Uc = uend[2 * b], Us = uend[2 * b + 1];
-            const int k0 = (b << 5) + s0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(full, vmax, o));
+        if (lane == 0) A.scale[row] = vmax;
+        const double inv = vmax > 0.0 ? 1.0 / vmax : 0.0;
+        const bool odd = lane & 1, hi = lane & 2;
+        auto quad_transpose = [&](uint32_t p) {
+            const uint32_t t1 = __shfl_xor_sync(full, p, 1);
+            p = __byte_perm(p, t1, odd ? 0x3715 : 0x6240);
+            const uint32_t t2 = __shfl_xor_sync(full, p, 2);
+            return __byte_perm(p, t2, hi ? 0x3276 : 0x5410);
+        };
+        const int dg = lane & 3, s4 = (lane >> 2) * 4;
+        for (int b = 0; b < NB; ++b) {
+            double P[2 * SMC], Uc, Us;
+            step_sums(b, P, Uc, Us);
+            const int k = (b << 5) + lane;
+            int8_t* blk = blk_row + (size_t)b * kI8BlockSet + dg * kI8Block;
             for (int s2 = 0; s2 < A.S; ++s2) {
-                double xc[4], xs[4];
-#pragma unroll
-                for (int m = 0; m < 4; ++m) value(k0 + m, s2, P, Uc, Us, xc[m], xs[m]);
-                if (A.tc_layout) {
-                    float* blk = blk_row + (size_t)b * 2 * kTcBlockFloats;
-#pragma unroll
-                    for (int g = 0; g < 2; ++g) {
-                        const int n = nbase + 2 * s2 + g;
-                        uint32_t h[4], l[4];
-#pragma unroll
-                        for (int m = 0; m < 4; ++m) tc::split_tf32_fast((float)(Real)(g ? xs[m] : xc[m]), h[m], l[m]);
-                        const size_t o = tc_swz(n, s0);
-                        *reinterpret_cast<uint4*>(blk + o) = make_uint4(h[0], h[1], h[2], h[3]);
-                        *reinterpret_cast<uint4*>(blk + kTcBlockFloats + o) = make_uint4(l[0], l[1], l[2], l[3]);
+                double xc, xs;
+                value(k, s2, P, Uc, Us, xc, xs);
+                const uint32_t wc = quad_transpose(i8_digits(xc * inv));
+                const uint32_t ws = quad_transpose(i8_digits(xs * inv));
+                *reinterpret_cast<uint32_t*>(blk + i8_swz(nbase + 2 * s2, s4)) = wc;
+                *reinterpret_cast<uint32_t*>(blk + i8_swz(nbase + 2 * s2 + 1, s4)) = ws;
+            }
+        }
+    } else {
+        for (int bc = 0; bc < NB; bc += 32) {
+            const int bl = bc + lane;
+            const bool has = bl < NB && boff[bl] != boff[bl + 1];
+            const unsigned ev_blocks = __ballot_sync(full, has);
+            unsigned quiet = __ballot_sync(full, bl < NB && !has);
+            // ---- event blocks, lane = step
+            for (unsigned h = ev_blocks; h; h &= h - 1) {
+                const int b = bc + __ffs(h) - 1;
+                double P[2 * SMC], Uc, Us;
+                step_sums(b, P, Uc, Us);
+                const int k = (b << 5) + lane;
+                for (int s2 = 0; s2 < A.S; ++s2) {
+                    double xc, xs;
+                    value(k, s2, P, Uc, Us, xc, xs);
+                    if (k < A.t_pad) {
+                        brow[(size_t)(2 * s2) * A.t_pad + k] = (Real)xc;
+                        brow[(size_t)(2 * s2 + 1) * A.t_pad + k] = (Real)xs;
                     }
-                } else {
+                }
+            }
+            // ---- blocks without events, 4 steps per lane
+            const int sub = lane >> 3, s0 = (lane & 7) * 4;
+            while (quiet) {
+                unsigned t = quiet;
+                for (int g = 0; g < sub && t; ++g) t &= t - 1;
+                const int b = t ? bc + __ffs(t) - 1 : -1;
+                for (int g = 0; g < 4 && quiet; ++g) quiet &= quiet - 1;
+                if (b < 0) continue;
+                const double* P = pbeg + (size_t)b * 2 * SMC;
+                const double Uc = uend[2 * b], Us = uend[2 * b + 1];
+                const int k0 = (b << 5) + s0;
+                for (int s2 = 0; s2 < A.S; ++s2) {
+                    double xc[4], xs[4];
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) value(k0 + m, s2, P, Uc, Us, xc[m], xs[m]);
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
                         const int k = k0 + m;
@@ -838,10 +872,11 @@ struct FactGeom {
     long cols_pad;
 };
 
+// real_size: 8 (FP64 GEMM, 64-column tiles), 4 (FP32 GEMM) or 1 (int8 tensor-core GEMM), 128-column tiles
 static FactGeom fact_geom(const SpectrumJob& job, size_t real_size) {
     FactGeom g;
     const int S = (int)job.n_sets;
-    const int cols = 16 * (real_size == 4 ? 8 : 4);
+    const int cols = real_size == 8 ? 64 : 128;
     g.tile_cols = cols;
     g.bpt = std::min(64, cols / (2 * S));
     g.tiles_per_frame = (int)((job.n_sel + g.bpt - 1) / g.bpt);
@@ -860,7 +895,8 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     const int S = (int)job.n_sets, M = (int)job.n_terms, SM = S * M;
     const int n_t = (int)job.n_t, n_cos = (int)job.n_cos, n_phi = (int)job.n_phi, n_w = (int)job.n_w;
     const int n_sel = (int)job.n_sel;
-    if (SM > 8 || 2 * S > 16 * gemm_tn<Real>())
+    constexpr bool tc = std::is_same<Real, int8_t>::value;
+    if (SM > 8 || 2 * S > (sizeof(Real) == 8 ? 64 : 128))
         throw Error{"the factored kernels support at most 8 (set, term) pairs; use the fp64_direct kernel"};
     if (job.has_damping) {
         const double span = job.t_arr[job.n_t - 1] - job.t_arr[0] + 4.0;
@@ -883,10 +919,10 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     }
     // beta
     CUDA_OK(cudaEventRecord(ev3[0], dev->stream));
-    const bool tc = sizeof(Real) == 4 && job.kernel == BGWX_KERNEL_MIXED;
     const int nkb = G.nblk;
-    const size_t beta_elems = tc ? (size_t)kn * n_cos * G.tiles_per_frame * nkb * 2 * kTcBlockFloats
+    const size_t beta_elems = tc ? (size_t)kn * n_cos * G.tiles_per_frame * nkb * kI8BlockSet
                                  : (size_t)kn * n_cos * G.cols_pad * G.t_pad;
+    if (tc) dev->beta_scale.ensure((size_t)kn * n_sel * n_cos * sizeof(double));
     dev->beta.ensure(beta_elems * sizeof(Real));
     if ((long)n_sel * 2 * S != G.cols_pad) {  // unused tile columns must read as zero
         // padding columns of the last tile are read by the GEMM: keep them zero
@@ -927,8 +963,8 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
                     (2 * (size_t)G.nblk + 1) * sizeof(int) + ((size_t)n_phi + 4);
         pw = (pw + 15) & ~(size_t)15;
         B.per_warp_bytes = (int)pw;
-        B.tc_layout = tc ? 1 : 0;
         B.tiles = G.tiles_per_frame;
+        B.scale = tc ? (double*)dev->beta_scale.p : nullptr;
         int warps = (int)std::min<size_t>(8, (200 * 1024) / pw);
         if (warps < 1) throw Error{"n_phi too large for the beta kernel"};
         const size_t smem = (size_t)warps * pw;
@@ -968,10 +1004,11 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     dev->last_row_parts = row_parts;
     dev->fact_partial.ensure((size_t)kn * G.tiles_per_frame * row_parts * per * sizeof(double2));
     A.partial = (double2*)dev->fact_partial.p;
-    if (tc) {
-        // time-phase table: frame independent, rebuilt only when w, cos-theta or t change
+    if constexpr (tc) {
+        // time-phase digits: frame independent; rebuilt on every call unless the
+        // caller (the batched ensemble) runs several calls on one grid
         const int n_wt = (n_w + 63) / 64;
-        const size_t atab_floats = (size_t)n_cos * n_wt * nkb * 2 * kTcBlockFloats;
+        const size_t atab_bytes = (size_t)n_cos * n_wt * nkb * kI8BlockSet;
         std::vector<double> key;
         key.reserve(3 + n_w + n_cos + n_t);
         key.push_back((double)n_w);
@@ -980,10 +1017,10 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         key.insert(key.end(), job.w, job.w + n_w);
         key.insert(key.end(), job.cos_thetax, job.cos_thetax + n_cos);
         key.insert(key.end(), job.t_arr, job.t_arr + n_t);
-        const bool had = dev->tc_atab.p && dev->tc_atab.cap >= atab_floats * sizeof(float);
-        dev->tc_atab.ensure(atab_floats * sizeof(float));
-        if (!had || dev->tc_key != key) {
-            launch_tc_phase_table(w, cos_t, t_arr, n_cos, n_w, n_t, (float*)dev->tc_atab.p, dev->stream);
+        const bool had = dev->tc_atab.p && dev->tc_atab.cap >= atab_bytes;
+        dev->tc_atab.ensure(atab_bytes);
+        if (!had || !dev->tc_key_reuse || dev->tc_key != key) {
+            launch_tc_phase_table(w, cos_t, t_arr, n_cos, n_w, n_t, (int8_t*)dev->tc_atab.p, dev->stream);
             ++launches;
             dev->tc_key = key;
         }
@@ -999,8 +1036,9 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         T.w = w;
         T.cos_t = cos_t;
         T.kfirst = (const int*)dev->fact_kfirst.p;
-        T.atab = (const float*)dev->tc_atab.p;
-        T.btab = (const float*)dev->beta.p;
+        T.atab = (const int8_t*)dev->tc_atab.p;
+        T.btab = (const int8_t*)dev->beta.p;
+        T.bscale = (const double*)dev->beta_scale.p;
         T.n_wt = n_wt;
         T.nkb = nkb;
         T.bpt = G.bpt;
@@ -1016,30 +1054,34 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         CUDA_OK(cudaGetLastError());
         ++launches;
         return launches;
+    } else {
+        constexpr int TN = gemm_tn<Real>();
+        const size_t smem = gemm_smem_bytes<Real, TN>(S);
+        if (smem > 227 * 1024) throw Error{"too many coefficient sets for the factored kernel's shared memory"};
+        CUDA_OK(cudaFuncSetAttribute(k_gemm<Real, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        const size_t gy = (size_t)kn * G.tiles_per_frame;
+        if (gy > 65535) throw Error{"too many column tiles in one k-hat chunk"};
+        dim3 grid((unsigned)((n_w + kWT - 1) / kWT), (unsigned)gy);
+        k_gemm<Real, TN><<<grid, kThreads, smem, dev->stream>>>(A);
+        CUDA_OK(cudaGetLastError());
+        ++launches;
+        CUDA_OK(cudaEventRecord(ev3[2], dev->stream));
+        dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
+        k_reduce_tiles<<<gr, 256, 0, dev->stream>>>(A.partial, G.tiles_per_frame, per, (int)kn, out);
+        CUDA_OK(cudaGetLastError());
+        ++launches;
+        return launches;
     }
-    constexpr int TN = gemm_tn<Real>();
-    const size_t smem = gemm_smem_bytes<Real, TN>(S);
-    if (smem > 227 * 1024) throw Error{"too many coefficient sets for the factored kernel's shared memory"};
-    CUDA_OK(cudaFuncSetAttribute(k_gemm<Real, TN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    const size_t gy = (size_t)kn * G.tiles_per_frame;
-    if (gy > 65535) throw Error{"too many column tiles in one k-hat chunk"};
-    dim3 grid((unsigned)((n_w + kWT - 1) / kWT), (unsigned)gy);
-    k_gemm<Real, TN><<<grid, kThreads, smem, dev->stream>>>(A);
-    CUDA_OK(cudaGetLastError());
-    ++launches;
-    CUDA_OK(cudaEventRecord(ev3[2], dev->stream));
-    dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
-    k_reduce_tiles<<<gr, 256, 0, dev->stream>>>(A.partial, G.tiles_per_frame, per, (int)kn, out);
-    CUDA_OK(cudaGetLastError());
-    ++launches;
-    return launches;
 }
 
 uint64_t launch_factored(Device* dev, const SpectrumJob& job, const D4* bub_frames, const uint32_t* sel,
                          const double* tau, const double* cos_t, const double* sin2, const double* cos2,
                          const double* coeffs, const double* powers, const double* t_arr, const double* cutw,
                          const double* w, size_t kn, double2* out, cudaEvent_t* ev3) {
-    if (job.kernel == BGWX_KERNEL_MIXED || job.kernel == BGWX_KERNEL_MIXED_SIMT)
+    if (job.kernel == BGWX_KERNEL_MIXED)
+        return launch_typed<int8_t>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w,
+                                    kn, out, ev3);
+    if (job.kernel == BGWX_KERNEL_MIXED_SIMT)
         return launch_typed<float>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w,
                                    kn, out, ev3);
     return launch_typed<double>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, kn,
@@ -1048,16 +1090,19 @@ uint64_t launch_factored(Device* dev, const SpectrumJob& job, const D4* bub_fram
 
 int factored_auto_row_parts(const Device* dev, const SpectrumJob& job, size_t kn) {
     if (job.kernel != BGWX_KERNEL_MIXED) return 1;
-    const FactGeom G = fact_geom(job, sizeof(float));
+    const FactGeom G = fact_geom(job, 1);
     return tc_row_parts((size_t)((job.n_w + 63) / 64) * kn * G.tiles_per_frame, (int)job.n_cos, dev->n_sm);
 }
 
 size_t factored_bytes_per_frame(const SpectrumJob& job) {
-    const size_t real =
-        (job.kernel == BGWX_KERNEL_MIXED || job.kernel == BGWX_KERNEL_MIXED_SIMT) ? sizeof(float) : sizeof(double);
+    const size_t real = job.kernel == BGWX_KERNEL_MIXED        ? 1
+                        : job.kernel == BGWX_KERNEL_MIXED_SIMT ? sizeof(float)
+                                                               : sizeof(double);
     const FactGeom G = fact_geom(job, real);
+    // int8 tensor-core path: the digit block sets and one FP64 scale per (bubble, row)
     const size_t beta = job.kernel == BGWX_KERNEL_MIXED
-                            ? (size_t)job.n_cos * G.tiles_per_frame * G.nblk * 2 * kTcBlockFloats * sizeof(float)
+                            ? (size_t)job.n_cos * G.tiles_per_frame * G.nblk * kI8BlockSet +
+                                  (size_t)job.n_sel * job.n_cos * sizeof(double)
                             : (size_t)job.n_cos * G.cols_pad * G.t_pad * real;
     // partials: up to 16 row parts per column tile on the tensor-core path
     const size_t parts = job.kernel == BGWX_KERNEL_MIXED ? 16 : 1;

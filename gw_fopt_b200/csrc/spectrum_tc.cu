@@ -1,38 +1,48 @@
-// Mixed-precision time-phase GEMM on the 5th-generation tensor cores.
+// Mixed-precision time-phase GEMM on the 5th-generation tensor cores, as an
+// exact integer product of digit slices.
 //
 // For each cos-theta row i the factored spectrum needs Y_i = M_i beta_i with
 // M_i[w, k] = e^{i w (1 - c_i) t_k} (rows: Re and Im of 64 frequencies) and
 // beta_i[k, col] (columns: bubble x set x {+, x}); the epilogue applies
 // e^{i w (t_a c_i - z_a)} per (w, bubble) and sums over the tile's bubbles
-// (spectrum_factored.cu holds the derivation).  Here the product runs as
-// tcgen05.mma kind::tf32 with FP32 accumulation in tensor memory, each FP32
-// operand split into two TF32 parts, x = x_hi + x_lo, and three products
-// A_hi B_lo + A_lo B_hi + A_hi B_hi per K step (the A_lo B_lo term is below
-// FP32 rounding), which keeps FP32-level operand accuracy.
+// (spectrum_factored.cu holds the derivation).
+//
+// Both operands are written as four signed 8-bit digits (spectrum_tc.cuh):
+// M = (m0 + m1/254 + m2/254^2 + m3/254^3)/127 and beta = s_a (b0 + ... )/127,
+// with one scale s_a per (frame, bubble, row) = max |beta| over the row's steps
+// and columns.  The product keeps the ten digit pairs (p, q) with p + q <= 3
+// (0-based); the pairs of one level L = p + q share the weight 254^-L, so
+//   Y = s_a / 127^2  sum_L 254^-L D_L,   D_L = sum_k sum_{p+q=L} m_p b_q,
+// and each D_L is accumulated EXACTLY by tcgen05.mma kind::i8 in a 32-bit
+// integer accumulator of tensor memory (|D_L| <= 4 * 127^2 * n_t < 2^31 for
+// n_t <= 32768).  The error is the digit truncation, about 2^-32 of the
+// operands' scales per term, against 2^-24 for FP32 operands; there is no
+// rounding in the accumulation at all, so the accumulators run over a whole
+// row of time steps and are read once per row.
 //
 // Both operands arrive pre-split and pre-swizzled from HBM: the time phases
-// from a per-call table (k_tc_phase_table, frame and bubble independent), beta
-// from k_beta, in 16 KB blocks of 128 rows x 32 steps.  One thread streams the
-// blocks of a 32-step stage into shared memory with bulk copies that complete
-// on the stage's mbarrier (transaction bytes); one thread issues the MMAs with
-// both operands in shared memory.
+// from a per-call table (k_tc_phase_table, FP64 sincos, frame and bubble
+// independent), beta from k_beta, as sets of four 4 KB digit blocks of 128
+// rows x 32 steps.  One thread streams each 32-step stage (A digits, B digits:
+// 32 KB) into shared memory with two bulk copies that complete on the stage's
+// mbarrier (transaction bytes); one thread issues the ten MMAs per stage.
 //
-// One CTA per (64-frequency tile, 128-column tile), looping over the rows i;
-// per row the K dimension is the time steps from the tile's first active
-// block of 32 steps on.  Warp roles (10 warps):
+// One CTA per (64-frequency tile, 128-column tile, range of cos-theta rows);
+// per row the K dimension is the time steps from the tile's first active block
+// of 32 steps on.  Warp roles (10 warps):
 //   0     bulk-copy producer (one thread)
 //   1     MMA issue (one thread) and tensor-memory allocation
 //   2-9   epilogue, two warpgroups of 64 columns each: thread = tensor-memory
-//         lane.  Per row the phases e^{i w (t_a c_i - z_a)} (FP64 argument
-//         reduction, FP32 sincos) go to a shared-memory table; every block of
-//         32 steps the accumulator (tcgen05.ld) is multiplied by them and
-//         summed per (w, set, +/x) in FP64.
-// Stages: 3 x 64 KB (A hi/lo, B hi/lo); the FP32 accumulator is double-
-// buffered in tensor memory across blocks of 32 steps.  Every wait is bounded:
-// on a timeout the block records an error flag, tells the other roles to stop,
-// waits for its issued MMAs and copies to finish and frees its tensor memory.
-//
-// Tensor memory: 256 columns, accumulators at columns 0 and 128.
+//         lane.  While a row's MMAs run, each warp fills its part of the FP64
+//         table s_a/127^2 e^{i w (t_a c_i - z_a)} (64 w x 64 bubbles, shared
+//         memory); when the row's accumulators are complete it reads the four
+//         levels (tcgen05.ld), combines them (level 0 in FP64, levels 1-3 in
+//         FP32, whose rounding lies below the truncation) and adds
+//         phase x value to FP64 sums per (w, set, +/x).
+// Stages: 4 x 32 KB.  Tensor memory: 512 columns, level L at columns 128 L.
+// Every wait is bounded: on a timeout the block records an error flag, tells
+// the other roles to stop, waits for its issued MMAs and copies to finish and
+// frees its tensor memory.
 
 #include <cuda_runtime.h>
 
@@ -55,62 +65,97 @@ namespace {
 constexpr int kTcRows = 128;     // GEMM rows: 64 frequencies x (Re, Im)
 constexpr int kTcWT = 64;        // frequencies per CTA
 constexpr int kTcCols = 128;     // GEMM columns per CTA
-constexpr int kTcKB = 32;        // time steps per stage (128 bytes of TF32)
-constexpr int kTcStages = 3;
-constexpr int kTcFoldKB = 1;     // blocks of 32 steps accumulated in tensor memory before the FP64 fold
+constexpr int kTcKB = 32;        // time steps per stage (32 bytes of int8)
+constexpr int kTcStages = 4;
 constexpr int kTcWarps = 10;
 constexpr int kTcThreads = 32 * kTcWarps;
-constexpr uint32_t kTmemCols = 256;
-constexpr int kBlockBytes = kTcBlockFloats * 4;   // 16 KB
-constexpr int kStageBytes = 4 * kBlockBytes;      // A hi, A lo, B hi, B lo
+constexpr uint32_t kTmemCols = 512;
+constexpr int kStageBytes = 2 * kI8BlockSet;  // A digits, B digits
 
 struct SmemLayout {
     static constexpr int stages = 0;
-    static constexpr int bars = kTcStages * kStageBytes;      // full[S], empty[S], accf[2], acce[2], drain
-    static constexpr int n_bars = 2 * kTcStages + 5;
+    static constexpr int etab = kTcStages * kStageBytes;       // double2[64 w][64 bubbles], XOR-swizzled
+    static constexpr int bars = etab + 64 * 64 * 16;          // full[S], empty[S], accf, acce, drain
+    static constexpr int n_bars = 2 * kTcStages + 3;
     static constexpr int tslot = bars + 8 * n_bars;
     static constexpr int abort_flag = tslot + 4;
     static constexpr int binfo = tslot + 16;                   // int[64]
     static constexpr int bt = binfo + 64 * 4;                  // double[64]
     static constexpr int bz = bt + 64 * 8;                     // double[64]
-    static constexpr int etab = bz + 64 * 8;                   // float2[64 w][64 bubbles], XOR-swizzled
-    static constexpr int total = etab + 64 * 64 * 8;
+    static constexpr int total = bz + 64 * 8;
 };
+static_assert(SmemLayout::total + 1024 <= 227 * 1024, "shared memory budget");
 
 // Phase-table slot of (frequency l, bubble b): rows of 64 bubbles, the bubble
-// index XORed with l % 16 so that the 16 frequencies read by a warp fall in
-// distinct banks.
-__device__ __forceinline__ int eslot(int l, int b) { return l * 64 + (b ^ (l & 15)); }
+// index XORed with l % 8 so that the 16 frequencies read by a warp fall in
+// distinct 16-byte bank groups (two wavefronts for 16 x 16 bytes).
+__device__ __forceinline__ int eslot(int l, int b) { return l * 64 + (b ^ (l & 7)); }
+
+// Shared-memory descriptor of a K-major, 32-byte-swizzled digit block (256-byte
+// aligned): bits [0,14) address >> 4, [16,30) leading byte offset >> 4 (unused
+// for this layout, 1), [32,46) stride byte offset >> 4 (256 bytes between
+// 8-row groups), [46,48) version 1, [61,64) layout 6 = 32-byte swizzle.
+__device__ __forceinline__ uint64_t sdesc_sw32(uint32_t addr) {
+    return (uint64_t)((addr >> 4) & 0x3fffu) | ((uint64_t)1 << 16) | ((uint64_t)(256 >> 4) << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)6 << 61);
+}
+
+// Instruction descriptor of kind::i8: S32 accumulator (bits [4,6) = 2), A and
+// B signed 8-bit (bits [7,10) and [10,13) = 1), K-major, dense, N >> 3 at
+// [17,23), M >> 4 at [24,29).
+__host__ __device__ constexpr uint32_t idesc_i8(int M, int N) {
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+// D[tmem] (+)= A[smem] * B[smem]^T in 32-bit integers; issued by one thread.
+__device__ __forceinline__ void mma_i8_ss(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t idesc,
+                                          uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// 16 consecutive 32-bit columns of this thread's lane.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr)
+        : "memory");
+}
 
 __global__ void k_tc_phase_table(const double* __restrict__ w, const double* __restrict__ cos_t,
                                  const double* __restrict__ t_arr, int n_cos, int n_w, int n_t, int n_wt, int nkb,
-                                 float* __restrict__ atab) {
+                                 int8_t* __restrict__ atab) {
     const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const size_t n_el = (size_t)n_cos * n_wt * nkb * kTcBlockFloats;
+    const size_t n_el = (size_t)n_cos * n_wt * nkb * kI8Block;
     if (q >= n_el) return;
-    const int e = (int)(q % kTcBlockFloats);
-    const size_t blk = q / kTcBlockFloats;  // (i, wt, kb)
+    const int e = (int)(q % kI8Block);
+    const size_t blk = q / kI8Block;  // (i, wt, kb)
     const int kb = (int)(blk % nkb);
     const int wt = (int)((blk / nkb) % n_wt);
     const int i = (int)(blk / ((size_t)nkb * n_wt));
     const int r = e >> 5, kk = e & 31;
     const int wi = wt * kTcWT + (r >> 1), k = kb * kTcKB + kk;
-    float v = 0.0f;
+    double v = 0.0;
     if (wi < n_w && k < n_t) {
         double sn, cs;
         sincos(w[wi] * ((1.0 - cos_t[i]) * t_arr[k]), &sn, &cs);
-        v = (float)((r & 1) ? sn : cs);
+        v = (r & 1) ? sn : cs;
     }
-    uint32_t hi, lo;
-    tc::split_tf32_fast(v, hi, lo);
-    float* out = atab + blk * 2 * kTcBlockFloats;
-    const size_t o = tc_swz(r, kk);
-    out[o] = __uint_as_float(hi);
-    out[kTcBlockFloats + o] = __uint_as_float(lo);
+    const uint32_t d = i8_digits(v);
+    int8_t* out = atab + blk * kI8BlockSet + i8_swz(r, kk);
+#pragma unroll
+    for (int s = 0; s < kI8Slices; ++s) out[(size_t)s * kI8Block] = (int8_t)(d >> (8 * s));
 }
 
 template <int S>
-__global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
+__global__ void __launch_bounds__(kTcThreads, 1) k_gemm_i8(TcArgs A) {
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                          ~static_cast<uintptr_t>(1023));
@@ -118,8 +163,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
     uint64_t* full = bars;
     uint64_t* empty = bars + kTcStages;
     uint64_t* accf = bars + 2 * kTcStages;
-    uint64_t* acce = accf + 2;
-    uint64_t* drain = acce + 2;
+    uint64_t* acce = accf + 1;
+    uint64_t* drain = acce + 1;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(sm + SmemLayout::tslot);
     volatile int* abort_flag = reinterpret_cast<volatile int*>(sm + SmemLayout::abort_flag);
     int* binfo = reinterpret_cast<int*>(sm + SmemLayout::binfo);
@@ -154,10 +199,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
             tc::mbar_init(&full[q], 1);   // the producer's arrive; the copies' bytes complete the phase
             tc::mbar_init(&empty[q], 1);  // the MMA thread's commit
         }
-        tc::mbar_init(&accf[0], 1);
-        tc::mbar_init(&accf[1], 1);
-        tc::mbar_init(&acce[0], 8);
-        tc::mbar_init(&acce[1], 8);
+        tc::mbar_init(accf, 1);  // the MMA thread's commit after a row's last stage
+        tc::mbar_init(acce, 8);  // every epilogue warp, once it holds the row's accumulators
         tc::mbar_init(drain, 1);
         *abort_flag = 0;
         tc::mbar_fence_init();
@@ -184,9 +227,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
         if (lane == 0 && active) {
             int it = 0;
             for (int i = i0; i < i1 && !failed; ++i) {
-                const float* arow = A.atab + ((size_t)(i * A.n_wt + wt) * nkb) * 2 * kTcBlockFloats;
-                const float* brow =
-                    A.btab + ((((size_t)frame * A.n_cos + i) * A.tiles_per_frame + tile) * nkb) * 2 * kTcBlockFloats;
+                const int8_t* arow = A.atab + ((size_t)(i * A.n_wt + wt) * nkb) * kI8BlockSet;
+                const int8_t* brow =
+                    A.btab + ((((size_t)frame * A.n_cos + i) * A.tiles_per_frame + tile) * nkb) * kI8BlockSet;
                 for (int kb = kb0; kb < nkb; ++kb, ++it) {
                     const int st = it % kTcStages;
                     if (!tc::mbar_wait_bounded_poll(&empty[st], ((it / kTcStages) & 1) ^ 1, abort_flag)) {
@@ -195,9 +238,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
                     }
                     unsigned char* dst = sm + SmemLayout::stages + st * kStageBytes;
                     tc::mbar_arrive_expect_tx(&full[st], kStageBytes);
-                    tc::bulk_g2s(dst, arow + (size_t)kb * 2 * kTcBlockFloats, 2 * kBlockBytes, &full[st]);
-                    tc::bulk_g2s(dst + 2 * kBlockBytes, brow + (size_t)kb * 2 * kTcBlockFloats, 2 * kBlockBytes,
-                                 &full[st]);
+                    tc::bulk_g2s(dst, arow + (size_t)kb * kI8BlockSet, kI8BlockSet, &full[st]);
+                    tc::bulk_g2s(dst + kI8BlockSet, brow + (size_t)kb * kI8BlockSet, kI8BlockSet, &full[st]);
                 }
             }
             // before the block ends, the copies this thread issued must have landed:
@@ -212,21 +254,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
     } else if (warp == 1) {
         // ---------------- MMA issue ----------------
         if (lane == 0 && active) {
-            const uint32_t idesc = tc::idesc_tf32(kTcRows, kTcCols);
-            int it = 0, seg = 0;
-            for (int i = i0; i < i1 && !failed; ++i) {
-                uint32_t dcol = 0, accumulate = 0;
+            const uint32_t idesc = idesc_i8(kTcRows, kTcCols);
+            int it = 0, row = 0;
+            for (int i = i0; i < i1 && !failed; ++i, ++row) {
+                // the epilogue has read the previous row's accumulators
+                if (!tc::mbar_wait_bounded_poll(acce, (row & 1) ^ 1, abort_flag)) {
+                    failed = true;
+                    break;
+                }
+                tc::tc_fence_after();
                 for (int kb = kb0; kb < nkb; ++kb, ++it) {
-                    if ((kb - kb0) % kTcFoldKB == 0) {  // a new accumulation segment
-                        const int buf = seg & 1;
-                        if (!tc::mbar_wait_bounded_poll(&acce[buf], ((seg >> 1) & 1) ^ 1, abort_flag)) {
-                            failed = true;
-                            break;
-                        }
-                        tc::tc_fence_after();
-                        dcol = tbase + 128 * buf;
-                        accumulate = 0;
-                    }
                     const int st = it % kTcStages;
                     if (!tc::mbar_wait_bounded_poll(&full[st], (it / kTcStages) & 1, abort_flag)) {
                         failed = true;
@@ -234,22 +271,27 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
                     }
                     tc::tc_fence_after();
                     const uint32_t base = tc::smem_u32(sm + SmemLayout::stages + st * kStageBytes);
-                    const uint32_t a_hi = base, a_lo = base + kBlockBytes;
-                    const uint32_t b_hi = base + 2 * kBlockBytes, b_lo = base + 3 * kBlockBytes;
-#pragma unroll
-                    for (int j = 0; j < kTcKB / 8; ++j) {
-                        tc::mma_tf32_ss(dcol, tc::sdesc_k128(a_hi + 32 * j), tc::sdesc_k128(b_lo + 32 * j), idesc,
-                                        accumulate);
-                        accumulate = 1;
-                        tc::mma_tf32_ss(dcol, tc::sdesc_k128(a_lo + 32 * j), tc::sdesc_k128(b_hi + 32 * j), idesc, 1);
-                        tc::mma_tf32_ss(dcol, tc::sdesc_k128(a_hi + 32 * j), tc::sdesc_k128(b_hi + 32 * j), idesc, 1);
-                    }
+                    // the ten digit pairs (p, q), p + q <= 3, into level p + q; the first
+                    // pair of each level in the row's first block starts that level's sum
+                    const uint32_t acc = kb == kb0 ? 0u : 1u;
+                    auto mma = [&](int p, int q, uint32_t a) {
+                        mma_i8_ss(tbase + 128 * (p + q), sdesc_sw32(base + p * kI8Block),
+                                  sdesc_sw32(base + kI8BlockSet + q * kI8Block), idesc, a);
+                    };
+                    mma(0, 0, acc);
+                    mma(0, 1, acc);
+                    mma(1, 0, 1u);
+                    mma(0, 2, acc);
+                    mma(1, 1, 1u);
+                    mma(2, 0, 1u);
+                    mma(0, 3, acc);
+                    mma(1, 2, 1u);
+                    mma(2, 1, 1u);
+                    mma(3, 0, 1u);
                     tc::mma_commit(&empty[st]);
-                    if ((kb - kb0) % kTcFoldKB == kTcFoldKB - 1 || kb == nkb - 1) {
-                        tc::mma_commit(&accf[seg & 1]);
-                        ++seg;
-                    }
                 }
+                if (failed) break;
+                tc::mma_commit(accf);
             }
             // wait for every MMA issued by this thread before the memory is freed
             tc::mma_commit(drain);
@@ -258,94 +300,91 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
         }
     } else {
         // ---------------- epilogue ----------------
-        // Tensor-core FP32 accumulation rounds each addition into a growing
-        // sum, so the accumulator is handed over every kTcFoldKB blocks of 32
-        // steps and its contribution, phase included (the phase is constant
-        // along a row), is added to FP64 sums per (w, set, +/x).  Each lane
-        // holds one GEMM row, Re (even lane) or Im (odd lane) of its
-        // frequency, and accumulates sum_b cos_b Y_b and sum_b sin_b Y_b of
-        // that row; Re C = sum cos Yr - sum sin Yi and Im C = sum cos Yi +
-        // sum sin Yr are formed once at the end.  Products are summed in FP32
-        // over the bubbles of a 32-column chunk (two interleaved chains), then
-        // added to the FP64 sums.
+        // Each lane holds one GEMM row, Re (even lane) or Im (odd lane) of its
+        // frequency, and accumulates sum_b cos_b Y_b and sum_b sin_b Y_b of that
+        // row in FP64; Re C = sum cos Yr - sum sin Yi and Im C = sum cos Yi +
+        // sum sin Yr are formed once at the end.
         const int q4 = warp & 3;             // tensor-memory lane quadrant of this warp
         const int half = (warp - 2) >> 2;    // which 64 columns
         const int r = 32 * q4 + lane;
         const int wl = r >> 1, part = r & 1;
         const int wi = w0 + wl;
         const uint32_t lanebase = (uint32_t)(32 * q4) << 16;
-        float2* etab = reinterpret_cast<float2*>(sm + SmemLayout::etab);
+        double2* etab = reinterpret_cast<double2*>(sm + SmemLayout::etab);
         double accC[CPB], accS[CPB];
 #pragma unroll
         for (int c = 0; c < CPB; ++c) accC[c] = accS[c] = 0.0;
+        constexpr float kInv254 = 1.0f / 254.0f;
         // the column offset is a compile-time constant in each instance, so that
         // every per-column index below is too (no dynamically indexed arrays)
         auto run = [&](auto half_c) {
             constexpr int c_lo = decltype(half_c)::value * (kTcCols / 2);
             constexpr int b_lo = c_lo / CPB, b_hi = (c_lo + kTcCols / 2 - 1) / CPB;
             constexpr int nb = b_hi - b_lo + 1;
-            int seg = 0;
-            for (int i = i0; active && i < i1 && !failed; ++i) {
-                // e^{i w (t_a c_i - z_a)} per (w, bubble) of this row; zero for empty columns.
-                // Each warp fills the entries it reads (its 16 frequencies, its bubbles).
+            int row = 0;
+            for (int i = i0; active && i < i1 && !failed; ++i, ++row) {
+                // s_a / 127^2 e^{i w (t_a c_i - z_a)} per (w, bubble) of this row; zero for
+                // empty columns.  Each warp fills the entries it reads (its 16
+                // frequencies, its bubbles) while the row's MMAs run.
                 const double ci = A.cos_t[i];
                 __syncwarp();
-#pragma unroll 4
                 for (int q = lane; q < 16 * nb; q += 32) {
                     const int b = b_lo + q % nb, l = 16 * q4 + q / nb;
-                    float2 e = make_float2(0.f, 0.f);
+                    double2 e = make_double2(0.0, 0.0);
                     if (b < A.bpt && binfo[b] >= 0 && w0 + l < A.n_w) {
+                        const double sc =
+                            A.bscale[((size_t)frame * A.n_sel + binfo[b]) * A.n_cos + i] * (1.0 / 16129.0);
                         double sn, cs;
-                        phase<float>(A.w[w0 + l] * (bt[b] * ci - bz[b]), sn, cs);
-                        e = make_float2((float)cs, (float)sn);
+                        sincos(A.w[w0 + l] * (bt[b] * ci - bz[b]), &sn, &cs);
+                        e = make_double2(sc * cs, sc * sn);
                     }
                     etab[eslot(l, b)] = e;
                 }
                 __syncwarp();
-                // this lane's phases for the whole row stay in registers
-                float2 evr[nb];
-#pragma unroll
-                for (int j = 0; j < nb; ++j) evr[j] = etab[eslot(wl, b_lo + j)];
-                const int nseg = (nkb - kb0 + kTcFoldKB - 1) / kTcFoldKB;
-                for (int g = 0; g < nseg; ++g, ++seg) {
-                    const int buf = seg & 1;
-                    if (!tc::warp_wait_bounded(&accf[buf], (seg >> 1) & 1, abort_flag)) {
-                        failed = true;
-                        break;
-                    }
-                    tc::tc_fence_after();
-                    // columns [n0, n0 + 32) from y; the chunk's phases are loaded first
-                    auto consume = [&](const uint32_t (&y)[32], auto n0_c) {
-                        constexpr int n0 = decltype(n0_c)::value;
-                        float pc[2][CPB], ps[2][CPB];
-#pragma unroll
-                        for (int c = 0; c < CPB; ++c) pc[0][c] = ps[0][c] = pc[1][c] = ps[1][c] = 0.f;
-#pragma unroll
-                        for (int c = 0; c < 32; ++c) {
-                            const int n = n0 + c;
-                            const int b = n / CPB, sc = n % CPB, h2 = b & 1;
-                            const float2 e = evr[b - b_lo];
-                            const float yv = __uint_as_float(y[c]);
-                            pc[h2][sc] = fmaf(e.x, yv, pc[h2][sc]);
-                            ps[h2][sc] = fmaf(e.y, yv, ps[h2][sc]);
-                        }
-#pragma unroll
-                        for (int q = 0; q < CPB; ++q) {
-                            accC[q] += (double)(pc[0][q] + pc[1][q]);
-                            accS[q] += (double)(ps[0][q] + ps[1][q]);
-                        }
-                    };
-                    const uint32_t dcol = (tbase + 128 * buf + c_lo) | lanebase;
-                    uint32_t y0[32], y1[32];
-                    tc::tmem_ld32(dcol, y0);
-                    tc::tmem_ld32(dcol + 32, y1);
-                    tc::tmem_wait_ld();
-                    tc::tc_fence_before();
-                    __syncwarp();
-                    if (lane == 0) tc::mbar_arrive(&acce[buf]);  // this warp's columns are in registers
-                    consume(y0, std::integral_constant<int, c_lo>{});
-                    consume(y1, std::integral_constant<int, c_lo + 32>{});
+                if (!tc::warp_wait_bounded(accf, row & 1, abort_flag)) {
+                    failed = true;
+                    break;
                 }
+                tc::tc_fence_after();
+                // columns [n0, n0 + 16): the four levels' integer sums combined
+                auto consume = [&](const uint32_t (&d0)[16], const uint32_t (&d1)[16], const uint32_t (&d2)[16],
+                                   const uint32_t (&d3)[16], auto n0_c) {
+                    constexpr int n0 = decltype(n0_c)::value;
+#pragma unroll
+                    for (int c = 0; c < 16; ++c) {
+                        const int n = n0 + c;
+                        const int b = n / CPB, sc = n % CPB;
+                        const float lo = fmaf(fmaf(fmaf((float)(int)d3[c], kInv254, (float)(int)d2[c]), kInv254,
+                                                   (float)(int)d1[c]),
+                                              kInv254, 0.0f);
+                        const double y = (double)(int)d0[c] + (double)lo;
+                        const double2 e = etab[eslot(wl, b)];
+                        accC[sc] = fma(e.x, y, accC[sc]);
+                        accS[sc] = fma(e.y, y, accS[sc]);
+                    }
+                };
+                auto chunk = [&](auto n0_c, bool last) {
+                    constexpr int n0 = decltype(n0_c)::value;
+                    const uint32_t col = (tbase + n0) | lanebase;
+                    uint32_t d0[16], d1[16], d2[16], d3[16];
+                    tc::tc_fence_after();
+                    tmem_ld16(col, d0);
+                    tmem_ld16(col + 128, d1);
+                    tmem_ld16(col + 256, d2);
+                    tmem_ld16(col + 384, d3);
+                    tc::tmem_wait_ld();
+                    if (last) {
+                        // this warp's columns of the row are in registers
+                        tc::tc_fence_before();
+                        __syncwarp();
+                        if (lane == 0) tc::mbar_arrive(acce);
+                    }
+                    consume(d0, d1, d2, d3, n0_c);
+                };
+                chunk(std::integral_constant<int, c_lo>{}, false);
+                chunk(std::integral_constant<int, c_lo + 16>{}, false);
+                chunk(std::integral_constant<int, c_lo + 32>{}, false);
+                chunk(std::integral_constant<int, c_lo + 48>{}, true);
             }
         };
         if (half == 0)
@@ -395,16 +434,16 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_tc(TcArgs A) {
 
 template <int S>
 void launch_s(const TcArgs& A, dim3 grid, size_t smem, cudaStream_t st) {
-    CUDA_OK(cudaFuncSetAttribute(k_gemm_tc<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_gemm_tc<S><<<grid, kTcThreads, smem, st>>>(A);
+    CUDA_OK(cudaFuncSetAttribute(k_gemm_i8<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gemm_i8<S><<<grid, kTcThreads, smem, st>>>(A);
 }
 
 }  // namespace
 
 void launch_tc_phase_table(const double* w, const double* cos_t, const double* t_arr, int n_cos, int n_w, int n_t,
-                           float* atab, cudaStream_t st) {
+                           int8_t* atab, cudaStream_t st) {
     const int n_wt = (n_w + kTcWT - 1) / kTcWT, nkb = (n_t + kTcKB - 1) / kTcKB;
-    const size_t n_el = (size_t)n_cos * n_wt * nkb * kTcBlockFloats;
+    const size_t n_el = (size_t)n_cos * n_wt * nkb * kI8Block;
     if (n_el / 256 + 1 > 0x7fffffffULL) throw Error{"time-phase table too large"};
     k_tc_phase_table<<<(unsigned)((n_el + 255) / 256), 256, 0, st>>>(w, cos_t, t_arr, n_cos, n_w, n_t, n_wt, nkb,
                                                                      atab);
@@ -430,6 +469,7 @@ int tc_row_parts(size_t n_ctas, int n_cos, int n_sm) {
 void launch_gemm_tc(const TcArgs& A, size_t kn, cudaStream_t st) {
     if (A.bpt * 2 * A.S > kTcCols) throw Error{"tensor-core GEMM: too many columns per tile"};
     if (A.row_parts < 1 || A.row_parts > A.n_cos) throw Error{"tensor-core GEMM: bad row split"};
+    if (A.n_t > kI8MaxSteps) throw Error{"the mixed kernel accumulates at most 32768 time steps exactly; use fp64_factored"};
     const size_t smem = SmemLayout::total + 1024;
     const size_t gy = kn * (size_t)A.tiles_per_frame * A.row_parts;
     if (gy > 65535) throw Error{"too many column tiles in one k-hat chunk"};

@@ -1,18 +1,55 @@
-// Tensor-core (tcgen05, TF32 split) time-phase GEMM of the mixed kernel, spectrum_tc.cu.
+// Tensor-core (tcgen05, int8 digit slices) time-phase GEMM of the mixed kernel, spectrum_tc.cu.
 #pragma once
+
+#include <cstdint>
 
 #include "device_common.cuh"
 
 namespace bgw {
 
-// Operand blocks in HBM: 128 rows x 32 time steps of TF32 in the K-major
-// 128-byte-swizzled layout of the UMMA descriptor (16 KB each), as a hi part
-// followed by a lo part (x = hi + lo).  Float index of (row n, step k) inside
-// a block; k in [0, 32).
-__host__ __device__ inline size_t tc_swz(int n, int k) {
-    return (size_t)(n >> 3) * 256 + (n & 7) * 32 + ((((k >> 2) ^ (n & 7))) << 2) + (k & 3);
+// Operand blocks in HBM: 128 rows x 32 time steps of int8 in the K-major
+// 32-byte-swizzled layout of the UMMA descriptor (4 KB per block): row n of a
+// block at byte (n/8)*256 + (n%8)*32, its 16-byte half h (steps 16h..16h+15)
+// at half position h ^ ((n/4) % 2).  Byte index of (row n, step k), k in [0, 32).
+__host__ __device__ inline int i8_swz(int n, int k) {
+    return (n >> 3) * 256 + (n & 7) * 32 + ((((k >> 4) ^ (n >> 2)) & 1) << 4) + (k & 15);
 }
-constexpr int kTcBlockFloats = 128 * 32;
+constexpr int kI8Slices = 4;                       // int8 digits per value
+constexpr int kI8Block = 128 * 32;                 // bytes of one digit block
+constexpr int kI8BlockSet = kI8Slices * kI8Block;  // the four digit blocks of one (rows, 32 steps) block
+
+// Digits of x in [-1, 1]: X = rint(x * 127 * 254^3) (|X| < 2^31) written in
+// balanced base 254, x = (d0 + d1/254 + d2/254^2 + d3/254^3) / 127 + e with
+// |e| <= 0.5 / (127 * 254^3) (2^-33 about) and every digit in [-127, 127].
+// u = X + 127 (254^3 + 254^2 + 254 + 1) is non-negative and below 2^32; its
+// base-254 digits D0 (not reduced, <= 254), D1, D2, D3 give d = D - 127.
+// Returned packed, byte s = digit d_s.
+constexpr double kI8Full = 127.0 * 254.0 * 254.0 * 254.0;  // 2 081 157 128
+constexpr uint32_t kI8Offset = 127u * (254u * 254u * 254u + 254u * 254u + 254u + 1u);
+__device__ __forceinline__ uint32_t i8_digits(double x) {
+    uint32_t u = (uint32_t)__double2int_rn(x * kI8Full) + kI8Offset;
+    const uint32_t d3 = u % 254u;
+    u /= 254u;
+    const uint32_t d2 = u % 254u;
+    u /= 254u;
+    const uint32_t d1 = u % 254u;
+    const uint32_t d0 = u / 254u;
+    // each byte holds D - 127 in two's complement
+    return ((d0 - 127u) & 0xffu) | (((d1 - 127u) & 0xffu) << 8) | (((d2 - 127u) & 0xffu) << 16) |
+           ((d3 - 127u) << 24);
+}
+
+// Four packed digit words (one step each, byte s = digit s) transposed into
+// four slice words (one digit each, byte m = step m).
+__device__ __forceinline__ void i8_transpose4(uint32_t p0, uint32_t p1, uint32_t p2, uint32_t p3,
+                                              uint32_t (&w)[4]) {
+    const uint32_t t0 = __byte_perm(p0, p1, 0x5140), t1 = __byte_perm(p2, p3, 0x5140);
+    const uint32_t t2 = __byte_perm(p0, p1, 0x7362), t3 = __byte_perm(p2, p3, 0x7362);
+    w[0] = __byte_perm(t0, t1, 0x5410);
+    w[1] = __byte_perm(t0, t1, 0x7632);
+    w[2] = __byte_perm(t2, t3, 0x5410);
+    w[3] = __byte_perm(t2, t3, 0x7632);
+}
 
 struct TcArgs {
     const D4* bub;          // rotated frames (kn, n_tot)
@@ -23,8 +60,9 @@ struct TcArgs {
     const double* w;
     const double* cos_t;
     const int* kfirst;      // (n_sel) first step with t_k > t_a
-    const float* atab;      // time phases: (n_cos, n_wt, nkb, hi|lo) blocks
-    const float* btab;      // beta: (kn, n_cos, tiles, nkb, hi|lo) blocks
+    const int8_t* atab;     // time-phase digits: (n_cos, n_wt, nkb) block sets
+    const int8_t* btab;     // beta digits: (kn, n_cos, tiles, nkb) block sets
+    const double* bscale;   // (kn, n_sel, n_cos): beta of row (frame, slot, i) = scale x digits
     int n_wt, nkb;
     int bpt;                // bubbles per 128-column tile
     int tiles_per_frame;
@@ -33,10 +71,11 @@ struct TcArgs {
     unsigned int* err;      // set non-zero when a pipeline wait gave up
 };
 
-// Fills atab (n_cos * n_wt * nkb * 2 blocks) with M_i[w, k] = e^{i w (1 - c_i) t_k}
-// (rows 2 l + {0: cos, 1: sin} of frequency tile wt, zero past n_w and n_t).
+// Fills atab (n_cos * n_wt * nkb block sets) with the digits of
+// M_i[w, k] = e^{i w (1 - c_i) t_k} (rows 2 l + {0: cos, 1: sin} of frequency
+// tile wt, zero past n_w and n_t).
 void launch_tc_phase_table(const double* w, const double* cos_t, const double* t_arr, int n_cos, int n_w, int n_t,
-                           float* atab, cudaStream_t st);
+                           int8_t* atab, cudaStream_t st);
 
 // Launches the GEMM + epilogue for kn frames on `st`.
 void launch_gemm_tc(const TcArgs& A, size_t kn, cudaStream_t st);
@@ -44,5 +83,8 @@ void launch_gemm_tc(const TcArgs& A, size_t kn, cudaStream_t st);
 // Row parts that make n_ctas x parts CTAs fill whole waves of one CTA per SM
 // best (at most n_cos / 8 parts).
 int tc_row_parts(size_t n_ctas, int n_cos, int n_sm);
+
+// Largest n_t the int8 GEMM accumulates exactly in 32-bit integers.
+constexpr int kI8MaxSteps = 32768;
 
 }  // namespace bgw

@@ -2,8 +2,11 @@
 (src/gw_fopt/bubble_dynamics/utils/data_gw_bulkflow.py, DataGwBulkFlow) on seeded
 synthetic bulk-flow output.
 
-Run in a container that has the reference source tree (its path is the first
-argument, default /root/reference).  The reference module imports the compiled
+Run in a container that has the reference source tree; its root directory is
+the required argument:
+
+    python tests/golden/make_postprocess_golden.py <reference-root>
+  The reference module imports the compiled
 extension gw_fopt.bubble_gw only for utils.sample; a stand-in that returns its
 first argument as an array is installed, and the rows carry their w and power
 lists directly.  filter_dataframe.py and data_gw_bulkflow.py are loaded from
@@ -40,7 +43,7 @@ def load_reference(root):
     return sys.modules["refpost.data_gw_bulkflow"].DataGwBulkFlow
 
 
-def main(root="/root/reference"):
+def main(root):
     DataGwBulkFlow = load_reference(root)
     rng = np.random.default_rng(20261204)
     K, S, W = 9, 3, 40
@@ -71,4 +74,6 @@ def main(root="/root/reference"):
 
 
 if __name__ == "__main__":
-    main(*sys.argv[1:])
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_postprocess_golden.py <reference-root>")
+    main(sys.argv[1])

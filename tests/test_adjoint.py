@@ -166,3 +166,82 @@ def test_autograd_vs_finite_differences(gpu_available):
         checked += 1
         assert abs(fd - gx[a, q]) <= FD_TOL * max(abs(fd), 1e-2 * scale), (a, q, fd, gx[a, q])
     assert checked >= 5
+
+
+@pytest.mark.gpu
+def test_config5_adjoint_vs_numpy_and_fd(gpu_available):
+    """Config 5 (256 bubbles at beta L = 6 with periodic images, 64x64 patches, T = 256, 64 w) on its
+    first k-hat: the library's FP64 adjoint against the numpy FP64 adjoint for the coefficients, the
+    powers and every bubble row (1e-9), and the autograd path of the fit loss against central
+    differences (h = 1e-6) of the library's FP64 forward for (xi, alpha, gamma, delta) and a sample of
+    nucleation coordinates (1e-5)."""
+    from gw_fopt_b200.autograd import BulkFlowSpectrum, SurfaceTensionFit, log_power_residual
+    c = W.config(5, k_subset=1)
+    n = c.interior.shape[0]
+    model = BulkFlowSpectrum(n_cos=c.n_cos, n_phi=c.n_phi, w=c.w, khat=c.khat, t_end=c.t_end, n_t=c.n_t,
+                             t_begin=c.t_begin, box=1.0, kernel="fp64_factored")
+    rng = np.random.default_rng(5)
+    G = rng.normal(size=(1, 2, 1, c.w.size)) + 1j * rng.normal(size=(1, 2, 1, c.w.size))
+    gc, gp, gx = model.vjp(c.coefficients, c.powers, c.interior, G)
+    oc, op, ob = OA.spectrum_vjp(c.interior, c.exterior, c.khat, c.n_cos, c.n_phi, c.w, c.t_begin, c.t_end,
+                                 c.n_t, G, c.coefficients, c.powers)
+    ox = ob[:n] + ob[n:].reshape(n, 6, 4).sum(1)
+    for got, ref in [(gc, oc), (gp, op), (gx, ox)]:
+        assert np.allclose(got, ref, rtol=1e-9, atol=1e-12 * np.abs(ref).max())
+
+    fit = SurfaceTensionFit(xi=1.5, alpha=1.0, gamma=0.0, delta=0.0)
+    x = torch.tensor(c.interior, dtype=torch.float64, requires_grad=True)
+    with torch.no_grad():
+        co_t, po_t = SurfaceTensionFit(xi=2.0, alpha=1.1, gamma=0.4, delta=-0.1)()
+        target = (model(co_t, po_t, x) ** 2).sum(-1).sum(1)
+    co, po = fit()
+    loss = log_power_residual(model(co, po, x), target)
+    loss.backward()
+
+    def f(xi=1.5, alpha=1.0, gamma=0.0, delta=0.0, xx=None):
+        with torch.no_grad():
+            cc, pp = SurfaceTensionFit(xi, alpha, gamma, delta)()
+            return float(log_power_residual(model(cc, pp, x if xx is None else xx), target))
+
+    base = dict(xi=1.5, alpha=1.0, gamma=0.0, delta=0.0)
+    for name in base:
+        p, q = dict(base), dict(base)
+        p[name] += H
+        q[name] -= H
+        fd = (f(**p) - f(**q)) / (2 * H)
+        an = float(getattr(fit, name).grad)
+        assert abs(fd - an) <= FD_TOL * max(abs(fd), 1e-12), (name, fd, an)
+    gxa = x.grad.numpy()
+    scale = np.abs(gxa).max()
+    checked = 0
+    for a in range(3, n, 8):
+        for q in range(4):
+            def fun(h, a=a, q=q):
+                xx = x.detach().clone()
+                xx[a, q] += h
+                return f(xx=xx)
+            fd, smooth = central_fd(fun)
+            if not smooth:
+                continue
+            checked += 1
+            assert abs(fd - gxa[a, q]) <= FD_TOL * max(abs(fd), 1e-2 * scale), (a, q, fd, gxa[a, q])
+    # 256 bubbles put kinks (collision-status flips) near most coordinates; enough stay smooth
+    assert checked >= 8
+
+
+@pytest.mark.gpu
+def test_adjoint_bitwise_repeatable(gpu_available):
+    """The bubble gradients are sums of many contributions accumulated by concurrent blocks; they
+    are formed as fixed-point integer sums, so repeated calls give the same bits."""
+    c = small_case(seed=9, n=8)
+    c["n_cos"], c["n_phi"], c["n_t"] = 16, 16, 48
+    c["kh"] = W.fibonacci_khat(4)
+    m = _library_model(c)
+    rng = np.random.default_rng(3)
+    G = rng.normal(size=(4, 2, 1, 5)) + 1j * rng.normal(size=(4, 2, 1, 5))
+    co, po = np.array([[0.7, 0.3]]), np.array([[5.0, 3.5]])
+    first = m.vjp(co, po, c["inter"], G)
+    for _ in range(3):
+        again = m.vjp(co, po, c["inter"], G)
+        for x, y in zip(first, again):
+            assert np.array_equal(x, y)

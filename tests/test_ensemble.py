@@ -92,3 +92,25 @@ def test_ensemble_matches_single_and_oracle(gpu_available, kernel):
         check(kernel, out[r], ref, f"ensemble r={r}")
     t = ens.last_timings()
     assert t["total_ms"] > 0 and t["launches"] > 0
+
+
+@pytest.mark.gpu
+def test_config4_realizations_per_w(gpu_available):
+    """Config 4 (the batched-ensemble workload: N_r ~ U{50..800}, beta_r L ~ U[5, 15], 96x96 patches,
+    T = 384, 128 w): its largest and smallest realizations and two others in one ensemble call on
+    2 k-hat, mixed against fp64_factored per realization, <= 1e-6 per w."""
+    c = W.ensemble_config(k_subset=2)
+    sizes = [inter.shape[0] for inter, _ in c.realizations]
+    pick = sorted({int(np.argmax(sizes)), int(np.argmin(sizes)), 0, 100})
+    reals = [c.realizations[r] for r in pick]
+    out = {}
+    for kernel in ("mixed", "fp64_factored"):
+        ens = BulkFlowEnsemble(reals, validate=False)
+        ens.set_resolution(c.n_cos, c.n_phi)
+        ens.set_gradient_scaling_params(c.coefficients.tolist(), c.powers.tolist())
+        ens.set_kernel(kernel)
+        out[kernel] = ens.compute_c_integral_khat(c.w, c.khat, t_begin=c.t_begin, t_end=c.t_end, n_t=c.n_t)
+    for q, r in enumerate(pick):
+        e = err_per_w(out["mixed"][q], out["fp64_factored"][q])
+        print(f"config4 realization {r} ({sizes[r]} bubbles): mixed vs fp64_factored per-w {e:.3e}")
+        assert e < 1e-6

@@ -21,9 +21,10 @@ from gw_fopt_b200 import workloads as W
 pytestmark = pytest.mark.gpu
 
 FP64_TOL = 1e-12
+FACTORED_PER_W_TOL = 1e-10
 MIXED_TOL = 1e-6
+SIMT_PER_W_BOUND = 1e-4
 KERNELS = ["fp64_direct", "fp64_factored", "mixed", "mixed_simt"]
-TOL = {"fp64_direct": FP64_TOL, "fp64_factored": FP64_TOL, "mixed": MIXED_TOL, "mixed_simt": MIXED_TOL}
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "golden_small.npz")
 
 
@@ -37,32 +38,30 @@ def err_per_w(got, ref):
     return float(np.max(num / np.maximum(den, 1e-300 + 1e-13 * scale)))
 
 
-def mixed_errors(got, ref):
-    """Error measures of the mixed-precision form against FP64:
-    global = ||got - ref||_2 / ||ref||_2 over the whole spectrum;
-    peak   = max_w ||got - ref||(w) / max_w ||ref||(w)   (per-w error on the spectrum's scale).
-    FP32 operands leave an absolute error floor that does not depend on w, so
-    the plain per-w relative error grows where |C(w)| falls in the spectral tail."""
-    g = got.reshape(-1, got.shape[-1])
-    r = ref.reshape(-1, ref.shape[-1])
-    num = np.linalg.norm(g - r, axis=0)
-    den = np.linalg.norm(r, axis=0)
-    return float(np.linalg.norm(g - r) / np.linalg.norm(r)), float(num.max() / den.max())
+def global_err(got, ref):
+    return float(np.linalg.norm(got - ref) / np.linalg.norm(ref))
 
 
 def check(kernel, got, ref, label):
-    """fp64_direct follows the reference's arithmetic term by term: per-w relative error <= 1e-12.
-    fp64_factored and mixed form the phase as w t (1 - c) + w (t_a c - z_a), whose rounding
-    differs from the reference's per-term rounding: their error is held to the tolerance in the
-    global and peak-scaled norms (per-w values are printed)."""
-    if kernel != "fp64_direct":
-        glob, peak = mixed_errors(got, ref)
-        print(f"{label} {kernel}: global {glob:.3e} peak-scaled {peak:.3e} per-w {err_per_w(got, ref):.3e}")
-        assert glob < TOL[kernel] and peak < TOL[kernel]
+    """Per-kernel tolerances, all asserted per w (norm over k-hat, +/x and sets at each w):
+    fp64_direct   follows the reference's arithmetic term by term: <= 1e-12 per w;
+    fp64_factored forms the phase as w t (1 - c) + w (t_a c - z_a), whose rounding differs
+                  from the reference's per-term rounding: <= 1e-12 globally and <= 1e-10 per w
+                  (the difference grows at spectral dips, where |C(w)| is small);
+    mixed         the int8 digit-slice tensor-core GEMM: <= 1e-6 per w;
+    mixed_simt    FP32 operands on CUDA cores: <= 1e-6 globally; per w only a regression
+                  bound (its absolute error floor, ~6e-8 of the terms, exceeds 1e-6 of |C(w)|
+                  at deep dips)."""
+    pw, glob = err_per_w(got, ref), global_err(got, ref)
+    print(f"{label} {kernel}: per-w max {pw:.3e} global {glob:.3e}")
+    if kernel == "fp64_direct":
+        assert pw < FP64_TOL
+    elif kernel == "fp64_factored":
+        assert glob < FP64_TOL and pw < FACTORED_PER_W_TOL
+    elif kernel == "mixed":
+        assert pw < MIXED_TOL
     else:
-        err = err_per_w(got, ref)
-        print(f"{label} {kernel}: max_w rel err {err:.3e}")
-        assert err < TOL[kernel]
+        assert glob < MIXED_TOL and pw < SIMT_PER_W_BOUND
 
 
 def golden_cases():
@@ -253,3 +252,32 @@ def test_python_fixed_bubble_and_masks(gpu_available):
     assert err_per_w(one, ref) < FP64_TOL
     with pytest.raises(IndexError):
         g.compute_c_integral_fixed_bubble(9, p["w"], 0.0, 15.0, 200)
+
+
+def test_config3_slice_per_w(gpu_available):
+    """Config 3 geometry (4096 bubbles, 28672 colliders with images, 192x192 patches, T = 1024,
+    256 w): 64 radiating bubbles spread over nucleation order with every collider present (an
+    exact partial sum, generalized_bulk_flow.rs:953-981), 2 k-hat, every w.
+    mixed vs fp64_factored <= 1e-6 per w; fp64_factored vs fp64_direct <= 1e-10 per w;
+    fp64_direct vs the oracle on one radiating bubble <= 1e-12 per w."""
+    c = W.config(3, k_subset=2)
+    sel = np.arange(0, c.n, 64)
+    out = {}
+    for kernel in ("fp64_direct", "fp64_factored", "mixed"):
+        g = make_flow(c.interior, c.exterior, c.n_cos, c.n_phi, c.coefficients, c.powers, kernel=kernel)
+        out[kernel] = g.compute_c_integral_khat(c.w, c.khat, t_begin=c.t_begin, t_end=c.t_end, n_t=c.n_t,
+                                                selected_bubbles=sel)
+    e_mixed = err_per_w(out["mixed"], out["fp64_factored"])
+    e_fact = err_per_w(out["fp64_factored"], out["fp64_direct"])
+    print(f"config3 slice: mixed vs fp64_factored per-w {e_mixed:.3e}; fp64_factored vs fp64_direct {e_fact:.3e}")
+    assert e_mixed < MIXED_TOL
+    assert e_fact < FACTORED_PER_W_TOL
+    # one radiating bubble, first k-hat, against the oracle
+    a = int(sel[3])
+    g = make_flow(c.interior, c.exterior, c.n_cos, c.n_phi, c.coefficients, c.powers, kernel="fp64_direct")
+    one = g.compute_c_integral_khat(c.w, c.khat[:1], t_begin=c.t_begin, t_end=c.t_end, n_t=c.n_t,
+                                    selected_bubbles=[a])
+    R = O.rotation_for_khat(c.khat[0])
+    ref = O.compute_c_integral(O.rotate(R, c.interior), O.rotate(R, c.exterior), c.n_cos, c.n_phi, c.w, c.t_end,
+                               c.n_t, t_begin=c.t_begin, coefficients=c.coefficients, powers=c.powers, selected=[a])
+    check("fp64_direct", one[0], ref, "config3 one bubble")

@@ -73,6 +73,26 @@ def test_noalloc_matches_allocating_entry_point(gpu_available):
         assert np.array_equal(got_codes, ref_codes[sel])
         assert np.array_equal(got_tau, ref_tau[sel])
 
+    # an index past the interior bubbles cannot be checked on the host (it lives in device
+    # memory): its row reads INT32_MIN codes and NaN delays, the other rows are unaffected
+    sel = np.array([3, n_int, 200], dtype=np.int64)
+    d_sel = torch.tensor(sel.astype(np.int32), device=dev)
+    codes = torch.full((sel.size, nd), 12345, dtype=torch.int32, device=dev)
+    tau = torch.full((sel.size, nd), -1.0, dtype=torch.float64, device=dev)
+    st = lib.bgwx_first_colliding_noalloc(
+        C.c_void_p(bubbles.data_ptr()), n_int, n_tot, C.c_void_p(d_sel.data_ptr()), sel.size,
+        C.c_void_p(dirs.data_ptr()), nd, C.c_void_p(codes.data_ptr()), C.c_void_p(tau.data_ptr()),
+        C.c_void_p(stream.cuda_stream))
+    assert st == L.OK, lib.bgw_last_error_message().decode()
+    torch.cuda.synchronize()
+    got_codes = codes.cpu().numpy().reshape(sel.size, n_cos, n_phi)
+    got_tau = tau.cpu().numpy().reshape(sel.size, n_cos, n_phi)
+    assert np.all(got_codes[1] == np.iinfo(np.int32).min)
+    assert np.all(np.isnan(got_tau[1]))
+    for row, a in ((0, 3), (2, 200)):
+        assert np.array_equal(got_codes[row], ref_codes[a])
+        assert np.array_equal(got_tau[row], ref_tau[a])
+
     # more radiating bubbles than the static work array holds: a clear error, nothing launched
     big = torch.zeros(513, dtype=torch.int32, device=dev)
     st = lib.bgwx_first_colliding_noalloc(
