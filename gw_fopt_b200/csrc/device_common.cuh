@@ -81,6 +81,7 @@ struct Device {
     DevBuf ens_out;                                  // batched ensemble: all realizations' spectra
     DevBuf pp_in, pp_small, pp_out;                  // spectrum post-processing: input, small tables, output
     DevBuf beta_scale;                               // int8 tensor-core GEMM: per-(bubble, row) beta scales
+    DevBuf fact_Dmax;                                // int8 tensor-core GEMM: per-(bubble, block) time-table maxima
     DevBuf tc_atab;                                  // int8 tensor-core GEMM: time-phase digits
     std::vector<double> tc_key;                      // (n_w, n_cos, n_t, w, cos-theta, t) of tc_atab
     bool tc_key_reuse = false;                       // set by the batched ensemble: one grid for all calls

@@ -348,6 +348,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
     __shared__ D4 s_pos[kList];
     __shared__ double s_nrm[kList];
     __shared__ double s_l1[kList];  // |dt| + |dx| + |dy| + |dz|
+    __shared__ double s_thr[kList]; // direction-independent part of the verification bound, see theta_of
     __shared__ double s_key[kList];
     __shared__ int s_idx[kList];
     __shared__ D4 s_opos[kMaxOutliers];
@@ -361,8 +362,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
     const size_t rpb = (n_rows + n_split - 1) / n_split;
     const size_t r_begin = min(n_rows, rpb * part), r_end = min(n_rows, rpb * (part + 1));
     const size_t d_begin = r_begin * row_len, d_end = r_end * row_len;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    constexpr int kWarps = kMaskListThreads / 32;
+    const int lane = threadIdx.x & 31;
     constexpr int kBatch = 2;
     constexpr int kRowsPerItem = 8;  // rows walked by a warp in one strip item
     const D4* B = bub + (size_t)k * n_tot;
@@ -395,6 +395,14 @@ __global__ void __launch_bounds__(kMaskListThreads)
         s_pos[q] = dc;
         s_nrm[q] = mdot(dc, dc);
         s_l1[q] = fabs(dc.t) + fabs(dc.x) + fabs(dc.y) + fabs(dc.z);
+        {
+            // theta = tau (1 + 1e-12) + 64 u (A rho1 + Q rho2) / dot with 1 / dot = 2 tau / nrm
+            // for a collider (nrm > 0): theta = tau (1 + 1e-12 + s_thr)
+            const double dx = sqrt(dc.x * dc.x + dc.y * dc.y + dc.z * dc.z);
+            const double Ac = fabs(dc.t) + dx, Qc = dc.t * dc.t + dx * dx;
+            s_thr[q] = s_nrm[q] > 0.0 ? 2.0 * (64.0 * 1.1102230246251565e-16) * (Ac * L->rho1 + Qc * L->rho2) / s_nrm[q]
+                                      : CUDART_INF;
+        }
         if (!(s_l1[q] < 1e5)) s_big = true;  // benign race: every writer stores true
     }
     for (int q = threadIdx.x; q < no; q += kMaskListThreads) {
@@ -404,8 +412,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
         s_onrm[q] = mdot(dc, dc);
     }
     __syncthreads();
-    const double kmax = L->kmax, rho1 = L->rho1, rho2 = L->rho2;
-    const double u64 = 64.0 * 1.1102230246251565e-16;
+    const double kmax = L->kmax;
     unsigned long long n_full = 0;
     // Work items: 32 consecutive directions of a row (a strip) over up to kRowsPerItem
     // consecutive rows.  A lane walks its column down the rows; each result, when it came
@@ -502,11 +509,9 @@ __global__ void __launch_bounds__(kMaskListThreads)
             }
             return ok;
         };
-        auto theta_of = [&](const D4& dc, double tau, double dot) {
-            const double dx = sqrt(dc.x * dc.x + dc.y * dc.y + dc.z * dc.z);
-            const double A = fabs(dc.t) + dx, Q = dc.t * dc.t + dx * dx;
-            return tau * (1.0 + 1e-12) + u64 * (A * rho1 + Q * rho2) / dot;
-        };
+        // The verification bound of listed candidate e with delay tau (the 1e-12 relative slack
+        // covers the few roundings of this form)
+        auto theta_of = [&](int e, double tau) { return tau * ((1.0 + 1e-12) + s_thr[e]); };
 
         // 0. the previous row's result at this column (the neighbouring patch in cos theta
         //    most often has the same first collider): checked against every listed collider up
@@ -519,7 +524,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
             if (ds > 1e-10) {
                 const double ts = __ddiv_rn(s_nrm[seed], dmul(2.0, ds));
                 if (ts > 0.0) {
-                    const double th = theta_of(ds_, ts, ds);
+                    const double th = theta_of(seed, ts);
                     int dummy = 0;
                     if (th < kmax && verify(s_idx[seed], ds_, s_nrm[seed], th, nullptr, dummy)) {
                         result = s_idx[seed];
@@ -577,7 +582,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
                 // 2. verify the candidate
                 const D4 dm = s_pos[bi];
                 const double nm = s_nrm[bi];
-                const double th = theta_of(dm, best, dotm);
+                const double th = theta_of(bi, best);
                 if (!(th < kmax)) {
                     full = true;
                 } else {
@@ -599,7 +604,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
                             const double nc = s_nrm[e];
                             const double tau = __ddiv_rn(nc, dmul(2.0, dot));
                             if (!(tau > 0.0)) continue;
-                            const double thf = theta_of(dc, tau, dot);
+                            const double thf = theta_of(e, tau);
                             if (!(thf < kmax)) {
                                 full = true;
                                 break;

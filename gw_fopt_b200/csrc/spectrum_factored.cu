@@ -79,6 +79,30 @@ __global__ void k_time_tables(const D4* __restrict__ bub, const uint32_t* __rest
     if (k == n_t - 1 && !on) kfirst[slot] = n_t;
 }
 
+// Per (bubble, block of 32 steps): the least and the largest D_q(k) of each
+// table column over the block's steps k < n_t (one warp, lane = step), stored
+// as (min, max) pairs.
+__global__ void k_time_maxima(const double* __restrict__ D, int n_sel, int n_t, int nblk, int Q,
+                              double* __restrict__ Dmax) {
+    const long wid = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (wid >= (long)n_sel * nblk) return;
+    const int slot = (int)(wid / nblk), b = (int)(wid % nblk);
+    const int k = (b << 5) + lane;
+    for (int q = 0; q < Q; ++q) {
+        const double v = k < n_t ? D[((size_t)slot * n_t + k) * Q + q] : 0.0;
+        double lo = v, hi = v;
+        for (int o = 16; o > 0; o >>= 1) {
+            lo = fmin(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+            hi = fmax(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+        }
+        if (lane == 0) {
+            Dmax[((size_t)wid * Q + q) * 2] = lo;
+            Dmax[((size_t)wid * Q + q) * 2 + 1] = hi;
+        }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // k_beta: one warp per row (frame, slot, i).  The row's collided patches
 // become events at the first step k_j with (t_k - t_a) >= tau_j (exact FP64
@@ -114,6 +138,7 @@ struct BetaArgs {
     int per_warp_bytes;
     int tiles;             // column tiles per frame (int8 digit layout)
     double* scale;         // int8 digit layout: (kn, n_sel, n_cos) row scales, max |beta| of the row
+    const double* Dmax;    // int8 digit layout: (n_sel, nblk, 1+S*M, 2) least and largest D over each block's steps
 };
 
 // x^p: binary powering for integral |p| <= 32 (a few ulp), pow() otherwise.
@@ -372,9 +397,10 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             for (int q = 0; q < 1 + SMC; ++q) g[q] = __ldg(Dk + q);
         }
         double vc = g[0] * Uc, vs = g[0] * Us;
+        const int t0 = s * A.M, t1 = t0 + A.M;  // the terms of set s
 #pragma unroll
         for (int t = 0; t < SMC; ++t) {
-            if (t / A.M != s) continue;
+            if (t < t0 || t >= t1) continue;
             vc += g[1 + t] * P[2 * t];
             vs += g[1 + t] * P[2 * t + 1];
         }
@@ -469,25 +495,114 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
         for (int q = 0; q < 2 * SMC; ++q) P[q] = pbeg[(size_t)b * 2 * SMC + q] + P[q];
     };
     if constexpr (kI8) {
-        // lane = step for every block.  Sweep 0: the row's scale, max |beta|.  Sweep 1: the
-        // digits.  A quad of lanes (4 steps) transposes its four packed digit words so that
-        // lane 4q + d holds digit d of steps 4q .. 4q + 3; one store instruction then fills
-        // 32 contiguous bytes of each of the four digit blocks.
+        // The row's scale is max |beta| over its steps and columns, found exactly without
+        // forming every value.  In block b, beta = rf (D0(k) U(k) + sum_m Dm(k) Pm(k)) is bounded
+        // by interval arithmetic over the per-block ranges of the time table and of U, Pm (constant
+        // in a block without events); blocks are formed (lane = step) in decreasing order of their
+        // bound until no bound exceeds the largest value found (most often one block: the last
+        // one, where dt^3 peaks).
         double vmax = 0.0;
-        for (int b = 0; b < NB; ++b) {
+        const double* Dmx = A.Dmax + (size_t)slot * NB * (1 + SMC) * 2;
+        auto block_max = [&](int b) {  // whole warp; lane = step
             double P[2 * SMC], Uc, Us;
             step_sums(b, P, Uc, Us);
             const int k = (b << 5) + lane;
+            double m = 0.0;
             for (int s2 = 0; s2 < A.S; ++s2) {
                 double xc, xs;
                 value(k, s2, P, Uc, Us, xc, xs);
-                vmax = fmax(vmax, fmax(fabs(xc), fabs(xs)));
+                m = fmax(m, fmax(fabs(xc), fabs(xs)));
+            }
+            return m;
+        };
+        for (int bc = 0; bc < NB; bc += 32) {
+            const int bl = bc + lane;
+            const bool has = bl < NB && boff[bl] != boff[bl + 1];
+            // a block holding events: U and Pm move by its events' weights within the block, so
+            // |U(k)| <= |U after the block| + sum |q| and |Pm(k)| <= |Pm before it| + sum |q f|
+            double addU = 0.0, addP[SMC];
+#pragma unroll
+            for (int q = 0; q < SMC; ++q) addP[q] = 0.0;
+            for (unsigned h = __ballot_sync(full, has); h; h &= h - 1) {
+                const int b = bc + __ffs(h) - 1;
+                double aU = 0.0, aP[SMC];
+#pragma unroll
+                for (int q = 0; q < SMC; ++q) aP[q] = 0.0;
+                for (int e = boff[b] + lane; e < boff[b + 1]; e += 32) {
+                    aU += fmax(fabs(evq[e]), fabs(evq[(size_t)EV + e]));
+#pragma unroll
+                    for (int q = 0; q < SMC; ++q)
+                        aP[q] += fmax(fabs(evq[(size_t)(2 + 2 * q) * EV + e]), fabs(evq[(size_t)(3 + 2 * q) * EV + e]));
+                }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    aU += __shfl_xor_sync(full, aU, o);
+#pragma unroll
+                    for (int q = 0; q < SMC; ++q) aP[q] += __shfl_xor_sync(full, aP[q], o);
+                }
+                if (lane == b - bc) {
+                    addU = aU;
+#pragma unroll
+                    for (int q = 0; q < SMC; ++q) addP[q] = aP[q];
+                }
+            }
+            double bnd = -1.0;  // this lane's block's bound (-1: none)
+            if (bl < NB) {
+                // interval arithmetic: beta of set s, column g lies in
+                // rf (D0 [U] + sum_m Dm [Pm]) with D in [min, max] over the block and U, Pm in
+                // [value at the block's end or start -/+ the block's event weights]
+                const double* mx = Dmx + (size_t)bl * (1 + SMC) * 2;
+                auto term = [&](double dlo, double dhi, double c, double a, double& lo, double& hi, double& sa) {
+                    const double c0 = c - a, c1 = c + a;
+                    const double p0 = dlo * c0, p1 = dlo * c1, p2 = dhi * c0, p3 = dhi * c1;
+                    lo += fmin(fmin(p0, p1), fmin(p2, p3));
+                    hi += fmax(fmax(p0, p1), fmax(p2, p3));
+                    sa += fmax(fabs(dlo), fabs(dhi)) * (fabs(c) + a);
+                };
+                for (int s2 = 0; s2 < A.S; ++s2) {
+                    const int t0 = s2 * A.M, t1 = t0 + A.M;
+#pragma unroll
+                    for (int g = 0; g < 2; ++g) {
+                        double lo = 0.0, hi = 0.0, sa = 0.0;
+                        term(mx[0], mx[1], uend[2 * bl + g], addU, lo, hi, sa);
+#pragma unroll
+                        for (int q = 0; q < SMC; ++q)
+                            if (q >= t0 && q < t1)
+                                term(mx[2 + 2 * q], mx[3 + 2 * q], pbeg[(size_t)bl * 2 * SMC + 2 * q + g], addP[q], lo,
+                                     hi, sa);
+                        // relative and absolute margins cover the rounding of these sums and of
+                        // the values themselves (a few ulp of the summed magnitudes)
+                        bnd = fmax(bnd, (fmax(fabs(lo), fabs(hi)) * (1.0 + 1e-12) + 1e-13 * sa) * rf);
+                    }
+                }
+            }
+            for (;;) {
+                double vm = fmax(vmax, __shfl_xor_sync(full, vmax, 16));  // lanes agree on vmax below
+                for (int o = 8; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(full, vm, o));
+                vmax = vm;
+                double bb = bnd;
+                int bi = lane;
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double ob = __shfl_xor_sync(full, bb, o);
+                    const int oi = __shfl_xor_sync(full, bi, o);
+                    if (ob > bb || (ob == bb && oi < bi)) {
+                        bb = ob;
+                        bi = oi;
+                    }
+                }
+                if (!(bb > vmax)) break;  // every remaining bound is covered
+                vmax = fmax(vmax, block_max(bc + bi));
+                if (lane == bi) bnd = -1.0;
             }
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(full, vmax, o));
         if (lane == 0) A.scale[row] = vmax;
         const double inv = vmax > 0.0 ? 1.0 / vmax : 0.0;
+        // digits.  Blocks with events: lane = step; a quad of lanes transposes its packed digit
+        // words so that lane 4q + d holds digit d of steps 4q .. 4q + 3.  Blocks without
+        // events: 4 steps per lane (8 lanes a block, 4 blocks at a time), transposed in
+        // registers.  Either way a store instruction fills whole 32-byte rows of the blocks.
         const bool odd = lane & 1, hi = lane & 2;
         auto quad_transpose = [&](uint32_t p) {
             const uint32_t t1 = __shfl_xor_sync(full, p, 1);
@@ -496,18 +611,56 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             return __byte_perm(p, t2, hi ? 0x3276 : 0x5410);
         };
         const int dg = lane & 3, s4 = (lane >> 2) * 4;
-        for (int b = 0; b < NB; ++b) {
-            double P[2 * SMC], Uc, Us;
-            step_sums(b, P, Uc, Us);
-            const int k = (b << 5) + lane;
-            int8_t* blk = blk_row + (size_t)b * kI8BlockSet + dg * kI8Block;
-            for (int s2 = 0; s2 < A.S; ++s2) {
-                double xc, xs;
-                value(k, s2, P, Uc, Us, xc, xs);
-                const uint32_t wc = quad_transpose(i8_digits(xc * inv));
-                const uint32_t ws = quad_transpose(i8_digits(xs * inv));
-                *reinterpret_cast<uint32_t*>(blk + i8_swz(nbase + 2 * s2, s4)) = wc;
-                *reinterpret_cast<uint32_t*>(blk + i8_swz(nbase + 2 * s2 + 1, s4)) = ws;
+        for (int bc = 0; bc < NB; bc += 32) {
+            const int bl = bc + lane;
+            const bool has = bl < NB && boff[bl] != boff[bl + 1];
+            const unsigned ev_blocks = __ballot_sync(full, has);
+            unsigned quiet = __ballot_sync(full, bl < NB && !has);
+            for (unsigned h = ev_blocks; h; h &= h - 1) {
+                const int b = bc + __ffs(h) - 1;
+                double P[2 * SMC], Uc, Us;
+                step_sums(b, P, Uc, Us);
+                const int k = (b << 5) + lane;
+                int8_t* blk = blk_row + (size_t)b * kI8BlockSet + dg * kI8Block;
+                for (int s2 = 0; s2 < A.S; ++s2) {
+                    double xc, xs;
+                    value(k, s2, P, Uc, Us, xc, xs);
+                    const uint32_t wc = quad_transpose(i8_digits(xc * inv));
+                    const uint32_t ws = quad_transpose(i8_digits(xs * inv));
+                    *reinterpret_cast<uint32_t*>(blk + i8_swz(nbase + 2 * s2, s4)) = wc;
+                    *reinterpret_cast<uint32_t*>(blk + i8_swz(nbase + 2 * s2 + 1, s4)) = ws;
+                }
+            }
+            const int sub = lane >> 3, s0 = (lane & 7) * 4;
+            while (quiet) {
+                unsigned t = quiet;
+                for (int g = 0; g < sub && t; ++g) t &= t - 1;
+                const int b = t ? bc + __ffs(t) - 1 : -1;
+                for (int g = 0; g < 4 && quiet; ++g) quiet &= quiet - 1;
+                if (b < 0) continue;
+                const double* P = pbeg + (size_t)b * 2 * SMC;
+                const double Uc = uend[2 * b], Us = uend[2 * b + 1];
+                const int k0 = (b << 5) + s0;
+                int8_t* blk = blk_row + (size_t)b * kI8BlockSet;
+                for (int s2 = 0; s2 < A.S; ++s2) {
+                    uint32_t pc[4], ps[4];
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        double xc, xs;
+                        value(k0 + m, s2, P, Uc, Us, xc, xs);
+                        pc[m] = i8_digits(xc * inv);
+                        ps[m] = i8_digits(xs * inv);
+                    }
+                    uint32_t wc[4], ws[4];
+                    i8_transpose4(pc[0], pc[1], pc[2], pc[3], wc);
+                    i8_transpose4(ps[0], ps[1], ps[2], ps[3], ws);
+                    const int oc = i8_swz(nbase + 2 * s2, s0), os = i8_swz(nbase + 2 * s2 + 1, s0);
+#pragma unroll
+                    for (int d = 0; d < kI8Slices; ++d) {
+                        *reinterpret_cast<uint32_t*>(blk + d * kI8Block + oc) = wc[d];
+                        *reinterpret_cast<uint32_t*>(blk + d * kI8Block + os) = ws[d];
+                    }
+                }
             }
         }
     } else {
@@ -922,7 +1075,16 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     const int nkb = G.nblk;
     const size_t beta_elems = tc ? (size_t)kn * n_cos * G.tiles_per_frame * nkb * kI8BlockSet
                                  : (size_t)kn * n_cos * G.cols_pad * G.t_pad;
-    if (tc) dev->beta_scale.ensure((size_t)kn * n_sel * n_cos * sizeof(double));
+    if (tc) {
+        // row scales, and the per-block maxima of the time table that bound them
+        dev->beta_scale.ensure((size_t)kn * n_sel * n_cos * sizeof(double));
+        dev->fact_Dmax.ensure((size_t)n_sel * nkb * (1 + SM) * 2 * sizeof(double));
+        const long warps = (long)n_sel * nkb;
+        k_time_maxima<<<(unsigned)((warps + 7) / 8), 256, 0, dev->stream>>>((const double*)dev->fact_D.p, n_sel, n_t,
+                                                                            nkb, 1 + SM, (double*)dev->fact_Dmax.p);
+        CUDA_OK(cudaGetLastError());
+        ++launches;
+    }
     dev->beta.ensure(beta_elems * sizeof(Real));
     if ((long)n_sel * 2 * S != G.cols_pad) {  // unused tile columns must read as zero
         // padding columns of the last tile are read by the GEMM: keep them zero
@@ -965,6 +1127,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         B.per_warp_bytes = (int)pw;
         B.tiles = G.tiles_per_frame;
         B.scale = tc ? (double*)dev->beta_scale.p : nullptr;
+        B.Dmax = tc ? (const double*)dev->fact_Dmax.p : nullptr;
         int warps = (int)std::min<size_t>(8, (200 * 1024) / pw);
         if (warps < 1) throw Error{"n_phi too large for the beta kernel"};
         const size_t smem = (size_t)warps * pw;

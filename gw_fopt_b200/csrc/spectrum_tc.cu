@@ -175,10 +175,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_i8(TcArgs A) {
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const int wt = blockIdx.x;
     const int w0 = wt * kTcWT;
-    // blockIdx.y = (frame, tile, part): part p takes the rows [i0, i1)
-    const int part_ = blockIdx.y % A.row_parts;
-    const int frame = blockIdx.y / A.row_parts / A.tiles_per_frame;
-    const int tile = (blockIdx.y / A.row_parts) % A.tiles_per_frame;
+    // blockIdx.y = (frame, part, tile), tile fastest: part p takes the rows [i0, i1).  CTAs
+    // resident together then share the time-phase digits of their rows (one part, many
+    // column tiles) and each column tile's beta (its frequency tiles) in L2.
+    const int tile = blockIdx.y % A.tiles_per_frame;
+    const int part_ = (blockIdx.y / A.tiles_per_frame) % A.row_parts;
+    const int frame = blockIdx.y / A.tiles_per_frame / A.row_parts;
     const int i0 = A.n_cos * part_ / A.row_parts, i1 = A.n_cos * (part_ + 1) / A.row_parts;
     const D4* B = A.bub + (size_t)frame * A.n_tot;
 

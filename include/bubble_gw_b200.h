@@ -37,11 +37,11 @@ typedef enum BgwxBoundaryCondition {
 /* Spectrum kernels.  FP64_DIRECT: plain FP64, one complex phase per
  * (bubble, cos-theta row, t, w), as the reference's loop nest.
  * FP64_FACTORED: FP64 with the time phase shared across bubbles (register
- * tiled).  MIXED: FP64 phase arguments with range reduction and FP64 final
- * sums, FP32 operands; the time-phase product runs on the tensor cores
- * (TF32 split in three products, FP32 accumulation per cos-theta row).
- * MIXED_SIMT: the same mixed form with the product on the FP32 CUDA cores
- * and FP32 partial sums folded into FP64 every 16 steps. */
+ * tiled).  MIXED: FP64 phases, tables and final sums; the time-phase product
+ * runs on the tensor cores as an exact integer product of four int8 digits
+ * per operand (relative error about 2^-33 of the operands' scales per term,
+ * n_t at most 32768).  MIXED_SIMT: FP32 operands with the product on the FP32
+ * CUDA cores and FP32 partial sums folded into FP64 every 16 steps. */
 typedef enum BgwxKernel {
     BGWX_KERNEL_FP64_DIRECT = 0,
     BGWX_KERNEL_FP64_FACTORED = 1,
