@@ -261,6 +261,7 @@ def run_b200(args):
     barrier()
     clocks = sampler.stop()
     launch_shape = g.last_launch_shape()
+    gemm_stages = g.last_gemm_stages()
     ms = max_over_ranks(e0.elapsed_time(e1), device="cuda")
     ms_step = ms / args.steps
     pte_total = cfg.pte * world
@@ -327,9 +328,15 @@ def run_b200(args):
         mp = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
         peak = 2.0 * mp["bf16_tflops_sustained"]
         achieved = 10.0 * gemm_flops / (tm["gemm_ms"] * 1e-3) / 1e12
+        # one launch covers frames_per_launch frames: their beta digits stream once, the time-phase
+        # digits are shared by the launch's frames
+        fpl = int(launch_shape[0]) if launch_shape and launch_shape[0] else 1
+        beta_bytes = 4.0 * cfg.n_cos * (cfg.n * 2 * S) * cfg.n_t
+        atab_bytes = 4.0 * cfg.n_cos * (2 * Wn) * cfg.n_t
         roofline = {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TOP/s (int8)",
-                    "frac": achieved / peak, "traffic": traffic * K if traffic else None,
-                    "traffic_unit": "DRAM bytes per step (per-frame ncu figure x frames)",
+                    "frac": achieved / peak, "traffic": traffic * fpl if traffic else None,
+                    "traffic_unit": "DRAM bytes per k_gemm_i8 launch (per-frame ncu figure x frames per launch)",
+                    "algorithmic_bytes_per_launch": fpl * beta_bytes + atab_bytes,
                     "traffic_source": traffic_note, "kernel": "k_gemm_i8",
                     "work": "10 digit-pair products x 2 x (2 n_w) x n_t x columns x n_cos int8 ops per frame",
                     "algorithmic_tflops": gemm_flops / (tm["gemm_ms"] * 1e-3) / 1e12,
@@ -347,7 +354,9 @@ def run_b200(args):
             kname = "k_spec_direct + k_reduce"
             work = "counted F = 6 PTE + 8 Phi + 20 Phi_t per step"
         roofline = {"bound": bound, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                    "frac": (achieved / peak) if achieved else None, "traffic": traffic * K if traffic else None,
+                    "frac": (achieved / peak) if achieved else None,
+                    "traffic": traffic * (int(launch_shape[0]) if launch_shape and launch_shape[0] else 1)
+                    if traffic else None, "traffic_unit": "DRAM bytes per launch",
                     "traffic_source": traffic_note, "kernel": kname,
                     "work": work, "peak_source": "of measured: bgwx_measure_compute_peaks (FMA chains on this GPU); "
                                                  "MEASURED_PEAKS.json holds HBM/bf16 only",
@@ -365,7 +374,7 @@ def run_b200(args):
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"khat-shard x{world}",
                        "tables": "time-phase digits rebuilt in every call (inside the timed steps)",
                        "launch_shape": dict(zip(("frames_per_launch", "row_parts"), launch_shape),
-                                            autotuned=not args.no_autotune)},
+                                            gemm_stages=gemm_stages, autotuned=not args.no_autotune)},
             "roofline": roofline, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
             "compare": compare}
     if compare:

@@ -25,7 +25,8 @@
 // Kernels:
 //   k_adj_mtab    the time-phase table M_i(w, k), once per call
 //   k_adj_pq      per (frame, row): Re P and Im Q as two real products of depth W
-//   k_adj_rows    one warp per (frame, bubble, row): the patch sums above, dL/dtau per patch
+//   k_adj_rows    one warp per (frame, bubble, row): the patch sums above in event form (suffix
+//                 sums over the steps read at each patch's collision step), dL/dtau per patch
 //   k_adj_bubble  per (frame, bubble): the row partials of t_a and z_a
 //   k_adj_geom    per (frame, bubble, patch): dL/dtau -> both bubbles of the collision, and the
 //                 bubble parts above, summed as fixed-point integers (deterministic; two passes:
@@ -198,24 +199,61 @@ __global__ void k_adj_ttab(const D4* __restrict__ bub, const uint32_t* __restric
     for (int m = 0; m < SM; ++m) row[4 + m] = on ? exp(-powers[m] * log(dtk)) * e : 0.0;
 }
 
+// ---------------------------------------------------------------------------
+// Row sums in event form.  The time grid is non-decreasing (t_begin <= t_end),
+// so dt_k = t_k - t_a is too, and the collided steps of patch j are the
+// suffix k >= kc_j: kc_j is the first step with dt_k >= tau_j (n_t when
+// tau_j <= 0 or the wall is never reached).  Every double sum over (patch j,
+// step k) of the direct form is then sum_j X_j . Y(kc_j), Y(k) = sum_{k'>=k}
+// y_k' a suffix sum of per-step vectors.  Per step k (zero where dt_k <= 0),
+// with g = 0, 1 the cos 2phi and sin 2phi weights, s_q the set of term q,
+// be_q = dt^{-p_q} e^{-dt/w} and c1_q = -p_q/dt - 1/w:
+//   T[g,q] = pre bb[g,s_q] be_q (3 d2 + d3 c1_q) + c_i Z[g,q]
+//   Z[g,q] = pd3 iq[g,s_q] be_q,   B[g,q] = pd3 bb[g,s_q] be_q,   L[g,q] = B[g,q] ln dt
+//   U[g]   = 3 pre d2 sum_s bb[g,s] + c_i V[g],   V[g] = pd3 sum_s iq[g,s]
+// and with x_jg = q_g(j), y_jq = tau_j^{p_q} e^{tau_j/w} (a_q r^p D = a_q y_jq be_q):
+//   acc_t  -= sum_j sum_g x_jg [sum_q a_q y_jq T(kc_j) + U(0) - U(kc_j)]
+//   acc_z  += sum_j sum_g x_jg [sum_q a_q y_jq Z(kc_j) + V(0) - V(kc_j)]
+//   tbar_j  = sum_g x_jg sum_q a_q y_jq (p_q/tau_j + 1/w) B(kc_j)
+//   abar_q += sum_j sum_g x_jg y_jq B(kc_j)
+//   pbar_q += a_q sum_j sum_g x_jg y_jq (ln tau_j B(kc_j) - L(kc_j))
+// One warp per (frame, bubble, row) walks the steps in chunks of 32 from the
+// last (lane = step): a warp suffix scan of each component plus the carry of
+// the later chunks, the chunk's suffix sums to shared memory, and each patch
+// whose kc_j falls in the chunk reads its entry once.  Work per row is
+// O(n_t + n_phi) where the direct form is O(n_t n_phi).
+constexpr int kRowWarps = 4;
+
+template <int SMC>
+__host__ __device__ constexpr int row_components() {
+    return 8 * SMC + 4;
+}
+
 template <int S, int SMC, int JPL>
-__global__ void __launch_bounds__(kAdjThreads) k_adj_rows(AdjArgs A, const double* __restrict__ tt) {
+__global__ void __launch_bounds__(32 * kRowWarps) k_adj_rows(AdjArgs A, const double* __restrict__ tt) {
     constexpr int S2 = 2 * S;
+    constexpr int M = SMC / S;
     constexpr int TW = 4 + SMC;
+    constexpr int C = row_components<SMC>();
+    constexpr int oT = 0, oZ = 2 * SMC, oB = 4 * SMC, oL = 6 * SMC, oU = 8 * SMC, oV = 8 * SMC + 2;
+    extern __shared__ double rows_smem[];
+    const unsigned full = 0xffffffffu;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const long row = (long)blockIdx.x * (blockDim.x >> 5) + warp;
+    double* sw = rows_smem + (size_t)warp * C * 32;  // [component][step in chunk]
+    const long row = (long)blockIdx.x * kRowWarps + warp;
     const long R = (long)A.n_sel * A.n_cos;  // rows per frame
     const int f = (int)(row / R);
     if (f >= A.kn) return;
     const int slot = (int)((row % R) / A.n_cos);
     const int i = (int)(row % A.n_cos);
-    const int M = A.M;
+    const int n_t = A.n_t;
     const int nd = A.n_cos * A.n_phi;
     const double ta = A.bub[(size_t)f * A.n_tot + A.sel[slot]].t;
     const double ci = A.cos_t[i];
     const double vi = (i == 0 || i == A.n_cos - 1) ? 0.5 : 1.0;
     const double rowc = 0.5 * (1.0 - ci * ci) * A.dphi * A.dcos * vi * A.dt / (6.0 * M_PI);
     const double invw = A.has_damp ? 1.0 / A.damp : 0.0;
+    const size_t pbase = ((size_t)f * A.n_sel + slot) * nd + (size_t)i * A.n_phi;
 
     double a_c[SMC], p_c[SMC];
 #pragma unroll
@@ -223,116 +261,163 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_rows(AdjArgs A, const doubl
         a_c[q] = A.coeffs[q];
         p_c[q] = A.powers[q];
     }
-    // per-patch factors of this lane's patches j = lane + 32 jj
-    double tau_j[JPL], q0[JPL], q1[JPL], tbar[JPL], lt[JPL], al[JPL][SMC], c2[JPL][SMC];
+    // collision step of this lane's patches j = lane + 32 jj (a monotone predicate: binary search)
+    double tau_j[JPL], tbar[JPL];
+    int kc[JPL];
+    double xs0 = 0.0, xs1 = 0.0;  // sum over the lane's patches of the two weights
 #pragma unroll
     for (int jj = 0; jj < JPL; ++jj) {
         const int j = lane + 32 * jj;
-        const bool ok = j < A.n_phi;
-        const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
-        const double tj = ok ? A.tau[((size_t)f * A.n_sel + slot) * nd + (size_t)i * A.n_phi + j] : 0.0;
+        const double tj = j < A.n_phi ? A.tau[pbase + j] : 0.0;
         tau_j[jj] = tj;
-        q0[jj] = ok ? wj * A.cos2[j] : 0.0;
-        q1[jj] = ok ? wj * A.sin2[j] : 0.0;
         tbar[jj] = 0.0;
-        const bool pos = tj > 0.0;
-        lt[jj] = pos ? log(tj) : 0.0;
-        const double et = (pos && A.has_damp) ? exp(tj * invw) : 1.0;
-#pragma unroll
-        for (int q = 0; q < SMC; ++q) {
-            al[jj][q] = pos ? exp(p_c[q] * lt[jj]) * et : 0.0;
-            c2[jj][q] = pos ? p_c[q] / tj + invw : 0.0;
+        int lo = n_t;
+        if (tj > 0.0) {
+            lo = 0;
+            int hi = n_t;
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (A.t_arr[mid] - ta >= tj) hi = mid;
+                else lo = mid + 1;
+            }
+        }
+        kc[jj] = lo;
+        if (j < A.n_phi) {
+            const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
+            xs0 += wj * A.cos2[j];
+            xs1 += wj * A.sin2[j];
         }
     }
+    // first step after the bubble's nucleation (dt_k > 0)
+    int k0 = 0;
+    {
+        int hi = n_t;
+        while (k0 < hi) {
+            const int mid = (k0 + hi) >> 1;
+            if (A.t_arr[mid] - ta > 0.0) hi = mid;
+            else k0 = mid + 1;
+        }
+    }
+
+    // sw[32 c] holds the suffix sum of component c from the start of the last chunk
+    // done (the carry into the next one): zero before the first
+#pragma unroll
+    for (int c = 0; c < C; ++c) sw[c * 32 + lane] = 0.0;
+    __syncwarp();
     double acc_t = 0.0, acc_z = 0.0, abar[SMC], pbar[SMC];
 #pragma unroll
     for (int q = 0; q < SMC; ++q) abar[q] = pbar[q] = 0.0;
 
     const size_t base = ((size_t)f * A.n_sel + slot) * A.n_cos + i;
-    const double* trow = tt + (size_t)slot * A.n_t * TW;
-    for (int k = 0; k < A.n_t; ++k) {
-        const double dtk = A.t_arr[k] - ta;
-        if (!(dtk > 0.0)) continue;
-        const double* tk = trow + (size_t)k * TW;
-        const double d2 = tk[0], d3 = tk[1], ld = tk[2], invd = tk[3];
-        double be[SMC], c1[SMC];
+    const double* trow = tt + (size_t)slot * n_t * TW;
+    for (int c0 = ((n_t - 1) >> 5) << 5; c0 >= (k0 & ~31); c0 -= 32) {
+        const int k = c0 + lane;
+        double y[C];
 #pragma unroll
-        for (int q = 0; q < SMC; ++q) {
-            be[q] = tk[4 + q];
-            c1[q] = -p_c[q] * invd - invw;
-        }
-        const double uk = (k == 0 || k == A.n_t - 1) ? 0.5 : 1.0;
-        const double pre = rowc * uk * A.cutw[k];
-        const double pd3 = pre * d3;
-        const size_t o = (base * A.n_t + k) * S2;
-        double bb[S2], iq[S2];
+        for (int c = 0; c < C; ++c) y[c] = 0.0;
+        if (k >= k0 && k < n_t) {
+            const double* tk = trow + (size_t)k * TW;
+            const double d2 = tk[0], d3 = tk[1], ld = tk[2], invd = tk[3];
+            const double uk = (k == 0 || k == n_t - 1) ? 0.5 : 1.0;
+            const double pre = rowc * uk * A.cutw[k];
+            const double pd3 = pre * d3;
+            const size_t o = (base * n_t + k) * S2;
+            double bb[S2], iq[S2];
 #pragma unroll
-        for (int g = 0; g < S2; ++g) {
-            bb[g] = A.s.bbar[o + g];
-            iq[g] = A.s.imq[o + g];
-        }
-#pragma unroll
-        for (int jj = 0; jj < JPL; ++jj) {
-            double Bs[S], Is[S];
-#pragma unroll
-            for (int s = 0; s < S; ++s) {
-                Bs[s] = bb[s] * q0[jj] + bb[S + s] * q1[jj];
-                Is[s] = iq[s] * q0[jj] + iq[S + s] * q1[jj];
+            for (int g = 0; g < S2; ++g) {
+                bb[g] = A.s.bbar[o + g];
+                iq[g] = A.s.imq[o + g];
             }
-            const double tj = tau_j[jj];
-            // the reference's status test (generalized_bulk_flow.rs:405)
-            if (tj > 0.0 && dtk >= tj) {
-                double fs[S], dfdt[S], dfdtau[S];
 #pragma unroll
-                for (int s = 0; s < S; ++s) fs[s] = dfdt[s] = dfdtau[s] = 0.0;
+            for (int g = 0; g < 2; ++g) {
+                double sb = 0.0, si = 0.0;
+#pragma unroll
+                for (int s = 0; s < S; ++s) {
+                    sb += bb[g * S + s];
+                    si += iq[g * S + s];
+                }
+                y[oV + g] = pd3 * si;
+                y[oU + g] = 3.0 * pre * d2 * sb + ci * y[oV + g];
 #pragma unroll
                 for (int q = 0; q < SMC; ++q) {
                     const int s = q / M;
-                    const double rpD = al[jj][q] * be[q];
-                    const double e = a_c[q] * rpD;
-                    fs[s] += e;
-                    dfdt[s] += e * c1[q];
-                    dfdtau[s] += e * c2[jj][q];
-                    const double wgt = pd3 * Bs[s] * rpD;
-                    abar[q] += wgt;
-                    pbar[q] += wgt * a_c[q] * (lt[jj] - ld);
+                    const double be = tk[4 + q];
+                    const double c1 = -p_c[q] * invd - invw;
+                    const double zq = pd3 * iq[g * S + s] * be;
+                    const double bq = pd3 * bb[g * S + s] * be;
+                    y[oZ + g * SMC + q] = zq;
+                    y[oB + g * SMC + q] = bq;
+                    y[oL + g * SMC + q] = bq * ld;
+                    y[oT + g * SMC + q] = pre * bb[g * S + s] * be * (3.0 * d2 + d3 * c1) + ci * zq;
                 }
-                double st = 0.0, sz = 0.0, sx = 0.0;
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    st += Bs[s] * (3.0 * d2 * fs[s] + d3 * dfdt[s]);
-                    sz += Is[s] * fs[s];
-                    sx += Bs[s] * dfdtau[s];
-                }
-                acc_t -= pre * st + ci * pd3 * sz;
-                acc_z += pd3 * sz;
-                tbar[jj] += pd3 * sx;
-            } else {
-                double sb = 0.0, sz = 0.0;
-#pragma unroll
-                for (int s = 0; s < S; ++s) {
-                    sb += Bs[s];
-                    sz += Is[s];
-                }
-                acc_t -= 3.0 * pre * d2 * sb + ci * pd3 * sz;
-                acc_z += pd3 * sz;
             }
         }
+        // inclusive suffix sums within the chunk, then the later chunks' total
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+#pragma unroll
+            for (int c = 0; c < C; ++c) {
+                const double v = __shfl_down_sync(full, y[c], off);
+                if (lane + off < 32) y[c] += v;
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < C; ++c) y[c] += sw[c * 32];
+        __syncwarp();
+#pragma unroll
+        for (int c = 0; c < C; ++c) sw[c * 32 + lane] = y[c];
+        __syncwarp();
+#pragma unroll
+        for (int jj = 0; jj < JPL; ++jj) {
+            const int kj = kc[jj];
+            if (kj < c0 || kj >= c0 + 32 || kj >= n_t) continue;
+            const double* e = sw + (kj - c0);  // component c at e[32 c]
+            const int j = lane + 32 * jj;
+            const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
+            const double x0 = wj * A.cos2[j], x1 = wj * A.sin2[j];
+            // the uncollided steps k < kc_j: the totals U(0) and V(0) are added after the loop
+            acc_t += x0 * e[32 * oU] + x1 * e[32 * (oU + 1)];
+            acc_z -= x0 * e[32 * oV] + x1 * e[32 * (oV + 1)];
+            const double tj = tau_j[jj];
+            const double lt = log(tj);
+            const double et = A.has_damp ? exp(tj * invw) : 1.0;
+            double tb = 0.0;
+#pragma unroll
+            for (int q = 0; q < SMC; ++q) {
+                const double yq = exp(p_c[q] * lt) * et;
+                const double c2 = p_c[q] / tj + invw;
+                const double Tx = x0 * e[32 * (oT + q)] + x1 * e[32 * (oT + SMC + q)];
+                const double Zx = x0 * e[32 * (oZ + q)] + x1 * e[32 * (oZ + SMC + q)];
+                const double Bx = x0 * e[32 * (oB + q)] + x1 * e[32 * (oB + SMC + q)];
+                const double Lx = x0 * e[32 * (oL + q)] + x1 * e[32 * (oL + SMC + q)];
+                const double ay = a_c[q] * yq;
+                acc_t -= ay * Tx;
+                acc_z += ay * Zx;
+                tb += ay * c2 * Bx;
+                abar[q] += yq * Bx;
+                pbar[q] += a_c[q] * yq * (lt * Bx - Lx);
+            }
+            tbar[jj] = tb;
+        }
+        __syncwarp();
     }
+    // every patch's uncollided part starts from the totals U(0), V(0)
+    acc_t -= xs0 * sw[32 * oU] + xs1 * sw[32 * (oU + 1)];
+    acc_z += xs0 * sw[32 * oV] + xs1 * sw[32 * (oV + 1)];
 #pragma unroll
     for (int jj = 0; jj < JPL; ++jj) {
         const int j = lane + 32 * jj;
-        if (j < A.n_phi) A.s.taubar[((size_t)f * A.n_sel + slot) * nd + (size_t)i * A.n_phi + j] = tbar[jj];
+        if (j < A.n_phi) A.s.taubar[pbase + j] = tbar[jj];
     }
     // fixed-order warp reduction of the row partials
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
-        acc_t += __shfl_down_sync(0xffffffffu, acc_t, off);
-        acc_z += __shfl_down_sync(0xffffffffu, acc_z, off);
+        acc_t += __shfl_down_sync(full, acc_t, off);
+        acc_z += __shfl_down_sync(full, acc_z, off);
 #pragma unroll
         for (int q = 0; q < SMC; ++q) {
-            abar[q] += __shfl_down_sync(0xffffffffu, abar[q], off);
-            pbar[q] += __shfl_down_sync(0xffffffffu, pbar[q], off);
+            abar[q] += __shfl_down_sync(full, abar[q], off);
+            pbar[q] += __shfl_down_sync(full, pbar[q], off);
         }
     }
     if (lane == 0) {
@@ -561,8 +646,9 @@ __global__ void k_adj_params(AdjArgs A, long n_rows) {
 // ---------------------------------------------------------------------------
 template <int S, int SMC, int JPL>
 static void launch_rows(const AdjArgs& A, long rows, cudaStream_t st, const double* tt) {
-    const int warps = kAdjThreads / 32;
-    k_adj_rows<S, SMC, JPL><<<(unsigned)((rows + warps - 1) / warps), kAdjThreads, 0, st>>>(A, tt);
+    const size_t smem = (size_t)kRowWarps * row_components<SMC>() * 32 * sizeof(double);
+    static_assert(kRowWarps * row_components<4>() * 32 * sizeof(double) <= 48 * 1024, "row kernel shared memory");
+    k_adj_rows<S, SMC, JPL><<<(unsigned)((rows + kRowWarps - 1) / kRowWarps), 32 * kRowWarps, smem, st>>>(A, tt);
 }
 
 template <int S, int SMC>

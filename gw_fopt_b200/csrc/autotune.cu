@@ -1,18 +1,20 @@
 // Measured launch shape of the factored spectrum kernels.
 //
-// Two knobs set how a spectrum call is cut into launches: the number of k-hat
+// Three knobs set how a spectrum call is cut into launches: the number of k-hat
 // frames per launch (each launch runs masks, beta and the GEMM over that many
 // frames; the memory budget gives the largest) and, for the tensor-core GEMM,
 // the number of cos-theta row parts each (frequency tile, column tile) is
-// split into (the wave-fill model picks one).  The tuner times a few
-// candidates around the automatic choice on a sample of the job's own frames
-// and keeps the fastest per frame.  Every candidate computes the same spectrum:
-// frames are independent and the row parts only regroup FP64 partial sums.
+// split into (the wave-fill model picks one) and its pipeline stages (3 to 5
+// stages of 32 steps).  The tuner times a few candidates around the automatic
+// choice on a sample of the job's own frames, keeps the fastest shape, then
+// times the stage counts at that shape.  Every candidate computes the same
+// spectrum: frames are independent, the row parts only regroup FP64 partial
+// sums and the stages only change the overlap of copies and MMAs.
 //
 // Choices are keyed by the device (name, multiprocessor count) and every size
 // the launch shapes depend on; they live for the process and, when
 // BGWX_AUTOTUNE_CACHE names a file, are read from and appended to that file
-// (one "key frames row_parts" line per shape).
+// (one "key frames row_parts stages" line per shape).
 
 #include <cuda_runtime.h>
 
@@ -52,9 +54,10 @@ void load_locked() {
     while (std::getline(in, line)) {
         std::istringstream ls(line);
         std::string key;
-        long long f = 0, r = 0;
+        long long f = 0, r = 0, st = 0;
         if (!(ls >> key >> f >> r) || f < 1 || r < 1 || r > 16) continue;  // malformed lines are skipped
-        g_cache[key] = LaunchShape{(size_t)f, (int)r};
+        if (!(ls >> st) || st < 3 || st > 5) st = 0;                       // older lines: automatic stages
+        g_cache[key] = LaunchShape{(size_t)f, (int)r, (int)st};
     }
 }
 
@@ -62,7 +65,7 @@ void append_locked(const std::string& key, const LaunchShape& s) {
     const char* path = cache_file();
     if (!path) return;
     std::ofstream out(path, std::ios::app);
-    if (out) out << key << ' ' << s.frames_per_launch << ' ' << s.row_parts << '\n';
+    if (out) out << key << ' ' << s.frames_per_launch << ' ' << s.row_parts << ' ' << s.gemm_stages << '\n';
 }
 
 std::string shape_key(const Device* dev, const SpectrumJob& job) {
@@ -160,6 +163,25 @@ LaunchShape autotune_launch_shape(Device* dev, const SpectrumJob& job) {
             }
         }
         if (best.frames_per_launch == 0) throw Error{"autotune: every candidate launch shape failed: " + last_err};
+        if (job.kernel == BGWX_KERNEL_MIXED) {
+            // the GEMM's pipeline stages at the chosen shape (4 was among the timed runs)
+            best.gemm_stages = 4;
+            sub.frames_per_launch = best.frames_per_launch;
+            sub.row_parts = best.row_parts;
+            for (int stg : {3, 5}) {
+                sub.gemm_stages = stg;
+                float ms = 0.0f;
+                try {
+                    ms = time_run(dev, sub, out);
+                } catch (const Error&) {
+                    continue;
+                }
+                if (ms < best_ms) {
+                    best_ms = ms;
+                    best.gemm_stages = stg;
+                }
+            }
+        }
     } catch (...) {
         cudaStreamSynchronize(dev->stream);
         cudaFree(out);

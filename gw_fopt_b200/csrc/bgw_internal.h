@@ -61,16 +61,19 @@ struct SpectrumJob {
     size_t n_k = 1;
     BgwxKernel kernel = BGWX_KERNEL_FP64_DIRECT;
     // launch shape; 0 = automatic (frames per launch from the memory budget,
-    // row parts from the wave-fill model).  frames_per_launch is capped by the
-    // budget; row_parts applies to the tensor-core GEMM only (at most 16).
+    // row parts from the wave-fill model, 4 GEMM stages).  frames_per_launch is
+    // capped by the budget; row_parts (at most 16) and gemm_stages (3 to 5)
+    // apply to the tensor-core GEMM only.
     size_t frames_per_launch = 0;
     int row_parts = 0;
+    int gemm_stages = 0;
 };
 
 // The launch shape a spectrum call used (or is to use).
 struct LaunchShape {
     size_t frames_per_launch = 0;
     int row_parts = 0;
+    int gemm_stages = 0;
 };
 
 struct MaskJob {

@@ -35,7 +35,7 @@ struct bgw_generalized_bulk_flow {
     size_t num_threads = 1;
     BgwxKernel kernel = BGWX_KERNEL_FP64_DIRECT;
     // launch shape of spectrum calls: fixed (non-zero), measured (autotune) or automatic
-    size_t frames_per_launch = 0, row_parts = 0;
+    size_t frames_per_launch = 0, row_parts = 0, gemm_stages = 0;
     bool autotune = false;
     bgw::Device* dev = nullptr;
     BgwxTimings timings{};
@@ -184,13 +184,15 @@ bgw::SpectrumJob settings_job(const bgw_generalized_bulk_flow* h, const std::vec
 // The handle's launch shape into a spectrum job: a fixed shape when one is
 // set, else the measured one when autotuning is on, else automatic.
 void apply_launch_shape(bgw_generalized_bulk_flow* h, bgw::SpectrumJob& job) {
-    if (h->frames_per_launch || h->row_parts) {
+    if (h->frames_per_launch || h->row_parts || h->gemm_stages) {
         job.frames_per_launch = h->frames_per_launch;
         job.row_parts = (int)h->row_parts;
+        job.gemm_stages = (int)h->gemm_stages;
     } else if (h->autotune) {
         const bgw::LaunchShape s = bgw::autotune_launch_shape(device(h), job);
         job.frames_per_launch = s.frames_per_launch;
         job.row_parts = s.row_parts;
+        job.gemm_stages = s.gemm_stages;
     }
 }
 
@@ -814,6 +816,22 @@ BgwStatus bgwx_generalized_bulk_flow_set_launch_shape(bgw_generalized_bulk_flow*
         if (row_parts > 16) throw Error{"row_parts must be at most 16"};
         h->frames_per_launch = frames_per_launch;
         h->row_parts = row_parts;
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_set_gemm_stages(bgw_generalized_bulk_flow* bulk_flow, size_t stages) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        if (stages != 0 && (stages < 3 || stages > 5)) throw Error{"gemm stages must be 0 (automatic) or 3 to 5"};
+        h->gemm_stages = stages;
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_last_gemm_stages(const bgw_generalized_bulk_flow* bulk_flow, size_t* out_stages) {
+    return run_ffi([&] {
+        if (!bulk_flow) throw Error{"bulk_flow must not be null"};
+        if (!out_stages) throw Error{"outputs must not be null"};
+        *out_stages = bulk_flow->dev ? (size_t)bgw::last_launch_shape(bulk_flow->dev).gemm_stages : 0;
     });
 }
 

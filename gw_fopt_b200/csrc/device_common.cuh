@@ -88,6 +88,7 @@ struct Device {
     DevBuf adj_gbar, adj_scratch, adj_grad, adj_mtab; // adjoint: cotangents, work arrays, gradients, phases
     size_t last_frames_per_launch = 0;               // launch shape of the last spectrum call
     int last_row_parts = 0;
+    int last_gemm_stages = 0;
     ~Device();
 };
 

@@ -566,6 +566,7 @@ LaunchShape last_launch_shape(const Device* dev) {
     LaunchShape s;
     s.frames_per_launch = dev->last_frames_per_launch;
     s.row_parts = dev->last_row_parts;
+    s.gemm_stages = dev->last_gemm_stages;
     return s;
 }
 
@@ -645,6 +646,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     if (job.frames_per_launch) kc = std::min(kc, job.frames_per_launch);
     dev->last_frames_per_launch = kc;
     dev->last_row_parts = job.kernel == BGWX_KERNEL_FP64_DIRECT ? 1 : 0;  // the factored launch records its own
+    dev->last_gemm_stages = 0;
     dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
     if (job.kernel == BGWX_KERNEL_FP64_DIRECT) dev->partial.ensure(kc * job.n_sel * per * sizeof(double2));
     double2* final_out = out_is_device ? reinterpret_cast<double2*>(out) : nullptr;

@@ -1207,6 +1207,8 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         T.bpt = G.bpt;
         T.tiles_per_frame = G.tiles_per_frame;
         T.row_parts = row_parts;
+        T.stages = job.gemm_stages > 0 ? job.gemm_stages : 4;
+        dev->last_gemm_stages = T.stages;
         T.partial = A.partial;
         T.err = reinterpret_cast<unsigned int*>(static_cast<unsigned char*>(dev->counters.p) + 8);
         launch_gemm_tc(T, kn, dev->stream);

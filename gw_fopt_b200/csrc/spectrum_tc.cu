@@ -66,17 +66,18 @@ constexpr int kTcRows = 128;     // GEMM rows: 64 frequencies x (Re, Im)
 constexpr int kTcWT = 64;        // frequencies per CTA
 constexpr int kTcCols = 128;     // GEMM columns per CTA
 constexpr int kTcKB = 32;        // time steps per stage (32 bytes of int8)
-constexpr int kTcStages = 4;
 constexpr int kTcWarps = 10;
 constexpr int kTcThreads = 32 * kTcWarps;
 constexpr uint32_t kTmemCols = 512;
 constexpr int kStageBytes = 2 * kI8BlockSet;  // A digits, B digits
 
+// Shared memory of a GEMM CTA with ST pipeline stages (3 to 5 fit next to the phase table).
+template <int ST>
 struct SmemLayout {
     static constexpr int stages = 0;
-    static constexpr int etab = kTcStages * kStageBytes;       // double2[64 w][64 bubbles], XOR-swizzled
-    static constexpr int bars = etab + 64 * 64 * 16;          // full[S], empty[S], accf, acce, drain
-    static constexpr int n_bars = 2 * kTcStages + 3;
+    static constexpr int etab = ST * kStageBytes;              // double2[64 w][64 bubbles], XOR-swizzled
+    static constexpr int bars = etab + 64 * 64 * 16;          // full[ST], empty[ST], accf, acce, drain
+    static constexpr int n_bars = 2 * ST + 3;
     static constexpr int tslot = bars + 8 * n_bars;
     static constexpr int abort_flag = tslot + 4;
     static constexpr int binfo = tslot + 16;                   // int[64]
@@ -84,7 +85,7 @@ struct SmemLayout {
     static constexpr int bz = bt + 64 * 8;                     // double[64]
     static constexpr int total = bz + 64 * 8;
 };
-static_assert(SmemLayout::total + 1024 <= 227 * 1024, "shared memory budget");
+static_assert(SmemLayout<5>::total + 1024 <= 227 * 1024, "shared memory budget");
 
 // Phase-table slot of (frequency l, bubble b): rows of 64 bubbles, the bubble
 // index XORed with l % 8 so that the 16 frequencies read by a warp fall in
@@ -154,8 +155,10 @@ __global__ void k_tc_phase_table(const double* __restrict__ w, const double* __r
     for (int s = 0; s < kI8Slices; ++s) out[(size_t)s * kI8Block] = (int8_t)(d >> (8 * s));
 }
 
-template <int S>
+template <int S, int ST>
 __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_i8(TcArgs A) {
+    constexpr int kTcStages = ST;
+    using SmemLayout = bgw::SmemLayout<ST>;
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     unsigned char* sm = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) &
                                                          ~static_cast<uintptr_t>(1023));
@@ -434,10 +437,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_i8(TcArgs A) {
     }
 }
 
+template <int S, int ST>
+void launch_st(const TcArgs& A, dim3 grid, cudaStream_t st) {
+    const size_t smem = SmemLayout<ST>::total + 1024;
+    CUDA_OK(cudaFuncSetAttribute(k_gemm_i8<S, ST>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_gemm_i8<S, ST><<<grid, kTcThreads, smem, st>>>(A);
+}
+
 template <int S>
-void launch_s(const TcArgs& A, dim3 grid, size_t smem, cudaStream_t st) {
-    CUDA_OK(cudaFuncSetAttribute(k_gemm_i8<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_gemm_i8<S><<<grid, kTcThreads, smem, st>>>(A);
+void launch_s(const TcArgs& A, dim3 grid, cudaStream_t st) {
+    switch (A.stages) {
+        case 3: launch_st<S, 3>(A, grid, st); break;
+        case 5: launch_st<S, 5>(A, grid, st); break;
+        default: launch_st<S, 4>(A, grid, st); break;
+    }
 }
 
 }  // namespace
@@ -472,19 +485,19 @@ void launch_gemm_tc(const TcArgs& A, size_t kn, cudaStream_t st) {
     if (A.bpt * 2 * A.S > kTcCols) throw Error{"tensor-core GEMM: too many columns per tile"};
     if (A.row_parts < 1 || A.row_parts > A.n_cos) throw Error{"tensor-core GEMM: bad row split"};
     if (A.n_t > kI8MaxSteps) throw Error{"the mixed kernel accumulates at most 32768 time steps exactly; use fp64_factored"};
-    const size_t smem = SmemLayout::total + 1024;
+    if (A.stages != 0 && (A.stages < 3 || A.stages > 5)) throw Error{"tensor-core GEMM: 3 to 5 pipeline stages"};
     const size_t gy = kn * (size_t)A.tiles_per_frame * A.row_parts;
     if (gy > 65535) throw Error{"too many column tiles in one k-hat chunk"};
     dim3 grid((unsigned)A.n_wt, (unsigned)gy);
     switch (A.S) {
-        case 1: launch_s<1>(A, grid, smem, st); break;
-        case 2: launch_s<2>(A, grid, smem, st); break;
-        case 3: launch_s<3>(A, grid, smem, st); break;
-        case 4: launch_s<4>(A, grid, smem, st); break;
-        case 5: launch_s<5>(A, grid, smem, st); break;
-        case 6: launch_s<6>(A, grid, smem, st); break;
-        case 7: launch_s<7>(A, grid, smem, st); break;
-        case 8: launch_s<8>(A, grid, smem, st); break;
+        case 1: launch_s<1>(A, grid, st); break;
+        case 2: launch_s<2>(A, grid, st); break;
+        case 3: launch_s<3>(A, grid, st); break;
+        case 4: launch_s<4>(A, grid, st); break;
+        case 5: launch_s<5>(A, grid, st); break;
+        case 6: launch_s<6>(A, grid, st); break;
+        case 7: launch_s<7>(A, grid, st); break;
+        case 8: launch_s<8>(A, grid, st); break;
         default: throw Error{"tensor-core GEMM supports at most 8 coefficient sets"};
     }
     CUDA_OK(cudaGetLastError());

@@ -67,6 +67,7 @@ struct TcArgs {
     int bpt;                // bubbles per 128-column tile
     int tiles_per_frame;
     int row_parts;          // CTAs per (frequency tile, column tile), each over a range of cos-theta rows
+    int stages;             // pipeline stages of 32 steps (3 to 5; 0: 4)
     double2* partial;       // (kn, tiles_per_frame, row_parts, 2, S, W)
     unsigned int* err;      // set non-zero when a pipeline wait gave up
 };

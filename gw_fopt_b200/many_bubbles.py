@@ -562,6 +562,17 @@ class GeneralizedBulkFlow:
         _call(L.lib().bgwx_generalized_bulk_flow_last_launch_shape(self._h, C.byref(f), C.byref(r)))
         return int(f.value), int(r.value)
 
+    def set_gemm_stages(self, stages: int = 0) -> None:
+        """Pipeline stages of the mixed kernel's tensor-core GEMM (B200 extension): 3, 4 or 5,
+        or 0 for the automatic (or autotuned) choice.  The result does not depend on it."""
+        _call(L.lib().bgwx_generalized_bulk_flow_set_gemm_stages(self._h, int(stages)))
+
+    def last_gemm_stages(self) -> int:
+        """GEMM stages of the last spectrum call (0 when it did not run the tensor-core GEMM)."""
+        n = C.c_size_t(0)
+        _call(L.lib().bgwx_generalized_bulk_flow_last_gemm_stages(self._h, C.byref(n)))
+        return int(n.value)
+
     # --- geometry -------------------------------------------------------------
     def _require_res(self, name="n_cos_thetax"):
         if self._n_cos is None:

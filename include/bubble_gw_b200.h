@@ -112,7 +112,8 @@ BgwStatus bgwx_generalized_bulk_flow_set_launch_shape(bgw_generalized_bulk_flow 
 /* Measured launch shapes: with enabled, the first spectrum call of each problem
  * shape (device, kernel, bubble counts, grids, coefficient sets) on a factored
  * kernel times candidate shapes around the automatic one on its own first
- * frames and keeps the fastest for the process; with the environment variable
+ * frames (frames per launch, GEMM row parts, then the mixed kernel's GEMM
+ * stages) and keeps the fastest for the process; with the environment variable
  * BGWX_AUTOTUNE_CACHE naming a file, choices are also read from and appended
  * to it.  The FP64 direct kernel has no tunable shape.  Off by default.
  * No counterpart in the reference. */
@@ -122,6 +123,16 @@ BgwStatus bgwx_generalized_bulk_flow_set_autotune(bgw_generalized_bulk_flow *bul
  * launch, GEMM row parts; zeros before the first call).  No counterpart. */
 BgwStatus bgwx_generalized_bulk_flow_last_launch_shape(const bgw_generalized_bulk_flow *bulk_flow,
                                                        size_t *out_frames_per_launch, size_t *out_row_parts);
+
+/* Pipeline stages of 32 time steps in the mixed kernel's tensor-core GEMM:
+ * 3, 4 or 5 (0 = automatic: 4, or the autotuner's measured choice).  The
+ * stage count changes only the overlap of copies and MMAs, not the result.
+ * No counterpart in the reference. */
+BgwStatus bgwx_generalized_bulk_flow_set_gemm_stages(bgw_generalized_bulk_flow *bulk_flow, size_t stages);
+
+/* GEMM stages of the last spectrum call (0 when it did not run the mixed
+ * kernel's GEMM).  No counterpart in the reference. */
+BgwStatus bgwx_generalized_bulk_flow_last_gemm_stages(const bgw_generalized_bulk_flow *bulk_flow, size_t *out_stages);
 
 /* First-collider codes (-1 None, i Interior(i), -(i+2) Exterior(i)) and the
  * collision delays of compute_delta_tab for interior bubbles [a_begin, a_end)

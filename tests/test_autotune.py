@@ -67,16 +67,25 @@ def test_autotune_choice_is_kept_and_exact(gpu_available, tmp_path, monkeypatch)
     f, r = g.last_launch_shape()
     assert f >= 1 and 1 <= r <= 16
     assert rel(out, ref) < 1e-13
+    st = g.last_gemm_stages()
+    assert st in (3, 4, 5)
     lines = cache.read_text().splitlines()
     assert len(lines) == 1
-    key, fs, rs = lines[0].split()
-    assert "k2:" in key and (int(fs), int(rs)) == (f, r)
+    key, fs, rs, ss = lines[0].split()
+    assert "k2:" in key and (int(fs), int(rs), int(ss)) == (f, r, st)
     # the second call of the same shape reuses the choice (nothing new is written)
     out2 = spectrum(c, g)
     np.testing.assert_array_equal(out2, out)
     assert g.last_launch_shape() == (f, r)
     assert len(cache.read_text().splitlines()) == 1
-    # a fixed shape takes precedence
+    assert g.last_gemm_stages() == st
+    # a fixed shape takes precedence; the GEMM's stage count does not change the result
     g.set_launch_shape(1, 1)
     spectrum(c, g)
     assert g.last_launch_shape() == (1, 1)
+    outs = {}
+    for stages in (3, 5):
+        g.set_gemm_stages(stages)
+        outs[stages] = spectrum(c, g)
+        assert g.last_gemm_stages() == stages
+    np.testing.assert_array_equal(outs[3], outs[5])
