@@ -252,14 +252,16 @@ def run_b200(args):
     sampler.start()
     barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.steps):
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    evs[0].record(stream)
+    for i in range(args.steps):
         step()
-    e1.record(stream)
+        evs[i + 1].record(stream)
     torch.cuda.synchronize()
     barrier()
     clocks = sampler.stop()
+    e0, e1 = evs[0], evs[-1]
+    step_ms = [evs[i].elapsed_time(evs[i + 1]) for i in range(args.steps)]
     launch_shape = g.last_launch_shape()
     gemm_stages = g.last_gemm_stages()
     ms = max_over_ranks(e0.elapsed_time(e1), device="cuda")
@@ -366,7 +368,8 @@ def run_b200(args):
     if not args.no_compare and world == 1:
         compare = compare_fp64(cfg, args.kernel, res, lib, L)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "warmup": args.warmup, "ms_per_step": ms_step, "step_ms": [round(x, 2) for x in step_ms],
+            "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64" if not args.kernel.startswith("mixed") else ("int8x4+f64" if args.kernel == "mixed" else "f32+f64"), "data": "synthetic",
             "config": {"workload": cfg.name, "bubbles": int(cfg.n), "colliders": int(cfg.n + cfg.exterior.shape[0]),
                        "n_cos": cfg.n_cos, "n_phi": cfg.n_phi, "n_t": cfg.n_t, "n_w": int(Wn),

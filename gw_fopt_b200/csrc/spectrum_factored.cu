@@ -158,7 +158,7 @@ __device__ __forceinline__ double tpow(double x, double p) {
 }
 
 template <class Real, int SMC>
-__global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ beta) {
+__global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1) k_beta(BetaArgs A, Real* __restrict__ beta) {
     extern __shared__ __align__(16) unsigned char sm_b[];
     constexpr int NQ = 2 + 2 * SMC;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -382,7 +382,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             : nullptr;
     // beta of coefficient set s at step k from the sums there: the table row
     // holds the step weight times dt^3 and times a_m dt^{3-p_m} e^{-dt/w}
-    auto value = [&](int k, int s, const double* P, double Uc, double Us, double& xc, double& xs) {
+    auto value = [&](int k, int s, const double* P, double Uc, double Us, double mul, double& xc, double& xs) {
         const double* Dk = Dslot + (size_t)min(k, A.n_t - 1) * (1 + SMC);
         double g[1 + SMC];
         if constexpr ((1 + SMC) % 2 == 0) {
@@ -404,7 +404,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             vc += g[1 + t] * P[2 * t];
             vs += g[1 + t] * P[2 * t + 1];
         }
-        const double r = k < A.n_t ? rf : 0.0;
+        const double r = k < A.n_t ? mul : 0.0;
         xc = r * vc;
         xs = r * vs;
     };
@@ -496,80 +496,90 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
     };
     if constexpr (kI8) {
         // The row's scale is max |beta| over its steps and columns, found exactly without
-        // forming every value.  In block b, beta = rf (D0(k) U(k) + sum_m Dm(k) Pm(k)) is bounded
-        // by interval arithmetic over the per-block ranges of the time table and of U, Pm (constant
-        // in a block without events); blocks are formed (lane = step) in decreasing order of their
-        // bound until no bound exceeds the largest value found (most often one block: the last
-        // one, where dt^3 peaks).
+        // forming every value.
+        // (a) Every event block is formed once (lane = step) and its 2S values are kept for the
+        //     digits: a block of at least 32 events in its own weight slots (plane 2s + g, slots
+        //     boff[b] + lane; its weights are not read again), smaller blocks in the block-total
+        //     table while it has room (the rest are formed again in (c)).  Blocks that use the
+        //     block-total table as their step table (more than 32 events) go first.
+        // (b) In a block without events U and Pm are constant, so beta = rf (D0(k) U + sum_m Dm(k)
+        //     Pm) is bounded by interval arithmetic over the per-block ranges of the time table;
+        //     such blocks are formed (lane = step) in decreasing order of their bound until no
+        //     bound exceeds the largest value found (most often one block: the last one, where
+        //     dt^3 peaks).
+        // (c) Digits of every block.
         double vmax = 0.0;
         const double* Dmx = A.Dmax + (size_t)slot * NB * (1 + SMC) * 2;
-        auto block_max = [&](int b) {  // whole warp; lane = step
-            double P[2 * SMC], Uc, Us;
-            step_sums(b, P, Uc, Us);
-            const int k = (b << 5) + lane;
-            double m = 0.0;
-            for (int s2 = 0; s2 < A.S; ++s2) {
-                double xc, xs;
-                value(k, s2, P, Uc, Us, xc, xs);
-                m = fmax(m, fmax(fabs(xc), fabs(xs)));
+        int* where = brun;  // per event block: -1 not kept, -2 own slots, c >= 0 table slot c
+        const int n_tab = (NQ * NB) / (64 * A.S);
+        int used_tab = 0;
+        auto kept = [&](int b, int& stride) -> double* {
+            const int w = where[b];
+            if (w == -2) {
+                stride = EV;
+                return evq + boff[b];
             }
-            return m;
+            stride = 32;
+            return w >= 0 ? btot + (size_t)w * 64 * A.S : nullptr;
         };
+        for (int sweep = 0; sweep < 2; ++sweep) {
+            for (int bc = 0; bc < NB; bc += 32) {
+                const int bl = bc + lane;
+                const int cnt = bl < NB ? boff[bl + 1] - boff[bl] : 0;
+                const bool pick = sweep == 0 ? cnt >= 32 : (cnt > 0 && cnt < 32);
+                for (unsigned h = __ballot_sync(full, pick); h; h &= h - 1) {
+                    const int b = bc + __ffs(h) - 1;
+                    double P[2 * SMC], Uc, Us;
+                    step_sums(b, P, Uc, Us);
+                    const int k = (b << 5) + lane;
+                    int code = -1;
+                    if (sweep == 0)
+                        code = -2;
+                    else if (used_tab < n_tab)
+                        code = used_tab++;
+                    __syncwarp();
+                    if (lane == 0) where[b] = code;
+                    __syncwarp();
+                    int stride = 0;
+                    double* dst = kept(b, stride);
+                    for (int s2 = 0; s2 < A.S; ++s2) {
+                        double xc, xs;
+                        value(k, s2, P, Uc, Us, rf, xc, xs);
+                        vmax = fmax(vmax, fmax(fabs(xc), fabs(xs)));
+                        if (dst) {
+                            dst[(size_t)(2 * s2) * stride + lane] = xc;
+                            dst[(size_t)(2 * s2 + 1) * stride + lane] = xs;
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(full, vmax, o));
         for (int bc = 0; bc < NB; bc += 32) {
             const int bl = bc + lane;
-            const bool has = bl < NB && boff[bl] != boff[bl + 1];
-            // a block holding events: U and Pm move by its events' weights within the block, so
-            // |U(k)| <= |U after the block| + sum |q| and |Pm(k)| <= |Pm before it| + sum |q f|
-            double addU = 0.0, addP[SMC];
-#pragma unroll
-            for (int q = 0; q < SMC; ++q) addP[q] = 0.0;
-            for (unsigned h = __ballot_sync(full, has); h; h &= h - 1) {
-                const int b = bc + __ffs(h) - 1;
-                double aU = 0.0, aP[SMC];
-#pragma unroll
-                for (int q = 0; q < SMC; ++q) aP[q] = 0.0;
-                for (int e = boff[b] + lane; e < boff[b + 1]; e += 32) {
-                    aU += fmax(fabs(evq[e]), fabs(evq[(size_t)EV + e]));
-#pragma unroll
-                    for (int q = 0; q < SMC; ++q)
-                        aP[q] += fmax(fabs(evq[(size_t)(2 + 2 * q) * EV + e]), fabs(evq[(size_t)(3 + 2 * q) * EV + e]));
-                }
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    aU += __shfl_xor_sync(full, aU, o);
-#pragma unroll
-                    for (int q = 0; q < SMC; ++q) aP[q] += __shfl_xor_sync(full, aP[q], o);
-                }
-                if (lane == b - bc) {
-                    addU = aU;
-#pragma unroll
-                    for (int q = 0; q < SMC; ++q) addP[q] = aP[q];
-                }
-            }
-            double bnd = -1.0;  // this lane's block's bound (-1: none)
-            if (bl < NB) {
-                // interval arithmetic: beta of set s, column g lies in
-                // rf (D0 [U] + sum_m Dm [Pm]) with D in [min, max] over the block and U, Pm in
-                // [value at the block's end or start -/+ the block's event weights]
+            double bnd = -1.0;  // this lane's block's bound (-1: none or an event block)
+            if (bl < NB && boff[bl] == boff[bl + 1]) {
+                // beta of set s, column g lies in rf (D0 [U] + sum_m Dm [Pm]) with D in [min, max]
+                // over the block and U, Pm the block's constants
                 const double* mx = Dmx + (size_t)bl * (1 + SMC) * 2;
-                auto term = [&](double dlo, double dhi, double c, double a, double& lo, double& hi, double& sa) {
-                    const double c0 = c - a, c1 = c + a;
-                    const double p0 = dlo * c0, p1 = dlo * c1, p2 = dhi * c0, p3 = dhi * c1;
-                    lo += fmin(fmin(p0, p1), fmin(p2, p3));
-                    hi += fmax(fmax(p0, p1), fmax(p2, p3));
-                    sa += fmax(fabs(dlo), fabs(dhi)) * (fabs(c) + a);
+                auto term = [&](double dlo, double dhi, double c, double& lo, double& hi, double& sa) {
+                    const double p0 = dlo * c, p1 = dhi * c;
+                    lo += fmin(p0, p1);
+                    hi += fmax(p0, p1);
+                    sa += fmax(fabs(dlo), fabs(dhi)) * fabs(c);
                 };
                 for (int s2 = 0; s2 < A.S; ++s2) {
                     const int t0 = s2 * A.M, t1 = t0 + A.M;
 #pragma unroll
                     for (int g = 0; g < 2; ++g) {
                         double lo = 0.0, hi = 0.0, sa = 0.0;
-                        term(mx[0], mx[1], uend[2 * bl + g], addU, lo, hi, sa);
+                        term(mx[0], mx[1], uend[2 * bl + g], lo, hi, sa);
 #pragma unroll
                         for (int q = 0; q < SMC; ++q)
                             if (q >= t0 && q < t1)
-                                term(mx[2 + 2 * q], mx[3 + 2 * q], pbeg[(size_t)bl * 2 * SMC + 2 * q + g], addP[q], lo,
-                                     hi, sa);
+                                term(mx[2 + 2 * q], mx[3 + 2 * q], pbeg[(size_t)bl * 2 * SMC + 2 * q + g], lo, hi, sa);
                         // relative and absolute margins cover the rounding of these sums and of
                         // the values themselves (a few ulp of the summed magnitudes)
                         bnd = fmax(bnd, (fmax(fabs(lo), fabs(hi)) * (1.0 + 1e-12) + 1e-13 * sa) * rf);
@@ -577,9 +587,6 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
                 }
             }
             for (;;) {
-                double vm = fmax(vmax, __shfl_xor_sync(full, vmax, 16));  // lanes agree on vmax below
-                for (int o = 8; o > 0; o >>= 1) vm = fmax(vm, __shfl_xor_sync(full, vm, o));
-                vmax = vm;
                 double bb = bnd;
                 int bi = lane;
                 for (int o = 16; o > 0; o >>= 1) {
@@ -591,15 +598,27 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
                     }
                 }
                 if (!(bb > vmax)) break;  // every remaining bound is covered
-                vmax = fmax(vmax, block_max(bc + bi));
+                {
+                    const int b = bc + bi, k = (b << 5) + lane;
+                    const double* P = pbeg + (size_t)b * 2 * SMC;
+                    const double Uc = uend[2 * b], Us = uend[2 * b + 1];
+                    double m = 0.0;
+                    for (int s2 = 0; s2 < A.S; ++s2) {
+                        double xc, xs;
+                        value(k, s2, P, Uc, Us, rf, xc, xs);
+                        m = fmax(m, fmax(fabs(xc), fabs(xs)));
+                    }
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(full, m, o));
+                    vmax = fmax(vmax, m);
+                }
                 if (lane == bi) bnd = -1.0;
             }
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) vmax = fmax(vmax, __shfl_xor_sync(full, vmax, o));
         if (lane == 0) A.scale[row] = vmax;
         const double inv = vmax > 0.0 ? 1.0 / vmax : 0.0;
-        // digits.  Blocks with events: lane = step; a quad of lanes transposes its packed digit
+        const double rinv = rf * inv;
+        // digits.  Event blocks: lane = step; a quad of lanes transposes its packed digit
         // words so that lane 4q + d holds digit d of steps 4q .. 4q + 3.  Blocks without
         // events: 4 steps per lane (8 lanes a block, 4 blocks at a time), transposed in
         // registers.  Either way a store instruction fills whole 32-byte rows of the blocks.
@@ -618,13 +637,20 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
             unsigned quiet = __ballot_sync(full, bl < NB && !has);
             for (unsigned h = ev_blocks; h; h &= h - 1) {
                 const int b = bc + __ffs(h) - 1;
-                double P[2 * SMC], Uc, Us;
-                step_sums(b, P, Uc, Us);
                 const int k = (b << 5) + lane;
+                int stride = 0;
+                const double* src = kept(b, stride);
+                double P[2 * SMC], Uc = 0.0, Us = 0.0;
+                if (!src) step_sums(b, P, Uc, Us);
                 int8_t* blk = blk_row + (size_t)b * kI8BlockSet + dg * kI8Block;
                 for (int s2 = 0; s2 < A.S; ++s2) {
                     double xc, xs;
-                    value(k, s2, P, Uc, Us, xc, xs);
+                    if (src) {
+                        xc = src[(size_t)(2 * s2) * stride + lane];
+                        xs = src[(size_t)(2 * s2 + 1) * stride + lane];
+                    } else {
+                        value(k, s2, P, Uc, Us, rf, xc, xs);
+                    }
                     const uint32_t wc = quad_transpose(i8_digits(xc * inv));
                     const uint32_t ws = quad_transpose(i8_digits(xs * inv));
                     *reinterpret_cast<uint32_t*>(blk + i8_swz(nbase + 2 * s2, s4)) = wc;
@@ -647,9 +673,9 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
                         double xc, xs;
-                        value(k0 + m, s2, P, Uc, Us, xc, xs);
-                        pc[m] = i8_digits(xc * inv);
-                        ps[m] = i8_digits(xs * inv);
+                        value(k0 + m, s2, P, Uc, Us, rinv, xc, xs);
+                        pc[m] = i8_digits(xc);
+                        ps[m] = i8_digits(xs);
                     }
                     uint32_t wc[4], ws[4];
                     i8_transpose4(pc[0], pc[1], pc[2], pc[3], wc);
@@ -677,7 +703,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
                 const int k = (b << 5) + lane;
                 for (int s2 = 0; s2 < A.S; ++s2) {
                     double xc, xs;
-                    value(k, s2, P, Uc, Us, xc, xs);
+                    value(k, s2, P, Uc, Us, rf, xc, xs);
                     if (k < A.t_pad) {
                         brow[(size_t)(2 * s2) * A.t_pad + k] = (Real)xc;
                         brow[(size_t)(2 * s2 + 1) * A.t_pad + k] = (Real)xs;
@@ -698,7 +724,7 @@ __global__ void __launch_bounds__(256) k_beta(BetaArgs A, Real* __restrict__ bet
                 for (int s2 = 0; s2 < A.S; ++s2) {
                     double xc[4], xs[4];
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) value(k0 + m, s2, P, Uc, Us, xc[m], xs[m]);
+                    for (int m = 0; m < 4; ++m) value(k0 + m, s2, P, Uc, Us, rf, xc[m], xs[m]);
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
                         const int k = k0 + m;

@@ -7,15 +7,16 @@
 // e^{i w (t_a c_i - z_a)} per (w, bubble) and sums over the tile's bubbles
 // (spectrum_factored.cu holds the derivation).
 //
-// Both operands are written as four signed 8-bit digits (spectrum_tc.cuh):
-// M = (m0 + m1/254 + m2/254^2 + m3/254^3)/127 and beta = s_a (b0 + ... )/127,
-// with one scale s_a per (frame, bubble, row) = max |beta| over the row's steps
-// and columns.  The product keeps the ten digit pairs (p, q) with p + q <= 3
-// (0-based); the pairs of one level L = p + q share the weight 254^-L, so
-//   Y = s_a / 127^2  sum_L 254^-L D_L,   D_L = sum_k sum_{p+q=L} m_p b_q,
+// Both operands are written as four signed 8-bit digits in balanced base 256
+// (spectrum_tc.cuh): M F = sum_p m_p 256^(3-p) and beta F = s_a sum_q b_q
+// 256^(3-q) with F = 0x7F7F7F7F, one scale s_a per (frame, bubble, row) =
+// max |beta| over the row's steps and columns.  The product keeps the ten
+// digit pairs (p, q) with p + q <= 3 (p = 0 the most significant digit); the
+// pairs of one level L = p + q share the weight 256^-L, so
+//   Y = s_a 256^6 / F^2  sum_L 256^-L D_L,   D_L = sum_k sum_{p+q=L} m_p b_q,
 // and each D_L is accumulated EXACTLY by tcgen05.mma kind::i8 in a 32-bit
-// integer accumulator of tensor memory (|D_L| <= 4 * 127^2 * n_t < 2^31 for
-// n_t <= 32768).  The error is the digit truncation, about 2^-32 of the
+// integer accumulator of tensor memory (|D_L| <= 4 * 128^2 * n_t < 2^31 for
+// n_t <= 32767).  The error is the digit truncation, about 2^-32 of the
 // operands' scales per term, against 2^-24 for FP32 operands; there is no
 // rounding in the accumulation at all, so the accumulators run over a whole
 // row of time steps and are read once per row.
@@ -34,7 +35,7 @@
 //   1     MMA issue (one thread) and tensor-memory allocation
 //   2-9   epilogue, two warpgroups of 64 columns each: thread = tensor-memory
 //         lane.  While a row's MMAs run, each warp fills its part of the FP64
-//         table s_a/127^2 e^{i w (t_a c_i - z_a)} (64 w x 64 bubbles, shared
+//         table s_a 256^6/F^2 e^{i w (t_a c_i - z_a)} (64 w x 64 bubbles, shared
 //         memory); when the row's accumulators are complete it reads the four
 //         levels (tcgen05.ld), combines them (level 0 in FP64, levels 1-3 in
 //         FP32, whose rounding lies below the truncation) and adds
@@ -319,7 +320,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_i8(TcArgs A) {
         double accC[CPB], accS[CPB];
 #pragma unroll
         for (int c = 0; c < CPB; ++c) accC[c] = accS[c] = 0.0;
-        constexpr float kInv254 = 1.0f / 254.0f;
+        constexpr float kInv256 = 1.0f / 256.0f;
         // the column offset is a compile-time constant in each instance, so that
         // every per-column index below is too (no dynamically indexed arrays)
         auto run = [&](auto half_c) {
@@ -328,7 +329,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_i8(TcArgs A) {
             constexpr int nb = b_hi - b_lo + 1;
             int row = 0;
             for (int i = i0; active && i < i1 && !failed; ++i, ++row) {
-                // s_a / 127^2 e^{i w (t_a c_i - z_a)} per (w, bubble) of this row; zero for
+                // s_a 256^6 / F^2 e^{i w (t_a c_i - z_a)} per (w, bubble) of this row; zero for
                 // empty columns.  Each warp fills the entries it reads (its 16
                 // frequencies, its bubbles) while the row's MMAs run.
                 const double ci = A.cos_t[i];
@@ -338,7 +339,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_i8(TcArgs A) {
                     double2 e = make_double2(0.0, 0.0);
                     if (b < A.bpt && binfo[b] >= 0 && w0 + l < A.n_w) {
                         const double sc =
-                            A.bscale[((size_t)frame * A.n_sel + binfo[b]) * A.n_cos + i] * (1.0 / 16129.0);
+                            A.bscale[((size_t)frame * A.n_sel + binfo[b]) * A.n_cos + i] * kI8PairScale;
                         double sn, cs;
                         sincos(A.w[w0 + l] * (bt[b] * ci - bz[b]), &sn, &cs);
                         e = make_double2(sc * cs, sc * sn);
@@ -359,9 +360,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_i8(TcArgs A) {
                     for (int c = 0; c < 16; ++c) {
                         const int n = n0 + c;
                         const int b = n / CPB, sc = n % CPB;
-                        const float lo = fmaf(fmaf(fmaf((float)(int)d3[c], kInv254, (float)(int)d2[c]), kInv254,
+                        const float lo = fmaf(fmaf(fmaf((float)(int)d3[c], kInv256, (float)(int)d2[c]), kInv256,
                                                    (float)(int)d1[c]),
-                                              kInv254, 0.0f);
+                                              kInv256, 0.0f);
                         const double y = (double)(int)d0[c] + (double)lo;
                         const double2 e = etab[eslot(wl, b)];
                         accC[sc] = fma(e.x, y, accC[sc]);
@@ -484,7 +485,7 @@ int tc_row_parts(size_t n_ctas, int n_cos, int n_sm) {
 void launch_gemm_tc(const TcArgs& A, size_t kn, cudaStream_t st) {
     if (A.bpt * 2 * A.S > kTcCols) throw Error{"tensor-core GEMM: too many columns per tile"};
     if (A.row_parts < 1 || A.row_parts > A.n_cos) throw Error{"tensor-core GEMM: bad row split"};
-    if (A.n_t > kI8MaxSteps) throw Error{"the mixed kernel accumulates at most 32768 time steps exactly; use fp64_factored"};
+    if (A.n_t > kI8MaxSteps) throw Error{"the mixed kernel accumulates at most 32767 time steps exactly; use fp64_factored"};
     if (A.stages != 0 && (A.stages < 3 || A.stages > 5)) throw Error{"tensor-core GEMM: 3 to 5 pipeline stages"};
     const size_t gy = kn * (size_t)A.tiles_per_frame * A.row_parts;
     if (gy > 65535) throw Error{"too many column tiles in one k-hat chunk"};

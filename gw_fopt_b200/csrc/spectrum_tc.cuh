@@ -18,25 +18,21 @@ constexpr int kI8Slices = 4;                       // int8 digits per value
 constexpr int kI8Block = 128 * 32;                 // bytes of one digit block
 constexpr int kI8BlockSet = kI8Slices * kI8Block;  // the four digit blocks of one (rows, 32 steps) block
 
-// Digits of x in [-1, 1]: X = rint(x * 127 * 254^3) (|X| < 2^31) written in
-// balanced base 254, x = (d0 + d1/254 + d2/254^2 + d3/254^3) / 127 + e with
-// |e| <= 0.5 / (127 * 254^3) (2^-33 about) and every digit in [-127, 127].
-// u = X + 127 (254^3 + 254^2 + 254 + 1) is non-negative and below 2^32; its
-// base-254 digits D0 (not reduced, <= 254), D1, D2, D3 give d = D - 127.
-// Returned packed, byte s = digit d_s.
-constexpr double kI8Full = 127.0 * 254.0 * 254.0 * 254.0;  // 2 081 157 128
-constexpr uint32_t kI8Offset = 127u * (254u * 254u * 254u + 254u * 254u + 254u + 1u);
+// Digits of x in [-1, 1]: X = rint(x F) with F = 0x7F7F7F7F (|X| <= F < 2^31)
+// written in balanced base 256, x F = sum_s d_s 256^(3-s) with the top digit
+// d_0 in [-127, 127] and d_1, d_2, d_3 in [-128, 127]; the representation error
+// is |e| <= 0.5 / F (2^-32 about).  Adding 128 to every digit gives the
+// ordinary base-256 digits of Y = X + 0x80808080, which lies in
+// [0x01010101, 0xFFFFFFFF] and so needs no carry beyond 32 bits: the digits are
+// the bytes of Y with the top bit flipped.  Returned packed, byte s = digit
+// d_s (d_0 the most significant).
+constexpr double kI8Full = 2139062143.0;  // F = 0x7F7F7F7F
+// x y = (256^6 / F^2) sum_L 256^-L sum_{s+r=L} d_s(x) d_r(y) for the digit
+// pairs of level L = s + r
+constexpr double kI8PairScale = 281474976710656.0 / (kI8Full * kI8Full);
 __device__ __forceinline__ uint32_t i8_digits(double x) {
-    uint32_t u = (uint32_t)__double2int_rn(x * kI8Full) + kI8Offset;
-    const uint32_t d3 = u % 254u;
-    u /= 254u;
-    const uint32_t d2 = u % 254u;
-    u /= 254u;
-    const uint32_t d1 = u % 254u;
-    const uint32_t d0 = u / 254u;
-    // each byte holds D - 127 in two's complement
-    return ((d0 - 127u) & 0xffu) | (((d1 - 127u) & 0xffu) << 8) | (((d2 - 127u) & 0xffu) << 16) |
-           ((d3 - 127u) << 24);
+    const uint32_t y = (uint32_t)__double2int_rn(x * kI8Full) + 0x80808080u;
+    return __byte_perm(y ^ 0x80808080u, 0u, 0x0123);
 }
 
 // Four packed digit words (one step each, byte s = digit s) transposed into
@@ -85,7 +81,8 @@ void launch_gemm_tc(const TcArgs& A, size_t kn, cudaStream_t st);
 // best (at most n_cos / 8 parts).
 int tc_row_parts(size_t n_ctas, int n_cos, int n_sm);
 
-// Largest n_t the int8 GEMM accumulates exactly in 32-bit integers.
-constexpr int kI8MaxSteps = 32768;
+// Largest n_t the int8 GEMM accumulates exactly in 32-bit integers: a level
+// sums at most 4 n_t products of magnitude <= 128^2, and 4 128^2 32767 < 2^31.
+constexpr int kI8MaxSteps = 32767;
 
 }  // namespace bgw

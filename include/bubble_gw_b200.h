@@ -39,8 +39,8 @@ typedef enum BgwxBoundaryCondition {
  * FP64_FACTORED: FP64 with the time phase shared across bubbles (register
  * tiled).  MIXED: FP64 phases, tables and final sums; the time-phase product
  * runs on the tensor cores as an exact integer product of four int8 digits
- * per operand (relative error about 2^-33 of the operands' scales per term,
- * n_t at most 32768).  MIXED_SIMT: FP32 operands with the product on the FP32
+ * per operand (relative error about 2^-32 of the operands' scales per term,
+ * n_t at most 32767).  MIXED_SIMT: FP32 operands with the product on the FP32
  * CUDA cores and FP32 partial sums folded into FP64 every 16 steps. */
 typedef enum BgwxKernel {
     BGWX_KERNEL_FP64_DIRECT = 0,
