@@ -124,6 +124,9 @@ def make_flow(cfg, kernel):
     g = mb.GeneralizedBulkFlow(lb)
     g.set_resolution(cfg.n_cos, cfg.n_phi)
     g.set_gradient_scaling_params(cfg.coefficients.tolist(), cfg.powers.tolist())
+    # the Python class hands the scaling parameters to the handle at its first compute call;
+    # the device-output steps below call the C ABI directly, so they are handed over here
+    g._push_params()
     g.set_kernel(kernel)
     return g
 
@@ -273,6 +276,8 @@ def run_b200(args):
     L.check(lib.bgwx_generalized_bulk_flow_set_stream(g._h, None))
     res = g.compute_c_integral_khat(cfg.w, cfg.khat, t_begin=cfg.t_begin, t_end=cfg.t_end, n_t=cfg.n_t)
     tm = g.last_timings()
+    # the timed device-output steps computed the same spectrum (same kernels and launch shape)
+    assert np.array_equal(out_dev.cpu().numpy(), res), "device-output steps differ from the public call"
     launches_per_step = int(tm["launches"])
 
     # end to end through the public API with host buffers

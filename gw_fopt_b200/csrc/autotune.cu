@@ -77,7 +77,7 @@ std::string shape_key(const Device* dev, const SpectrumJob& job) {
     std::ostringstream k;
     k << name << ':' << dev->n_sm << ":k" << (int)job.kernel << ":int" << job.n_int << ":tot" << job.n_tot << ":sel"
       << job.n_sel << ":c" << job.n_cos << ":p" << job.n_phi << ":t" << job.n_t << ":w" << job.n_w << ":s"
-      << job.n_sets << ":m" << job.n_terms << ":d" << (job.has_damping ? 1 : 0) << ":K" << job.n_k;
+      << job.n_sets << ":m" << job.n_terms << ":d" << (job.has_damping ? 1 : 0) << ":K" << job.n_k << ":R" << job.n_real;
     return k.str();
 }
 
@@ -135,7 +135,7 @@ LaunchShape autotune_launch_shape(Device* dev, const SpectrumJob& job) {
     SpectrumJob sub = job;
     sub.n_k = n_s;  // the first n_s frames (rot rows are frame-major)
     if (!job.rot) sub.n_k = 1;
-    const size_t out_bytes = sub.n_k * 2 * job.n_sets * job.n_w * sizeof(double2);
+    const size_t out_bytes = std::max<size_t>(1, job.n_real) * sub.n_k * 2 * job.n_sets * job.n_w * sizeof(double2);
     double* out = nullptr;
     CUDA_OK(cudaMalloc(&out, out_bytes));
     LaunchShape best;

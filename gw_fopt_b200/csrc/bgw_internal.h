@@ -67,7 +67,23 @@ struct SpectrumJob {
     size_t frames_per_launch = 0;
     int row_parts = 0;
     int gemm_stages = 0;
+    // Several realizations in one call (the batched ensemble, factored kernels): `bubbles` holds
+    // them one after another (n_tot rows in all; n_int = n_tot), `sel` has one slot per radiating
+    // bubble, padded so that each realization starts a GEMM column tile (padding slots hold
+    // kNoSlot), `ranges` (n_sel pairs) gives each slot's realization rows (first, count) and
+    // `real_tiles` (n_real + 1) the first column tile of each realization.  The output is then
+    // (n_real, n_k, 2, n_sets, n_w).
+    const uint32_t* ranges = nullptr;
+    const uint32_t* real_tiles = nullptr;
+    size_t n_real = 0;
 };
+
+// A padding slot of a batched job.
+constexpr uint32_t kNoSlot = 0xFFFFFFFFu;
+
+// Radiating bubbles per GEMM column tile of a factored-kernel job (each batched
+// realization starts a tile).
+size_t factored_bubbles_per_tile(const SpectrumJob& job);
 
 // The launch shape a spectrum call used (or is to use).
 struct LaunchShape {
@@ -119,11 +135,15 @@ int factored_auto_row_parts(const Device* dev, const SpectrumJob& job, size_t kn
 // the automatic one.  Throws Error.
 LaunchShape autotune_launch_shape(Device* dev, const SpectrumJob& job);
 
-// Runs one job per realization back to back on the handle's stream (largest
-// first, so the grow-only work arrays are sized once) into one device array
-// and copies it out once; out: (R, n_k, 2, n_sets, n_w) complex as
-// interleaved doubles.  Jobs with no radiating bubble yield zeros.
-void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out, BgwxTimings* timings);
+// The spectra of R realizations that share every setting but their bubbles,
+// into one device array copied out once; out: (R, n_k, 2, n_sets, n_w)
+// complex as interleaved doubles.  On the factored kernels all realizations
+// form one batched job (each pipeline launch covers every realization of its
+// frames; the launch shape of jobs[0], or a measured one when `autotune`); the
+// FP64 direct kernel runs one job per realization back to back.  Realizations
+// with no radiating bubble yield zeros.
+void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out, BgwxTimings* timings,
+                  bool autotune = false);
 
 // Vector-Jacobian product of the spectrum: gbar (n_k, 2, n_sets, n_w)
 // complex cotangents dL/dRe C + i dL/dIm C (interleaved doubles) ->

@@ -480,10 +480,15 @@ BgwStatus bgwx_generalized_bulk_flow_compute_ensemble_khat(
             jobs[r].n_tot = ni + ne;
             jobs[r].sel = ids[r].data();
             jobs[r].n_sel = ni;
+            // a fixed launch shape applies to the batched launches (the measured one is taken there)
+            jobs[r].frames_per_launch = h->frames_per_launch;
+            jobs[r].row_parts = (int)h->row_parts;
+            jobs[r].gemm_stages = (int)h->gemm_stages;
         }
+        const bool fixed = h->frames_per_launch || h->row_parts || h->gemm_stages;
         h->timings = BgwxTimings{};
         std::vector<double> result(2 * expected, 0.0);
-        bgw::run_ensemble(device(h), jobs, result.data(), &h->timings);
+        bgw::run_ensemble(device(h), jobs, result.data(), &h->timings, h->autotune && !fixed);
         BgwComplex64* o = const_cast<BgwComplex64*>(slice(out, out_len, "out"));
         for (size_t q = 0; q < expected; ++q) o[q] = BgwComplex64{result[2 * q], result[2 * q + 1]};
     });

@@ -77,14 +77,14 @@ struct Device {
     std::vector<cudaEvent_t> fact_ev;   // 3 per k-hat chunk: before beta, before GEMM, after GEMM
     DevBuf bub, bubrot, dirs, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, sel, rot, cosphi, sinphi;
     DevBuf tau, codes, partial, out, counters, nblists;
+    DevBuf ranges, real_tiles;  // batched jobs: per-slot realization rows, first tile per realization
     DevBuf fact_D, fact_kfirst, beta, fact_partial;  // factored-kernel work arrays
     DevBuf ens_out;                                  // batched ensemble: all realizations' spectra
     DevBuf pp_in, pp_small, pp_out;                  // spectrum post-processing: input, small tables, output
     DevBuf beta_scale;                               // int8 tensor-core GEMM: per-(bubble, row) beta scales
     DevBuf fact_Dmax;                                // int8 tensor-core GEMM: per-(bubble, block) time-table maxima
     DevBuf tc_atab;                                  // int8 tensor-core GEMM: time-phase digits
-    std::vector<double> tc_key;                      // (n_w, n_cos, n_t, w, cos-theta, t) of tc_atab
-    bool tc_key_reuse = false;                       // set by the batched ensemble: one grid for all calls
+    bool tc_atab_valid = false;  // tc_atab holds the current call's time-phase digits
     DevBuf adj_gbar, adj_scratch, adj_grad, adj_mtab; // adjoint: cotangents, work arrays, gradients, phases
     size_t last_frames_per_launch = 0;               // launch shape of the last spectrum call
     int last_row_parts = 0;

@@ -196,18 +196,24 @@ __device__ __forceinline__ void collider_bounds(const D4& d, double& key, double
 
 __global__ void __launch_bounds__(kNbThreads)
     k_neighbors(const D4* __restrict__ bub, size_t n_int, size_t n_tot, const uint32_t* __restrict__ sel,
-                NbList* __restrict__ out) {
+                const uint2* __restrict__ ranges, NbList* __restrict__ out) {
     __shared__ unsigned hist[2048];
     __shared__ unsigned s_prefix, s_mask, s_need, s_count, s_nout;
     __shared__ double s_key[kList];
     __shared__ int s_idx[kList];
     __shared__ double s_r1[kNbThreads], s_r2[kNbThreads];
     const int slot = blockIdx.x;
-    const uint32_t a = sel[slot];
+    uint32_t a = sel[slot];
     NbList* L = out + slot;
     if (a >= n_int) {  // not an interior bubble: marked, never dereferenced
         if (threadIdx.x == 0) L->count = -1;
         return;
+    }
+    if (ranges) {  // several realizations: this slot's colliders are its own realization's rows
+        const uint2 r = ranges[slot];
+        bub += r.x;
+        n_tot = r.y;
+        a -= r.x;
     }
     const D4 xa = bub[a];
     const size_t n_c = n_tot - 1;  // colliders other than a
@@ -340,7 +346,8 @@ __global__ void __launch_bounds__(kNbThreads)
 // chunks of the range independently (no block barrier after the prologue).
 __global__ void __launch_bounds__(kMaskListThreads)
     k_masks_list(const D4* __restrict__ bub, size_t n_int, size_t n_tot, const uint32_t* __restrict__ sel,
-                 size_t n_sel, const NbList* __restrict__ lists, const D4* __restrict__ dirs, size_t nd,
+                 const uint2* __restrict__ ranges, size_t n_sel, const NbList* __restrict__ lists,
+                 const D4* __restrict__ dirs, size_t nd,
                  size_t row_len, unsigned n_split, double* __restrict__ tau_out, int32_t* __restrict__ code_out,
                  unsigned long long* __restrict__ counters) {
     // per listed collider: Delta = x_c - x_a and its Minkowski norm, computed once
@@ -365,8 +372,8 @@ __global__ void __launch_bounds__(kMaskListThreads)
     const int lane = threadIdx.x & 31;
     constexpr int kBatch = 2;
     constexpr int kRowsPerItem = 8;  // rows walked by a warp in one strip item
-    const D4* B = bub + (size_t)k * n_tot;
-    const uint32_t a = sel[slot];
+    const D4* B = bub + (size_t)k * n_tot;  // frame k
+    uint32_t a = sel[slot];
     const NbList* L = lists + slot;
     const int n = L->count;
     __shared__ bool s_big;  // a listed Delta too large for the candidate filter's margin
@@ -384,6 +391,12 @@ __global__ void __launch_bounds__(kMaskListThreads)
             if (code_row) code_row[d] = INT32_MIN;
         }
         return;
+    }
+    if (ranges) {  // several realizations: this slot's colliders are its own realization's rows
+        const uint2 r = ranges[slot];
+        B += r.x;
+        n_tot = r.y;
+        a -= r.x;
     }
     const int no = L->n_outliers;
     const D4 xa = B[a];
@@ -677,21 +690,21 @@ void launch_masks_with_lists(cudaStream_t stream, const D4* bub, size_t n_int, s
         return;
     }
     if (n_sel > 0x7fffffffULL) throw Error{"too many radiating bubbles"};
-    k_neighbors<<<(unsigned)n_sel, kNbThreads, 0, stream>>>(bub, n_int, n_tot, sel, lists);
+    k_neighbors<<<(unsigned)n_sel, kNbThreads, 0, stream>>>(bub, n_int, n_tot, sel, nullptr, lists);
     CUDA_OK(cudaGetLastError());
     // the directions' row structure is not known here: one row of nd directions
     const unsigned n_split = mask_split(nd, nd, n_sel);
     const size_t gx = (size_t)n_split * n_sel;
     if (gx > 0x7fffffffULL) throw Error{"too many (bubble, patch) pairs for one launch"};
-    k_masks_list<<<dim3((unsigned)gx, 1), kMaskListThreads, 0, stream>>>(bub, n_int, n_tot, sel, n_sel, lists, dirs,
-                                                                        nd, nd, n_split, tau, codes, counters);
+    k_masks_list<<<dim3((unsigned)gx, 1), kMaskListThreads, 0, stream>>>(bub, n_int, n_tot, sel, nullptr, n_sel, lists,
+                                                                        dirs, nd, nd, n_split, tau, codes, counters);
     CUDA_OK(cudaGetLastError());
 }
 
 void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames, size_t n_int, size_t n_tot,
-                          const uint32_t* sel, size_t n_sel, const D4* dirs, size_t nd, size_t row_len, size_t kn,
-                          double* tau, int32_t* codes, unsigned long long* counters, bool build_lists,
-                          uint64_t* launches) {
+                          const uint32_t* sel, const uint2* ranges, size_t n_sel, const D4* dirs, size_t nd,
+                          size_t row_len, size_t kn, double* tau, int32_t* codes, unsigned long long* counters,
+                          bool build_lists, uint64_t* launches) {
     if (row_len == 0 || nd % row_len != 0) row_len = nd;
     if (n_tot < 2) {
         // a lone bubble has no collider: every direction is None
@@ -702,7 +715,7 @@ void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames
     dev->nblists.ensure(n_sel * sizeof(NbList));
     if (build_lists) {
         if (n_sel > 0x7fffffffULL) throw Error{"too many radiating bubbles"};
-        k_neighbors<<<(unsigned)n_sel, kNbThreads, 0, dev->stream>>>(bub_unrot, n_int, n_tot, sel,
+        k_neighbors<<<(unsigned)n_sel, kNbThreads, 0, dev->stream>>>(bub_unrot, n_int, n_tot, sel, ranges,
                                                                       (NbList*)dev->nblists.p);
         CUDA_OK(cudaGetLastError());
         if (launches) ++*launches;
@@ -711,7 +724,7 @@ void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames
     const size_t gx = (size_t)n_split * n_sel;
     if (gx > 0x7fffffffULL || kn > 65535) throw Error{"too many (bubble, patch) pairs for one launch"};
     dim3 grid((unsigned)gx, (unsigned)kn);
-    k_masks_list<<<grid, kMaskListThreads, 0, dev->stream>>>(bub_frames, n_int, n_tot, sel, n_sel,
+    k_masks_list<<<grid, kMaskListThreads, 0, dev->stream>>>(bub_frames, n_int, n_tot, sel, ranges, n_sel,
                                                              (const NbList*)dev->nblists.p, dirs, nd, row_len, n_split, tau,
                                                              codes, counters);
     CUDA_OK(cudaGetLastError());

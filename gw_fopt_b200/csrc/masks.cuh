@@ -30,10 +30,13 @@ void launch_masks_with_lists(cudaStream_t stream, const D4* bub, size_t n_int, s
 
 // Builds the lists (when build_lists) from the unrotated bubbles and runs the
 // list-based exact search for kn frames.  tau/codes: (kn, n_sel, nd); the
-// directions are rows of row_len (n_phi) consecutive patches.
+// directions are rows of row_len (n_phi) consecutive patches.  ranges (device,
+// n_sel, may be null): several realizations in one bubble array, slot s's
+// colliders are rows [ranges[s].x, ranges[s].x + ranges[s].y) of each frame of
+// n_tot rows and sel holds indices into the whole array.
 void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames, size_t n_int, size_t n_tot,
-                          const uint32_t* sel, size_t n_sel, const D4* dirs, size_t nd, size_t row_len, size_t kn,
-                          double* tau, int32_t* codes, unsigned long long* counters, bool build_lists,
-                          uint64_t* launches);
+                          const uint32_t* sel, const uint2* ranges, size_t n_sel, const D4* dirs, size_t nd,
+                          size_t row_len, size_t kn, double* tau, int32_t* codes, unsigned long long* counters,
+                          bool build_lists, uint64_t* launches);
 
 }  // namespace bgw

@@ -582,7 +582,7 @@ void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_
     CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
     CUDA_OK(cudaEventRecord(dev->ev[0], dev->stream));
     uint64_t nl = 0;
-    launch_mask_pipeline(dev, bub, bub, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, job.n_phi, 1, (double*)dev->tau.p,
+    launch_mask_pipeline(dev, bub, bub, job.n_int, job.n_tot, sel, nullptr, job.n_sel, dirs, nd, job.n_phi, 1, (double*)dev->tau.p,
                          (int32_t*)dev->codes.p, (unsigned long long*)dev->counters.p, true, &nl);
     CUDA_OK(cudaEventRecord(dev->ev[1], dev->stream));
     CUDA_OK(cudaMemcpyAsync(out_codes, dev->codes.p, job.n_sel * nd * sizeof(int32_t), cudaMemcpyDeviceToHost,
@@ -638,6 +638,13 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     double* w = upload(dev, dev->w, job.w, W, tm);
     uint32_t* sel = upload(dev, dev->sel, job.sel, job.n_sel, tm);
     double* rot = job.rot ? upload(dev, dev->rot, job.rot, 9 * K, tm) : nullptr;
+    const bool batched = job.n_real > 0;
+    if (batched && (job.kernel == BGWX_KERNEL_FP64_DIRECT || job.tensor))
+        throw Error{"batched realizations run on the factored kernels only"};
+    const uint2* ranges =
+        batched ? reinterpret_cast<const uint2*>(upload(dev, dev->ranges, job.ranges, 2 * job.n_sel, tm)) : nullptr;
+    const uint32_t* real_tiles = batched ? upload(dev, dev->real_tiles, job.real_tiles, job.n_real + 1, tm) : nullptr;
+    const size_t out_blocks = batched ? job.n_real * K : K;  // (realization,) frame blocks of the output
     double* cosphi = job.tensor ? upload(dev, dev->cosphi, job.cosphi, job.n_phi, tm) : nullptr;
     double* sinphi = job.tensor ? upload(dev, dev->sinphi, job.sinphi, job.n_phi, tm) : nullptr;
 
@@ -651,7 +658,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     if (job.kernel == BGWX_KERNEL_FP64_DIRECT) dev->partial.ensure(kc * job.n_sel * per * sizeof(double2));
     double2* final_out = out_is_device ? reinterpret_cast<double2*>(out) : nullptr;
     if (!final_out) {
-        dev->out.ensure(K * per * sizeof(double2));
+        dev->out.ensure(out_blocks * per * sizeof(double2));
         final_out = (double2*)dev->out.p;
     }
     const size_t n_chunks = (K + kc - 1) / kc;
@@ -666,6 +673,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
         dev->fact_ev.push_back(e);
     }
     if (rot) dev->bubrot.ensure(kc * job.n_tot * sizeof(D4));
+    dev->tc_atab_valid = false;  // the time-phase digits are built by this call's first chunk
     if (!nested) {
         dev->counters.ensure(64);
         CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
@@ -699,8 +707,8 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             fb = (const D4*)dev->bubrot.p;
         }
         CUDA_OK(cudaEventRecord(cev[0], dev->stream));
-        launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, job.n_phi, kn, (double*)dev->tau.p,
-                             nullptr, (unsigned long long*)dev->counters.p, k0 == 0, &launches);
+        launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, ranges, job.n_sel, dirs, nd, job.n_phi, kn,
+                             (double*)dev->tau.p, nullptr, (unsigned long long*)dev->counters.p, k0 == 0, &launches);
         CUDA_OK(cudaEventRecord(cev[1], dev->stream));
         if (job.kernel == BGWX_KERNEL_FP64_DIRECT) {
             SpecArgs A;
@@ -745,7 +753,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             ++launches;
         } else {
             launches += launch_factored(dev, job, fb, sel, (const double*)dev->tau.p, cos_t, sin2, cos2, coeffs,
-                                        powers, t_arr, cutw, w, kn, final_out + k0 * per, &dev->fact_ev[3 * ci]);
+                                        powers, t_arr, cutw, w, k0, kn, final_out, real_tiles, &dev->fact_ev[3 * ci]);
         }
         CUDA_OK(cudaEventRecord(cev[2], dev->stream));
     }
@@ -755,7 +763,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
         if (!nested) check_counters(dev, nullptr);
         return;
     }
-    CUDA_OK(cudaMemcpyAsync(out, final_out, K * per * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
+    CUDA_OK(cudaMemcpyAsync(out, final_out, out_blocks * per * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
     unsigned long long fbk = 0;
     check_counters(dev, &fbk);
     float total = 0, ms_masks = 0, ms_spec = 0;
@@ -784,39 +792,77 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
         tm->launches += launches;
         tm->directions += K * job.n_sel * nd;
         tm->fallbacks += fbk;
-        tm->d2h_bytes += (double)(K * per * sizeof(double2));
+        tm->d2h_bytes += (double)(out_blocks * per * sizeof(double2));
     }
 }
 
-void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out, BgwxTimings* tm) {
+void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out, BgwxTimings* tm, bool autotune) {
     CUDA_OK(cudaSetDevice(dev->id));
     const size_t R = jobs.size();
     if (R == 0) return;
-    const size_t per_r = jobs[0].n_k * 2 * jobs[0].n_sets * jobs[0].n_w;  // complex values per realization
+    const SpectrumJob& j0 = jobs[0];
+    const size_t per_r = j0.n_k * 2 * j0.n_sets * j0.n_w;  // complex values per realization
+    const bool batched = j0.kernel != BGWX_KERNEL_FP64_DIRECT;
+    // One job over every realization: bubbles one realization after another, radiating slots
+    // padded so that each realization starts a GEMM column tile; each launch of the pipeline
+    // (rotation, masks, beta, GEMM, reduction) then covers all realizations of its frames.
+    SpectrumJob b = j0;
+    std::vector<double> bub;
+    std::vector<uint32_t> sel, ranges, real_tiles(R + 1, 0);
+    size_t radiating = 0;
+    if (batched) {
+        const size_t bpt = factored_bubbles_per_tile(j0);
+        size_t rows = 0, tiles = 0;
+        for (size_t r = 0; r < R; ++r) {
+            const SpectrumJob& j = jobs[r];
+            real_tiles[r] = (uint32_t)tiles;
+            bub.insert(bub.end(), j.bubbles, j.bubbles + 4 * j.n_tot);
+            const size_t nt = (j.n_sel + bpt - 1) / bpt;
+            for (size_t q = 0; q < nt * bpt; ++q) {
+                sel.push_back(q < j.n_sel ? (uint32_t)(rows + j.sel[q]) : kNoSlot);
+                ranges.push_back((uint32_t)rows);
+                ranges.push_back((uint32_t)j.n_tot);
+            }
+            rows += j.n_tot;
+            tiles += nt;
+            radiating += j.n_sel;
+            if (rows > 0xFFFFFFF0ULL || sel.size() > 0x7FFFFFFFULL) throw Error{"ensemble too large for one call"};
+        }
+        real_tiles[R] = (uint32_t)tiles;
+        b.bubbles = bub.data();
+        b.n_tot = rows;
+        b.n_int = rows;  // sel holds indices into the whole array; padding slots are kNoSlot
+        b.sel = sel.data();
+        b.n_sel = sel.size();
+        b.ranges = ranges.data();
+        b.real_tiles = real_tiles.data();
+        b.n_real = R;
+        if (autotune && radiating > 0) {
+            const LaunchShape s = autotune_launch_shape(dev, b);
+            b.frames_per_launch = s.frames_per_launch;
+            b.row_parts = s.row_parts;
+            b.gemm_stages = s.gemm_stages;
+        }
+    }
     dev->ens_out.ensure(R * per_r * sizeof(double2));
     double2* eo = (double2*)dev->ens_out.p;
     CUDA_OK(cudaMemsetAsync(eo, 0, R * per_r * sizeof(double2), dev->stream));
-    std::vector<size_t> order(R);
-    for (size_t r = 0; r < R; ++r) order[r] = r;
-    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) {
-        return jobs[a].n_sel * jobs[a].n_tot > jobs[b].n_sel * jobs[b].n_tot;
-    });
     BgwxTimings local{};
     dev->counters.ensure(64);
     CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
     CUDA_OK(cudaEventRecord(dev->ev[6], dev->stream));
-    // every realization shares the (w, cos-theta, t) grid: the time-phase
-    // digits are built by the first call and reused by the others
-    struct Reuse {
-        Device* d;
-        explicit Reuse(Device* d_) : d(d_) { d->tc_key_reuse = false; }
-        void on() { d->tc_key_reuse = true; }
-        ~Reuse() { d->tc_key_reuse = false; }
-    } reuse(dev);
-    for (size_t r : order) {
-        if (jobs[r].n_sel == 0) continue;
-        run_spectrum(dev, jobs[r], reinterpret_cast<double*>(eo + r * per_r), true, &local, true);
-        reuse.on();
+    if (batched) {
+        if (radiating > 0) run_spectrum(dev, b, reinterpret_cast<double*>(eo), true, &local, true);
+    } else {
+        std::vector<size_t> order(R);
+        for (size_t r = 0; r < R; ++r) order[r] = r;
+        std::stable_sort(order.begin(), order.end(), [&](size_t x, size_t y) {
+            return jobs[x].n_sel * jobs[x].n_tot > jobs[y].n_sel * jobs[y].n_tot;
+        });
+        for (size_t r : order) {
+            if (jobs[r].n_sel == 0) continue;
+            run_spectrum(dev, jobs[r], reinterpret_cast<double*>(eo + r * per_r), true, &local, true);
+        }
     }
     CUDA_OK(cudaEventRecord(dev->ev[7], dev->stream));
     CUDA_OK(cudaMemcpyAsync(out, eo, R * per_r * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
@@ -900,7 +946,7 @@ void run_adjoint(Device* dev, const SpectrumJob& job, const double* gbar, double
             ++launches;
             fb = (const D4*)dev->bubrot.p;
         }
-        launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, job.n_phi, kn, (double*)dev->tau.p,
+        launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, nullptr, job.n_sel, dirs, nd, job.n_phi, kn, (double*)dev->tau.p,
                              (int32_t*)dev->codes.p, (unsigned long long*)dev->counters.p, k0 == 0, &launches);
         launches += launch_adjoint_chunk(dev, job, fb, sel, (const double*)dev->tau.p, (const int32_t*)dev->codes.p,
                                          dirs, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w,
@@ -977,7 +1023,7 @@ void run_integrand(Device* dev, const SpectrumJob& job, double* out, BgwxTimings
         CUDA_OK(cudaFuncSetAttribute(k_tensor_direct<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     uint64_t launches = 0;
     CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
-    launch_mask_pipeline(dev, bub, bub, job.n_int, job.n_tot, sel, job.n_sel, dirs, nd, job.n_phi, 1, (double*)dev->tau.p,
+    launch_mask_pipeline(dev, bub, bub, job.n_int, job.n_tot, sel, nullptr, job.n_sel, dirs, nd, job.n_phi, 1, (double*)dev->tau.p,
                          nullptr, (unsigned long long*)dev->counters.p, true, &launches);
     for (size_t s0 = 0; s0 < job.n_sel; s0 += chunk) {
         const size_t n = std::min(chunk, job.n_sel - s0);

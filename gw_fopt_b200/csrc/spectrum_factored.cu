@@ -61,9 +61,9 @@ __global__ void k_time_tables(const D4* __restrict__ bub, const uint32_t* __rest
                               const double* __restrict__ t_arr, int n_t, const double* __restrict__ powers,
                               const double* __restrict__ coeffs, const double* __restrict__ cutw, int SM,
                               int has_damp, double damp, double* __restrict__ D, int* __restrict__ kfirst) {
-    const int slot = blockIdx.y;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (slot >= n_sel || k >= n_t) return;
+    const int slot = blockIdx.x;
+    const int k = blockIdx.y * blockDim.x + threadIdx.x;
+    if (slot >= n_sel || k >= n_t || sel[slot] == kNoSlot) return;
     const double ta = bub[sel[slot]].t;
     const double dt = t_arr[k] - ta;
     double* row = D + ((size_t)slot * n_t + k) * (1 + SM);
@@ -174,17 +174,29 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
     int* boff = reinterpret_cast<int*>(pbeg + (size_t)2 * SMC * NB);  // [NB+1]
     int* brun = boff + NB + 1;                                  // [NB]
     uint8_t* evs = reinterpret_cast<uint8_t*>(brun + NB);       // [n_phi + 4] step of each event within its block
+    // a crowded event block's per-step counts and running offsets [2][32], and its events in step order [n_phi]
+    int* scnt = reinterpret_cast<int*>(evs + ((A.n_phi + 4 + 3) & ~3));
+    uint16_t* sperm = reinterpret_cast<uint16_t*>(scnt + 64);
     const int slot = (int)((row / A.n_cos) % A.n_sel);
+    if (A.sel[slot] == kNoSlot) return;  // a padding slot of a batched job: its columns are never read
     const int i = (int)(row % A.n_cos);
     const long frame = row / ((long)A.n_cos * A.n_sel);
-    const double ta = A.bub[A.sel[slot]].t;
     const double* trow = A.tau + (size_t)row * A.n_phi;
+    // The delays of patches j = lane + 32 jj, jj < kMaxJ, are loaded first, all at once (one
+    // memory latency for the row), and kept for both passes over the patches.
+    constexpr int kMaxJ = 6;
+    double tj_c[kMaxJ];
+#pragma unroll
+    for (int jj = 0; jj < kMaxJ; ++jj) {
+        const int j = 32 * jj + lane;
+        tj_c[jj] = j < A.n_phi ? __ldcs(trow + j) : 0.0;
+    }
+    const double ta = A.bub[A.sel[slot]].t;
     const unsigned full = 0xffffffffu;
     const double inv_dt = 1.0 / A.dt;  // the estimate below is only a starting point
-    auto block_of = [&](int j, int& kj) -> int {
+    auto block_of = [&](int j, double tj, int& kj) -> int {
         kj = A.n_t;
         if (j >= A.n_phi) return -2;  // not a patch
-        const double tj = trow[j];
         if (!(tj > 0.0)) return -1;    // never collides
         // first k with (t_k - t_a) >= tau_j: arithmetic estimate, then exact
         // comparisons (the predicate is monotone in k) settle the boundary
@@ -199,7 +211,6 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
     __syncwarp();
     // pass 1: events per block; never-colliding weights (lane sums, fixed-order reduction).
     // The first collided step of patches j = lane + 32 jj, jj < kMaxJ, is kept for pass 2.
-    constexpr int kMaxJ = 8;
     int kj_c[kMaxJ], b_c[kMaxJ];
     double nc = 0.0, ns = 0.0;
     auto pass1 = [&](int j, int b) {
@@ -217,13 +228,14 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
         if (32 * jj >= A.n_phi) break;
         const int j = 32 * jj + lane;
         kj_c[jj] = 0;
-        b_c[jj] = block_of(j, kj_c[jj]);
+        b_c[jj] = block_of(j, tj_c[jj], kj_c[jj]);
         pass1(j, b_c[jj]);
     }
     for (int j0 = 32 * kMaxJ; j0 < A.n_phi; j0 += 32) {
         int kj;
-        const int b = block_of(j0 + lane, kj);
-        pass1(j0 + lane, b);
+        const int j = j0 + lane;
+        const int b = block_of(j, j < A.n_phi ? trow[j] : 0.0, kj);
+        pass1(j, b);
     }
     for (int o = 16; o > 0; o >>= 1) {
         nc += __shfl_down_sync(full, nc, o);
@@ -242,7 +254,7 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
     __syncwarp();
     // pass 2: scatter events (stable in j within a block)
     const unsigned lt = (1u << lane) - 1u;
-    auto pass2 = [&](int j, int kj, int b) {
+    auto pass2 = [&](int j, double tj, int kj, int b) {
         const unsigned m = __match_any_sync(full, b);
         int pos = 0;
         if (b >= 0) pos = brun[b] + __popc(m & lt);
@@ -251,7 +263,6 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
         __syncwarp();
         if (b >= 0) {
             evs[pos] = (uint8_t)(kj & 31);
-            const double tj = trow[j];
             const double wj = (j == 0 || j == A.n_phi - 1) ? 0.5 : 1.0;
             const double qc = wj * A.cos2[j], qs = wj * A.sin2[j];
             double* q = evq + pos;
@@ -269,12 +280,14 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
 #pragma unroll
     for (int jj = 0; jj < kMaxJ; ++jj) {
         if (32 * jj >= A.n_phi) break;
-        pass2(32 * jj + lane, kj_c[jj], b_c[jj]);
+        pass2(32 * jj + lane, tj_c[jj], kj_c[jj], b_c[jj]);
     }
     for (int j0 = 32 * kMaxJ; j0 < A.n_phi; j0 += 32) {
         int kj;
-        const int b = block_of(j0 + lane, kj);
-        pass2(j0 + lane, kj, b);
+        const int j = j0 + lane;
+        const double tj = j < A.n_phi ? trow[j] : 0.0;
+        const int b = block_of(j, tj, kj);
+        pass2(j, tj, kj, b);
     }
     __syncwarp();
     // block totals of every weight: the lanes take a block's events in strides
@@ -422,36 +435,46 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
         double dq[NQ];
 #pragma unroll
         for (int q = 0; q < NQ; ++q) dq[q] = 0.0;
-        if (NB >= 32 && e1 - e0 > 32) {
-            // Many events: lanes take 32 events at a time; the events of one step
-            // (a __match_any group) are added by the group's lowest lane in event
-            // order and the group sum is added to that step's row of a table in the
-            // (by now unused) block-total array, rounds in event order.
-            double* D = btot;  // [NQ][32 steps]
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) D[q * 32 + lane] = 0.0;
+        if (e1 - e0 > 32) {
+            // Many events: the block's events are counting-sorted by their step (stable in event
+            // order; ranks within 32 events from __match_any groups), then each lane adds the
+            // events of its own step in event order.
+            int* run = scnt + 32;
+            scnt[lane] = 0;
             __syncwarp();
             for (int r0 = e0; r0 < e1; r0 += 32) {
                 const int e = r0 + lane;
-                const bool valid = e < e1;
-                const int se = valid ? (int)evs[e] : 32 + lane;
+                const int se = e < e1 ? (int)evs[e] : 32 + lane;
                 const unsigned m = __match_any_sync(full, se);
-                if (valid && lane == __ffs(m) - 1) {
-                    double g[NQ];
-#pragma unroll
-                    for (int q = 0; q < NQ; ++q) g[q] = 0.0;
-                    for (unsigned mm = m; mm; mm &= mm - 1) {
-                        const double* qe = evq + (r0 + __ffs(mm) - 1);
-#pragma unroll
-                        for (int q = 0; q < NQ; ++q) g[q] += qe[(size_t)q * EV];
-                    }
-#pragma unroll
-                    for (int q = 0; q < NQ; ++q) D[q * 32 + se] += g[q];
-                }
+                if (e < e1 && lane == __ffs(m) - 1) scnt[se] += __popc(m);
                 __syncwarp();
             }
+            const int c = scnt[lane];
+            int incl = c;
 #pragma unroll
-            for (int q = 0; q < NQ; ++q) dq[q] = D[q * 32 + lane];
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(full, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int ex = incl - c;  // first position of this lane's step
+            run[lane] = ex;
+            __syncwarp();
+            const unsigned lt = (1u << lane) - 1u;
+            for (int r0 = e0; r0 < e1; r0 += 32) {
+                const int e = r0 + lane;
+                const bool v = e < e1;
+                const int se = v ? (int)evs[e] : 32 + lane;
+                const unsigned m = __match_any_sync(full, se);
+                if (v) sperm[run[se] + __popc(m & lt)] = (uint16_t)e;
+                __syncwarp();
+                if (v && lane == __ffs(m) - 1) run[se] += __popc(m);
+                __syncwarp();
+            }
+            for (int r = 0; r < c; ++r) {
+                const double* qe = evq + sperm[ex + r];
+#pragma unroll
+                for (int q = 0; q < NQ; ++q) dq[q] += qe[(size_t)q * EV];
+            }
             __syncwarp();
         } else {
             const uint32_t pat = 0x01010101u * (uint32_t)lane;
@@ -500,8 +523,7 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
         // (a) Every event block is formed once (lane = step) and its 2S values are kept for the
         //     digits: a block of at least 32 events in its own weight slots (plane 2s + g, slots
         //     boff[b] + lane; its weights are not read again), smaller blocks in the block-total
-        //     table while it has room (the rest are formed again in (c)).  Blocks that use the
-        //     block-total table as their step table (more than 32 events) go first.
+        //     table while it has room (the rest are formed again in (c)).
         // (b) In a block without events U and Pm are constant, so beta = rf (D0(k) U + sum_m Dm(k)
         //     Pm) is bounded by interval arithmetic over the per-block ranges of the time table;
         //     such blocks are formed (lane = step) in decreasing order of their bound until no
@@ -522,37 +544,29 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
             stride = 32;
             return w >= 0 ? btot + (size_t)w * 64 * A.S : nullptr;
         };
-        for (int sweep = 0; sweep < 2; ++sweep) {
-            for (int bc = 0; bc < NB; bc += 32) {
-                const int bl = bc + lane;
-                const int cnt = bl < NB ? boff[bl + 1] - boff[bl] : 0;
-                const bool pick = sweep == 0 ? cnt >= 32 : (cnt > 0 && cnt < 32);
-                for (unsigned h = __ballot_sync(full, pick); h; h &= h - 1) {
-                    const int b = bc + __ffs(h) - 1;
-                    double P[2 * SMC], Uc, Us;
-                    step_sums(b, P, Uc, Us);
-                    const int k = (b << 5) + lane;
-                    int code = -1;
-                    if (sweep == 0)
-                        code = -2;
-                    else if (used_tab < n_tab)
-                        code = used_tab++;
-                    __syncwarp();
-                    if (lane == 0) where[b] = code;
-                    __syncwarp();
-                    int stride = 0;
-                    double* dst = kept(b, stride);
-                    for (int s2 = 0; s2 < A.S; ++s2) {
-                        double xc, xs;
-                        value(k, s2, P, Uc, Us, rf, xc, xs);
-                        vmax = fmax(vmax, fmax(fabs(xc), fabs(xs)));
-                        if (dst) {
-                            dst[(size_t)(2 * s2) * stride + lane] = xc;
-                            dst[(size_t)(2 * s2 + 1) * stride + lane] = xs;
-                        }
+        for (int bc = 0; bc < NB; bc += 32) {
+            const int bl = bc + lane;
+            for (unsigned h = __ballot_sync(full, bl < NB && boff[bl] != boff[bl + 1]); h; h &= h - 1) {
+                const int b = bc + __ffs(h) - 1;
+                double P[2 * SMC], Uc, Us;
+                step_sums(b, P, Uc, Us);
+                const int k = (b << 5) + lane;
+                const int code = boff[b + 1] - boff[b] >= 32 ? -2 : (used_tab < n_tab ? used_tab++ : -1);
+                __syncwarp();
+                if (lane == 0) where[b] = code;
+                __syncwarp();
+                int stride = 0;
+                double* dst = kept(b, stride);
+                for (int s2 = 0; s2 < A.S; ++s2) {
+                    double xc, xs;
+                    value(k, s2, P, Uc, Us, rf, xc, xs);
+                    vmax = fmax(vmax, fmax(fabs(xc), fabs(xs)));
+                    if (dst) {
+                        dst[(size_t)(2 * s2) * stride + lane] = xc;
+                        dst[(size_t)(2 * s2 + 1) * stride + lane] = xs;
                     }
-                    __syncwarp();
                 }
+                __syncwarp();
             }
         }
 #pragma unroll
@@ -597,7 +611,11 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
                         bi = oi;
                     }
                 }
-                if (!(bb > vmax)) break;  // every remaining bound is covered
+                // Every remaining bound is covered once no bound exceeds vmax (1 + 1e-10): a value up
+                // to that much above the scale still maps to |x F| <= F + 0.22, which rounds into the
+                // digit range.  (Without the slack, blocks whose values all equal the maximum, as after
+                // the last collision with powers = 3, would each be formed.)
+                if (!(bb > vmax * (1.0 + 1e-10))) break;
                 {
                     const int b = bc + bi, k = (b << 5) + lane;
                     const double* P = pbeg + (size_t)b * 2 * SMC;
@@ -743,6 +761,10 @@ template <class Real, int SMC>
 static void launch_beta_smc(const BetaArgs& B, Real* out, size_t smem, unsigned blocks, int threads,
                             cudaStream_t st) {
     CUDA_OK(cudaFuncSetAttribute(k_beta<Real, SMC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // three blocks per SM need the largest shared-memory carveout; without the preference the
+    // driver may pick a smaller one (two blocks per SM) depending on the kernels run before
+    CUDA_OK(cudaFuncSetAttribute(k_beta<Real, SMC>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 (int)cudaSharedmemCarveoutMaxShared));
     k_beta<Real, SMC><<<blocks, threads, smem, st>>>(B, out);
 }
 
@@ -822,7 +844,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm(FactArgs A) {
 
     if (tid < 64) {
         const int slot = tile * A.bpt + tid;
-        const bool ok = tid < A.bpt && slot < A.n_sel;
+        const bool ok = tid < A.bpt && slot < A.n_sel && A.sel[slot] != kNoSlot;
         binfo[tid] = ok ? slot : -1;
         if (ok) {
             const D4 xa = B[A.sel[slot]];
@@ -1028,6 +1050,25 @@ __global__ void k_reduce_tiles(const double2* __restrict__ partial, int tiles, s
     out[(size_t)k * per + q] = acc;
 }
 
+// Batched jobs: frame k of realization r is the sum of its own column tiles'
+// partials, in the order of k_reduce_tiles (tiles, then row parts).
+__global__ void k_reduce_real(const double2* __restrict__ partial, const uint32_t* __restrict__ real_tiles,
+                              int tiles_per_frame, int parts, size_t per, int kn, size_t n_k, size_t k0,
+                              double2* __restrict__ out) {
+    const size_t q = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = blockIdx.y;
+    const int r = blockIdx.z;
+    if (q >= per || k >= kn) return;
+    double2 acc = make_double2(0.0, 0.0);
+    const double2* p = partial + (size_t)k * tiles_per_frame * parts * per + q;
+    for (size_t t = (size_t)real_tiles[r] * parts; t < (size_t)real_tiles[r + 1] * parts; ++t) {
+        const double2 v = p[t * per];
+        acc.x += v.x;
+        acc.y += v.y;
+    }
+    out[((size_t)r * n_k + k0 + k) * per + q] = acc;
+}
+
 // ---------------------------------------------------------------------------
 template <class Real, int TN>
 static size_t gemm_smem_bytes(int S) {
@@ -1066,11 +1107,29 @@ static FactGeom fact_geom(const SpectrumJob& job, size_t real_size) {
     return g;
 }
 
+// Sums the column-tile partials of kn frames: per frame (single job) or per
+// (realization, frame) (batched job).
+static uint64_t reduce_tiles(Device* dev, const SpectrumJob& job, const double2* partial, int tiles_per_frame,
+                             int parts, size_t per, size_t k0, size_t kn, double2* out, const uint32_t* real_tiles) {
+    if (job.n_real > 0) {
+        if (job.n_real > 65535) throw Error{"too many realizations in one batched call"};
+        dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn, (unsigned)job.n_real);
+        k_reduce_real<<<gr, 256, 0, dev->stream>>>(partial, real_tiles, tiles_per_frame, parts, per, (int)kn,
+                                                   job.n_k, k0, out);
+    } else {
+        dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
+        k_reduce_tiles<<<gr, 256, 0, dev->stream>>>(partial, tiles_per_frame * parts, per, (int)kn, out + k0 * per);
+    }
+    CUDA_OK(cudaGetLastError());
+    return 1;
+}
+
 template <class Real>
 static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_frames, const uint32_t* sel,
                              const double* tau, const double* cos_t, const double* sin2, const double* cos2,
                              const double* coeffs, const double* powers, const double* t_arr, const double* cutw,
-                             const double* w, size_t kn, double2* out, cudaEvent_t* ev3) {
+                             const double* w, size_t k0, size_t kn, double2* out, const uint32_t* real_tiles,
+                             cudaEvent_t* ev3) {
     const int S = (int)job.n_sets, M = (int)job.n_terms, SM = S * M;
     const int n_t = (int)job.n_t, n_cos = (int)job.n_cos, n_phi = (int)job.n_phi, n_w = (int)job.n_w;
     const int n_sel = (int)job.n_sel;
@@ -1087,9 +1146,9 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     // per-bubble time tables (frame independent)
     dev->fact_D.ensure((size_t)n_sel * n_t * (1 + SM) * sizeof(double));
     dev->fact_kfirst.ensure((size_t)n_sel * sizeof(int));
-    if (n_sel > 65535) throw Error{"too many radiating bubbles for the time-table grid"};
+    if ((n_t + 127) / 128 > 65535) throw Error{"too many time steps for the time-table grid"};
     {
-        dim3 g((unsigned)((n_t + 127) / 128), (unsigned)n_sel);
+        dim3 g((unsigned)n_sel, (unsigned)((n_t + 127) / 128));
         k_time_tables<<<g, 128, 0, dev->stream>>>(bub_frames, sel, n_sel, t_arr, n_t, powers, coeffs, cutw, SM,
                                                   job.has_damping ? 1 : 0, job.damping, (double*)dev->fact_D.p,
                                                   (int*)dev->fact_kfirst.p);
@@ -1148,7 +1207,8 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         B.t_pad = G.t_pad;
         const int NQ = 2 + 2 * SM;
         size_t pw = (size_t)n_phi * NQ * sizeof(double) + 2 * (size_t)NQ * G.nblk * sizeof(double) +
-                    (2 * (size_t)G.nblk + 1) * sizeof(int) + ((size_t)n_phi + 4);
+                    (2 * (size_t)G.nblk + 1) * sizeof(int) + (((size_t)n_phi + 4 + 3) & ~(size_t)3) +
+                    64 * sizeof(int) + (size_t)n_phi * sizeof(uint16_t);
         pw = (pw + 15) & ~(size_t)15;
         B.per_warp_bytes = (int)pw;
         B.tiles = G.tiles_per_frame;
@@ -1194,24 +1254,15 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
     dev->fact_partial.ensure((size_t)kn * G.tiles_per_frame * row_parts * per * sizeof(double2));
     A.partial = (double2*)dev->fact_partial.p;
     if constexpr (tc) {
-        // time-phase digits: frame independent; rebuilt on every call unless the
-        // caller (the batched ensemble) runs several calls on one grid
+        // time-phase digits: frame independent, built by the first launch chunk of each call
+        // (0.8 ms at config 3) and reused by the others
         const int n_wt = (n_w + 63) / 64;
         const size_t atab_bytes = (size_t)n_cos * n_wt * nkb * kI8BlockSet;
-        std::vector<double> key;
-        key.reserve(3 + n_w + n_cos + n_t);
-        key.push_back((double)n_w);
-        key.push_back((double)n_cos);
-        key.push_back((double)n_t);
-        key.insert(key.end(), job.w, job.w + n_w);
-        key.insert(key.end(), job.cos_thetax, job.cos_thetax + n_cos);
-        key.insert(key.end(), job.t_arr, job.t_arr + n_t);
-        const bool had = dev->tc_atab.p && dev->tc_atab.cap >= atab_bytes;
-        dev->tc_atab.ensure(atab_bytes);
-        if (!had || !dev->tc_key_reuse || dev->tc_key != key) {
+        if (!dev->tc_atab_valid || dev->tc_atab.cap < atab_bytes) {
+            dev->tc_atab.ensure(atab_bytes);
             launch_tc_phase_table(w, cos_t, t_arr, n_cos, n_w, n_t, (int8_t*)dev->tc_atab.p, dev->stream);
             ++launches;
-            dev->tc_key = key;
+            dev->tc_atab_valid = true;
         }
         TcArgs T;
         T.bub = bub_frames;
@@ -1240,10 +1291,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         launch_gemm_tc(T, kn, dev->stream);
         ++launches;
         CUDA_OK(cudaEventRecord(ev3[2], dev->stream));
-        dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
-        k_reduce_tiles<<<gr, 256, 0, dev->stream>>>(A.partial, G.tiles_per_frame * row_parts, per, (int)kn, out);
-        CUDA_OK(cudaGetLastError());
-        ++launches;
+        launches += reduce_tiles(dev, job, A.partial, G.tiles_per_frame, row_parts, per, k0, kn, out, real_tiles);
         return launches;
     } else {
         constexpr int TN = gemm_tn<Real>();
@@ -1257,10 +1305,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         CUDA_OK(cudaGetLastError());
         ++launches;
         CUDA_OK(cudaEventRecord(ev3[2], dev->stream));
-        dim3 gr((unsigned)((per + 255) / 256), (unsigned)kn);
-        k_reduce_tiles<<<gr, 256, 0, dev->stream>>>(A.partial, G.tiles_per_frame, per, (int)kn, out);
-        CUDA_OK(cudaGetLastError());
-        ++launches;
+        launches += reduce_tiles(dev, job, A.partial, G.tiles_per_frame, 1, per, k0, kn, out, real_tiles);
         return launches;
     }
 }
@@ -1268,15 +1313,23 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
 uint64_t launch_factored(Device* dev, const SpectrumJob& job, const D4* bub_frames, const uint32_t* sel,
                          const double* tau, const double* cos_t, const double* sin2, const double* cos2,
                          const double* coeffs, const double* powers, const double* t_arr, const double* cutw,
-                         const double* w, size_t kn, double2* out, cudaEvent_t* ev3) {
+                         const double* w, size_t k0, size_t kn, double2* out, const uint32_t* real_tiles,
+                         cudaEvent_t* ev3) {
     if (job.kernel == BGWX_KERNEL_MIXED)
         return launch_typed<int8_t>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w,
-                                    kn, out, ev3);
+                                    k0, kn, out, real_tiles, ev3);
     if (job.kernel == BGWX_KERNEL_MIXED_SIMT)
         return launch_typed<float>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w,
-                                   kn, out, ev3);
-    return launch_typed<double>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, kn,
-                                out, ev3);
+                                   k0, kn, out, real_tiles, ev3);
+    return launch_typed<double>(dev, job, bub_frames, sel, tau, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w, k0,
+                                kn, out, real_tiles, ev3);
+}
+
+size_t factored_bubbles_per_tile(const SpectrumJob& job) {
+    const size_t real = job.kernel == BGWX_KERNEL_MIXED        ? 1
+                        : job.kernel == BGWX_KERNEL_MIXED_SIMT ? sizeof(float)
+                                                               : sizeof(double);
+    return (size_t)fact_geom(job, real).bpt;
 }
 
 int factored_auto_row_parts(const Device* dev, const SpectrumJob& job, size_t kn) {

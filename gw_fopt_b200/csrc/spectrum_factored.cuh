@@ -32,13 +32,16 @@ __device__ __forceinline__ void phase<float>(double arg, double& s, double& c) {
 }
 
 
-// Launches the factored spectrum for kn frames whose masks are in `tau`;
-// writes (kn, 2, S, W) complex sums into out.  Returns the number of kernel
+// Launches the factored spectrum for frames [k0, k0 + kn) whose masks are in
+// `tau`; writes (kn, 2, S, W) complex sums into out + k0 (2 S W), or, for a
+// batched job (job.n_real > 0; real_tiles on the device), frame k of
+// realization r into out + (r n_k + k) (2 S W).  Returns the number of kernel
 // launches.
 uint64_t launch_factored(Device* dev, const SpectrumJob& job, const D4* bub_frames, const uint32_t* sel,
                          const double* tau, const double* cos_t, const double* sin2, const double* cos2,
                          const double* coeffs, const double* powers, const double* t_arr, const double* cutw,
-                         const double* w, size_t kn, double2* out, cudaEvent_t* ev3);
+                         const double* w, size_t k0, size_t kn, double2* out, const uint32_t* real_tiles,
+                         cudaEvent_t* ev3);
 
 // Device bytes per k-hat frame of the factored path's work arrays.
 size_t factored_bytes_per_frame(const SpectrumJob& job);

@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) k_gemm_i8(TcArgs A) {
 
     if (tid < 64) {
         const int slot = tile * A.bpt + tid;
-        const bool ok = tid < A.bpt && slot < A.n_sel;
+        const bool ok = tid < A.bpt && slot < A.n_sel && A.sel[slot] != kNoSlot;
         binfo[tid] = ok ? slot : -1;
         bt[tid] = 0.0;
         bz[tid] = 0.0;

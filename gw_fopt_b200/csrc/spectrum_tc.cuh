@@ -30,8 +30,12 @@ constexpr double kI8Full = 2139062143.0;  // F = 0x7F7F7F7F
 // x y = (256^6 / F^2) sum_L 256^-L sum_{s+r=L} d_s(x) d_r(y) for the digit
 // pairs of level L = s + r
 constexpr double kI8PairScale = 281474976710656.0 / (kI8Full * kI8Full);
+// X is the low word of x F + 1.5 2^52: the sum lies in [2^52, 2^53), where the
+// spacing of doubles is 1, so the fused multiply-add rounds x F to an integer
+// and the low 32 mantissa bits hold it in two's complement.
 __device__ __forceinline__ uint32_t i8_digits(double x) {
-    const uint32_t y = (uint32_t)__double2int_rn(x * kI8Full) + 0x80808080u;
+    const double r = fma(x, kI8Full, 6755399441055744.0);
+    const uint32_t y = (uint32_t)__double2loint(r) + 0x80808080u;
     return __byte_perm(y ^ 0x80808080u, 0u, 0x0123);
 }
 

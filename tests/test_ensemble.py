@@ -114,3 +114,29 @@ def test_config4_realizations_per_w(gpu_available):
         e = err_per_w(out["mixed"][q], out["fp64_factored"][q])
         print(f"config4 realization {r} ({sizes[r]} bubbles): mixed vs fp64_factored per-w {e:.3e}")
         assert e < 1e-6
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kernel", ["mixed", "fp64_factored"])
+def test_batched_multi_tile_realizations_bitwise(gpu_available, kernel):
+    """Realizations of more than one GEMM column tile (70 and 150 radiating bubbles, the column
+    tiles padded per realization) next to a 3-bubble one, in one batched call: every realization's
+    block equals its own single-configuration call bit for bit when both use the same cos-theta row
+    split, and the masks of each realization see only its own colliders."""
+    reals = [W.exponential_nucleation(70, 9.0, seed=5), W.exponential_nucleation(3, 6.0, seed=6),
+             W.exponential_nucleation(150, 12.0, seed=7)]
+    n_cos, n_phi, n_t = 24, 16, 96
+    w = np.geomspace(1.0, 500.0, 10)
+    kh = W.fibonacci_khat(2)
+    co, po = [[1.0]], [[5.0]]
+    ens = BulkFlowEnsemble(reals, validate=False)
+    ens.set_resolution(n_cos, n_phi)
+    ens.set_gradient_scaling_params(co, po)
+    ens.set_kernel(kernel)
+    L.check(L.lib().bgwx_generalized_bulk_flow_set_launch_shape(ens._h, 1, 2))
+    out = ens.compute_c_integral_khat(w, kh, t_end=1.5, n_t=n_t)
+    for r, (inter, ext) in enumerate(reals):
+        g = make_flow(inter, ext, n_cos, n_phi, co, po, kernel=kernel)
+        g.set_launch_shape(2, 2)
+        single = g.compute_c_integral_khat(w, kh, t_end=1.5, n_t=n_t)
+        assert np.array_equal(out[r], single), r
