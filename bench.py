@@ -476,6 +476,7 @@ def run_ensemble_bench(args, once=False):
         run()
         t = ens.last_timings()
         print(json.dumps({"config": c.name, "kernel": args.kernel, "total_ms": t["total_ms"],
+                          "masks_ms": t["masks_ms"], "beta_ms": t["beta_ms"], "gemm_ms": t["gemm_ms"],
                           "launches": t["launches"], "pte_per_s": pte / (t["total_ms"] * 1e-3)}), flush=True)
         return
     for _ in range(args.warmup):
@@ -493,7 +494,8 @@ def run_ensemble_bench(args, once=False):
             "dtype": "int8x4+f64" if args.kernel == "mixed" else args.kernel, "data": "synthetic",
             "config": {"workload": c.name, "realizations": len(c.realizations), "n_khat": int(c.khat.shape[0]),
                        "bubbles": int(sum(r[0].shape[0] for r in c.realizations)), "kernel": args.kernel,
-                       "pte_per_step": pte},
+                       "pte_per_step": pte,
+                       "stages_ms": {k: t[k] for k in ("masks_ms", "beta_ms", "gemm_ms")}},
             "e2e": {"value": pte / (np.mean(wall_ms) * 1e-3), "unit": UNIT, "h2d_bytes_per_step": int(t["h2d_bytes"]),
                     "d2h_bytes_per_step": int(t["d2h_bytes"]), "ms_per_step": float(np.mean(wall_ms)),
                     "timing": "host wall clock around the synchronous public call"},
@@ -560,6 +562,21 @@ def run_adjoint_bench(args, once=False):
                        "forward_ms": float(np.mean(fwd)), "backward_ms": float(np.mean(bwd)), "loss": loss},
             "e2e": {"value": pte / (np.mean(wall) * 1e-3), "unit": UNIT, "ms_per_step": float(np.mean(wall)),
                     "timing": "host wall clock of the whole fit step"}}
+    if not args.no_compare and args.kernel != "fp64_factored":
+        # the forward spectrum of the fitted parameters against the FP64 factored kernel, per w
+        ref_model = BulkFlowSpectrum(n_cos=c.n_cos, n_phi=c.n_phi, w=c.w, khat=c.khat, t_end=c.t_end, n_t=c.n_t,
+                                     t_begin=c.t_begin, box=1.0, kernel="fp64_factored")
+        with torch.no_grad():
+            co, po = fit()
+            got = model(co, po, x).numpy()
+            ref = ref_model(co, po, x).numpy()
+        d = (got - ref).reshape(-1, c.w.size, 2) if got.shape[-1] == 2 else (got - ref).reshape(-1, c.w.size)
+        r = ref.reshape(d.shape)
+        ax = tuple(q for q in range(d.ndim) if q != 1)
+        per_w = np.sqrt((d ** 2).sum(axis=ax)) / np.sqrt((r ** 2).sum(axis=ax))
+        line["compare"] = {"mixed_error_vs_fp64": {"per_w_max": float(per_w.max()),
+                                                   "global": float(np.linalg.norm(d) / np.linalg.norm(r)),
+                                                   "sample": "all k-hat, the fit step's parameters"}}
     print(json.dumps(line), flush=True)
 
 

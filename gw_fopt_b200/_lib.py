@@ -32,7 +32,7 @@ class BgwxTimings(C.Structure):
     _fields_ = [("masks_ms", C.c_double), ("spectrum_ms", C.c_double), ("total_ms", C.c_double),
                 ("h2d_bytes", C.c_double), ("d2h_bytes", C.c_double), ("launches", C.c_uint64),
                 ("directions", C.c_uint64), ("fallbacks", C.c_uint64), ("beta_ms", C.c_double),
-                ("gemm_ms", C.c_double)]
+                ("gemm_ms", C.c_double), ("graph_replays", C.c_uint64)]
 
 
 _dp = C.POINTER(C.c_double)

@@ -114,7 +114,7 @@ void device_destroy(Device*);
 // the error counters and return without synchronising: their caller does
 // both once.
 void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_device, BgwxTimings* timings,
-                  bool nested = false);
+                  bool nested = false, bool uploads_only = false);
 
 // The launch shape of the last run_spectrum on this device (frames per launch
 // and GEMM row parts actually used).

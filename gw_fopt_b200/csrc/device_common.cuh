@@ -52,6 +52,7 @@ struct DevBuf {
     size_t cap = 0;
     std::vector<unsigned char> shadow;
     bool shadow_valid = false;
+    unsigned long long gen = 0;  // (re)allocations of this buffer
     void ensure(size_t bytes) {
         if (bytes <= cap) return;
         if (p) cudaFree(p);
@@ -61,6 +62,7 @@ struct DevBuf {
         CUDA_OK(cudaMalloc(&p, want));
         cap = want;
         shadow_valid = false;
+        ++gen;
     }
     ~DevBuf() {
         if (p) cudaFree(p);
@@ -84,12 +86,41 @@ struct Device {
     DevBuf beta_scale;                               // int8 tensor-core GEMM: per-(bubble, row) beta scales
     DevBuf fact_Dmax;                                // int8 tensor-core GEMM: per-(bubble, block) time-table maxima
     DevBuf tc_atab;                                  // int8 tensor-core GEMM: time-phase digits
+    bool capturing = false;      // the stream is being captured into a CUDA graph
+    size_t last_n_chunks = 0;    // launch chunks of the last run_spectrum (their events hold its stage times)
+    // the batched ensemble's launch sequence: sized by an eager run of a shape, captured by the
+    // next call of that shape and replayed by later ones
+    std::string ens_sized_key, ens_graph_key;
+    unsigned long long ens_sized_gen = 0, ens_graph_gen = 0;
+    cudaGraphExec_t ens_graph = nullptr;
+    uint64_t ens_graph_launches = 0;
+    size_t ens_graph_chunks = 0;
+    bool last_factored = false;
     bool tc_atab_valid = false;  // tc_atab holds the current call's time-phase digits
     DevBuf adj_gbar, adj_scratch, adj_grad, adj_mtab; // adjoint: cotangents, work arrays, gradients, phases
     size_t last_frames_per_launch = 0;               // launch shape of the last spectrum call
     int last_row_parts = 0;
     int last_gemm_stages = 0;
+    // Changes whenever one of this device's buffers is reallocated: a captured CUDA graph holds
+    // buffer addresses and stays valid only while the count is unchanged.
+    unsigned long long buffers_generation() const {
+        unsigned long long g = 0;
+        for (const DevBuf* b : {&bub, &bubrot, &dirs, &cos_t, &sin2, &cos2, &coeffs, &powers, &t_arr, &cutw, &w, &sel,
+                                &rot, &cosphi, &sinphi, &tau, &codes, &partial, &out, &counters, &nblists, &ranges,
+                                &real_tiles, &fact_D, &fact_kfirst, &beta, &fact_partial, &ens_out, &beta_scale,
+                                &fact_Dmax, &tc_atab})
+            g += b->gen;
+        return g;
+    }
     ~Device();
 };
+
+// Records a timing event on the device's stream.  Inside a stream capture a
+// plain record only orders the graph's nodes; an external record becomes a
+// node that records the event whenever the graph runs.
+inline void record_event(Device* d, cudaEvent_t e) {
+    CUDA_OK(d->capturing ? cudaEventRecordWithFlags(e, d->stream, cudaEventRecordExternal)
+                         : cudaEventRecord(e, d->stream));
+}
 
 }  // namespace bgw

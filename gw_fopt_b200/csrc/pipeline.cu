@@ -69,6 +69,7 @@ void device_drop_resident(Device* d) {
 
 Device::~Device() {
     if (stream) cudaStreamSynchronize(stream);
+    if (ens_graph) cudaGraphExecDestroy(ens_graph);
     if (own_stream) cudaStreamDestroy(own_stream);
     for (auto& e : ev)
         if (e) cudaEventDestroy(e);
@@ -605,6 +606,32 @@ void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_
     }
 }
 
+// Per-stage device times of the last run_spectrum's launch chunks (masks, then
+// spectrum = beta + GEMM for the factored kernels), once its work is complete.
+static void add_stage_times(Device* dev, BgwxTimings* tm) {
+    float ms_masks = 0, ms_spec = 0, ms_beta = 0, ms_gemm = 0;
+    // diagnostic only: an event that was not recorded leaves the stage times at zero
+    auto el = [](float& acc, cudaEvent_t a, cudaEvent_t b) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, a, b) == cudaSuccess)
+            acc += ms;
+        else
+            cudaGetLastError();
+    };
+    for (size_t ci = 0; ci < dev->last_n_chunks; ++ci) {
+        el(ms_masks, dev->chunk_ev[3 * ci], dev->chunk_ev[3 * ci + 1]);
+        el(ms_spec, dev->chunk_ev[3 * ci + 1], dev->chunk_ev[3 * ci + 2]);
+        if (dev->last_factored) {
+            el(ms_beta, dev->fact_ev[3 * ci], dev->fact_ev[3 * ci + 1]);
+            el(ms_gemm, dev->fact_ev[3 * ci + 1], dev->fact_ev[3 * ci + 2]);
+        }
+    }
+    tm->masks_ms += ms_masks;
+    tm->spectrum_ms += ms_spec;
+    tm->beta_ms += ms_beta;
+    tm->gemm_ms += ms_gemm;
+}
+
 // Error counters of a call: [0] mask fallbacks (u64), [1] non-zero when a
 // tensor-core pipeline wait gave up.
 static void check_counters(Device* dev, unsigned long long* fallbacks) {
@@ -616,7 +643,7 @@ static void check_counters(Device* dev, unsigned long long* fallbacks) {
 }
 
 void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_device, BgwxTimings* tm,
-                  bool nested) {
+                  bool nested, bool uploads_only) {
     CUDA_OK(cudaSetDevice(dev->id));
     const size_t nd = job.n_cos * job.n_phi;
     const size_t S = job.n_sets, W = job.n_w, K = job.n_k;
@@ -647,6 +674,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     const size_t out_blocks = batched ? job.n_real * K : K;  // (realization,) frame blocks of the output
     double* cosphi = job.tensor ? upload(dev, dev->cosphi, job.cosphi, job.n_phi, tm) : nullptr;
     double* sinphi = job.tensor ? upload(dev, dev->sinphi, job.sinphi, job.n_phi, tm) : nullptr;
+    if (uploads_only) return;  // the inputs are resident; a captured launch sequence follows
 
     // frames per chunk: bounded by the mask buffer budget (and by the job's launch shape)
     size_t kc = std::min(K, spectrum_max_frames_per_launch(job));
@@ -694,7 +722,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
         CUDA_OK(cudaFuncSetAttribute(k_tensor_direct<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
 
     uint64_t launches = 0;
-    CUDA_OK(cudaEventRecord(dev->ev[4], dev->stream));
+    record_event(dev, dev->ev[4]);
     for (size_t k0 = 0, ci = 0; k0 < K; k0 += kc, ++ci) {
         const size_t kn = std::min(kc, K - k0);
         cudaEvent_t* cev = &dev->chunk_ev[3 * ci];
@@ -706,10 +734,10 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             ++launches;
             fb = (const D4*)dev->bubrot.p;
         }
-        CUDA_OK(cudaEventRecord(cev[0], dev->stream));
+        record_event(dev, cev[0]);
         launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, ranges, job.n_sel, dirs, nd, job.n_phi, kn,
                              (double*)dev->tau.p, nullptr, (unsigned long long*)dev->counters.p, k0 == 0, &launches);
-        CUDA_OK(cudaEventRecord(cev[1], dev->stream));
+        record_event(dev, cev[1]);
         if (job.kernel == BGWX_KERNEL_FP64_DIRECT) {
             SpecArgs A;
             A.bub = fb;
@@ -755,9 +783,11 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             launches += launch_factored(dev, job, fb, sel, (const double*)dev->tau.p, cos_t, sin2, cos2, coeffs,
                                         powers, t_arr, cutw, w, k0, kn, final_out, real_tiles, &dev->fact_ev[3 * ci]);
         }
-        CUDA_OK(cudaEventRecord(cev[2], dev->stream));
+        record_event(dev, cev[2]);
     }
-    CUDA_OK(cudaEventRecord(dev->ev[5], dev->stream));
+    record_event(dev, dev->ev[5]);
+    dev->last_n_chunks = n_chunks;
+    dev->last_factored = job.kernel != BGWX_KERNEL_FP64_DIRECT;
     if (out_is_device) {
         if (tm) tm->launches += launches;
         if (!nested) check_counters(dev, nullptr);
@@ -766,34 +796,98 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     CUDA_OK(cudaMemcpyAsync(out, final_out, out_blocks * per * sizeof(double2), cudaMemcpyDeviceToHost, dev->stream));
     unsigned long long fbk = 0;
     check_counters(dev, &fbk);
-    float total = 0, ms_masks = 0, ms_spec = 0;
+    float total = 0;
     CUDA_OK(cudaEventElapsedTime(&total, dev->ev[4], dev->ev[5]));
-    float ms_beta = 0, ms_gemm = 0;
-    for (size_t ci = 0; ci < n_chunks; ++ci) {
-        float a = 0, b = 0;
-        CUDA_OK(cudaEventElapsedTime(&a, dev->chunk_ev[3 * ci], dev->chunk_ev[3 * ci + 1]));
-        CUDA_OK(cudaEventElapsedTime(&b, dev->chunk_ev[3 * ci + 1], dev->chunk_ev[3 * ci + 2]));
-        ms_masks += a;
-        ms_spec += b;
-        if (job.kernel != BGWX_KERNEL_FP64_DIRECT) {
-            float c = 0, d = 0;
-            CUDA_OK(cudaEventElapsedTime(&c, dev->fact_ev[3 * ci], dev->fact_ev[3 * ci + 1]));
-            CUDA_OK(cudaEventElapsedTime(&d, dev->fact_ev[3 * ci + 1], dev->fact_ev[3 * ci + 2]));
-            ms_beta += c;
-            ms_gemm += d;
-        }
-    }
     if (tm) {
-        tm->masks_ms += ms_masks;
-        tm->spectrum_ms += ms_spec;
-        tm->beta_ms += ms_beta;
-        tm->gemm_ms += ms_gemm;
+        add_stage_times(dev, tm);
         tm->total_ms += total;
         tm->launches += launches;
         tm->directions += K * job.n_sel * nd;
         tm->fallbacks += fbk;
         tm->d2h_bytes += (double)(out_blocks * per * sizeof(double2));
     }
+}
+
+// The launch sequence of a batched job as a CUDA graph.  Its kernels take the
+// job's sizes and scalars by value and the device buffers by address, so a
+// graph serves later calls whose key (every size, scalar and launch-shape
+// choice) and buffer generation match; the inputs themselves are uploaded
+// before each launch.  The first call of a key runs eagerly and sizes the
+// grow-only buffers, the second captures the sequence (no allocation can
+// happen during the capture then), later calls replay it.
+static std::string batched_key(const SpectrumJob& b) {
+    std::string k;
+    auto put = [&](double v) {
+        char buf[32];
+        std::snprintf(buf, sizeof buf, "%a:", v);
+        k += buf;
+    };
+    for (double v : {(double)b.kernel, (double)b.n_tot, (double)b.n_sel, (double)b.n_real, (double)b.n_cos,
+                     (double)b.n_phi, (double)b.n_t, (double)b.n_w, (double)b.n_sets, (double)b.n_terms,
+                     (double)b.has_damping, b.damping, b.dt, (double)b.n_k, (double)b.frames_per_launch,
+                     (double)b.row_parts, (double)b.gemm_stages})
+        put(v);
+    return k;
+}
+
+static void run_batched(Device* dev, SpectrumJob b, double2* eo, BgwxTimings* local) {
+    // the frames per launch are fixed here: a captured sequence must not depend on free memory
+    if (!b.frames_per_launch) b.frames_per_launch = std::min(b.n_k, spectrum_max_frames_per_launch(b));
+    const std::string key = batched_key(b);
+    double* out = reinterpret_cast<double*>(eo);
+    run_spectrum(dev, b, out, true, local, true, true);  // uploads what changed
+    if (dev->ens_graph && dev->ens_graph_key == key && dev->ens_graph_gen == dev->buffers_generation()) {
+        CUDA_OK(cudaGraphLaunch(dev->ens_graph, dev->stream));
+        local->launches += dev->ens_graph_launches;
+        dev->last_n_chunks = dev->ens_graph_chunks;
+        dev->last_factored = true;
+        ++local->graph_replays;
+        return;
+    }
+    if (dev->ens_sized_key != key || dev->ens_sized_gen != dev->buffers_generation()) {
+        run_spectrum(dev, b, out, true, local, true);
+        dev->ens_sized_key = key;
+        dev->ens_sized_gen = dev->buffers_generation();
+        return;
+    }
+    if (dev->ens_graph) {
+        CUDA_OK(cudaGraphExecDestroy(dev->ens_graph));
+        dev->ens_graph = nullptr;
+    }
+    BgwxTimings cap{};
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(dev->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+        cudaGetLastError();  // a stream that cannot be captured: run eagerly
+        run_spectrum(dev, b, out, true, local, true);
+        return;
+    }
+    dev->capturing = true;
+    try {
+        run_spectrum(dev, b, out, true, &cap, true);
+    } catch (...) {
+        dev->capturing = false;
+        cudaStreamEndCapture(dev->stream, &graph);
+        if (graph) cudaGraphDestroy(graph);
+        cudaGetLastError();
+        throw;
+    }
+    dev->capturing = false;
+    CUDA_OK(cudaStreamEndCapture(dev->stream, &graph));
+    cudaGraphExec_t exec = nullptr;
+    const cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CUDA_OK(e);
+    if (dev->buffers_generation() != dev->ens_sized_gen) {  // a buffer moved during the capture: do not keep it
+        cudaGraphExecDestroy(exec);
+        throw Error{"batched ensemble: a device buffer was reallocated while the launch sequence was captured"};
+    }
+    dev->ens_graph = exec;
+    dev->ens_graph_key = key;
+    dev->ens_graph_gen = dev->buffers_generation();
+    dev->ens_graph_launches = cap.launches;
+    dev->ens_graph_chunks = dev->last_n_chunks;
+    CUDA_OK(cudaGraphLaunch(exec, dev->stream));
+    local->launches += cap.launches;
 }
 
 void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out, BgwxTimings* tm, bool autotune) {
@@ -852,7 +946,7 @@ void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out
     CUDA_OK(cudaMemsetAsync(dev->counters.p, 0, 64, dev->stream));
     CUDA_OK(cudaEventRecord(dev->ev[6], dev->stream));
     if (batched) {
-        if (radiating > 0) run_spectrum(dev, b, reinterpret_cast<double*>(eo), true, &local, true);
+        if (radiating > 0) run_batched(dev, b, eo, &local);
     } else {
         std::vector<size_t> order(R);
         for (size_t r = 0; r < R; ++r) order[r] = r;
@@ -870,6 +964,8 @@ void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out
     float total = 0;
     CUDA_OK(cudaEventElapsedTime(&total, dev->ev[6], dev->ev[7]));
     if (tm) {
+        if (batched && radiating > 0) add_stage_times(dev, tm);  // the one batched run's stages
+        tm->graph_replays += local.graph_replays;
         tm->total_ms += total;
         tm->launches += local.launches;
         tm->h2d_bytes += local.h2d_bytes;

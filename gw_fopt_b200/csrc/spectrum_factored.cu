@@ -682,16 +682,47 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
                 const int b = t ? bc + __ffs(t) - 1 : -1;
                 for (int g = 0; g < 4 && quiet; ++g) quiet &= quiet - 1;
                 if (b < 0) continue;
-                const double* P = pbeg + (size_t)b * 2 * SMC;
-                const double Uc = uend[2 * b], Us = uend[2 * b + 1];
                 const int k0 = (b << 5) + s0;
+                // the block's constant sums, with rf / scale folded in: 1 + SMC products per
+                // value (steps past n_t, in the last block only, go through value())
+                const bool tail = k0 + 4 > A.n_t;
+                double P[2 * SMC];
+#pragma unroll
+                for (int q = 0; q < 2 * SMC; ++q) P[q] = rinv * pbeg[(size_t)b * 2 * SMC + q];
+                const double Uc = rinv * uend[2 * b], Us = rinv * uend[2 * b + 1];
+                const double* Db = Dslot + (size_t)k0 * (1 + SMC);
                 int8_t* blk = blk_row + (size_t)b * kI8BlockSet;
                 for (int s2 = 0; s2 < A.S; ++s2) {
                     uint32_t pc[4], ps[4];
+                    const int t0 = s2 * A.M, t1 = t0 + A.M;  // the terms of set s2
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
                         double xc, xs;
-                        value(k0 + m, s2, P, Uc, Us, rinv, xc, xs);
+                        if (tail) {
+                            value(k0 + m, s2, P, Uc, Us, 1.0, xc, xs);
+                        } else {
+                            const double* Dk = Db + (size_t)m * (1 + SMC);
+                            double g[1 + SMC];
+                            if constexpr ((1 + SMC) % 2 == 0) {
+#pragma unroll
+                                for (int q = 0; q < 1 + SMC; q += 2) {
+                                    const double2 v = __ldg(reinterpret_cast<const double2*>(Dk + q));
+                                    g[q] = v.x;
+                                    g[q + 1] = v.y;
+                                }
+                            } else {
+#pragma unroll
+                                for (int q = 0; q < 1 + SMC; ++q) g[q] = __ldg(Dk + q);
+                            }
+                            xc = g[0] * Uc;
+                            xs = g[0] * Us;
+#pragma unroll
+                            for (int q = 0; q < SMC; ++q) {
+                                if (SMC > 1 && (q < t0 || q >= t1)) continue;
+                                xc = fma(g[1 + q], P[2 * q], xc);
+                                xs = fma(g[1 + q], P[2 * q + 1], xs);
+                            }
+                        }
                         pc[m] = i8_digits(xc);
                         ps[m] = i8_digits(xs);
                     }
@@ -1156,7 +1187,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         ++launches;
     }
     // beta
-    CUDA_OK(cudaEventRecord(ev3[0], dev->stream));
+    record_event(dev, ev3[0]);
     const int nkb = G.nblk;
     const size_t beta_elems = tc ? (size_t)kn * n_cos * G.tiles_per_frame * nkb * kI8BlockSet
                                  : (size_t)kn * n_cos * G.cols_pad * G.t_pad;
@@ -1223,7 +1254,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         ++launches;
     }
     // GEMM + epilogue
-    CUDA_OK(cudaEventRecord(ev3[1], dev->stream));
+    record_event(dev, ev3[1]);
     FactArgs A;
     A.bub = bub_frames;
     A.n_tot = job.n_tot;
@@ -1290,7 +1321,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         T.err = reinterpret_cast<unsigned int*>(static_cast<unsigned char*>(dev->counters.p) + 8);
         launch_gemm_tc(T, kn, dev->stream);
         ++launches;
-        CUDA_OK(cudaEventRecord(ev3[2], dev->stream));
+        record_event(dev, ev3[2]);
         launches += reduce_tiles(dev, job, A.partial, G.tiles_per_frame, row_parts, per, k0, kn, out, real_tiles);
         return launches;
     } else {
@@ -1304,7 +1335,7 @@ static uint64_t launch_typed(Device* dev, const SpectrumJob& job, const D4* bub_
         k_gemm<Real, TN><<<grid, kThreads, smem, dev->stream>>>(A);
         CUDA_OK(cudaGetLastError());
         ++launches;
-        CUDA_OK(cudaEventRecord(ev3[2], dev->stream));
+        record_event(dev, ev3[2]);
         launches += reduce_tiles(dev, job, A.partial, G.tiles_per_frame, 1, per, k0, kn, out, real_tiles);
         return launches;
     }

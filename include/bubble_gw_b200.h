@@ -61,6 +61,7 @@ typedef struct BgwxTimings {
     uint64_t fallbacks; /* directions resolved by the exact slow path */
     double beta_ms;     /* factored kernels: beta producer */
     double gemm_ms;     /* factored kernels: time-phase GEMM and epilogue */
+    uint64_t graph_replays; /* batched ensemble: 1 when the call replayed its captured CUDA graph */
 } BgwxTimings;
 
 #ifdef __cplusplus

@@ -140,3 +140,43 @@ def test_batched_multi_tile_realizations_bitwise(gpu_available, kernel):
         g.set_launch_shape(2, 2)
         single = g.compute_c_integral_khat(w, kh, t_end=1.5, n_t=n_t)
         assert np.array_equal(out[r], single), r
+
+
+@pytest.mark.gpu
+def test_batched_graph_capture_and_replay(gpu_available):
+    """The batched launch sequence runs eagerly on the first call of a problem shape, is captured
+    into a CUDA graph by the second and replayed by later calls: all three give the same bits, and a
+    replay with other realizations of the same sizes (uploaded before the graph is launched) equals
+    their own eager calls."""
+    def reals_for(seed):
+        return [W.exponential_nucleation(n, 8.0, seed=seed + q) for q, n in enumerate((40, 9, 70))]
+
+    n_cos, n_phi, n_t = 16, 12, 64
+    w = np.geomspace(1.0, 300.0, 8)
+    kh = W.fibonacci_khat(2)
+
+    def make(reals):
+        e = BulkFlowEnsemble(reals, validate=False)
+        e.set_resolution(n_cos, n_phi)
+        e.set_gradient_scaling_params([[1.0]], [[5.0]])
+        e.set_kernel("mixed")
+        return e
+
+    first = reals_for(20)
+    ens = make(first)
+    outs, replays = [], []
+    for _ in range(3):
+        outs.append(ens.compute_c_integral_khat(w, kh, t_end=1.5, n_t=n_t))
+        replays.append(ens.last_timings()["graph_replays"])
+    assert replays == [0, 0, 1]
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+    # same sizes, other bubbles (the ensemble's arrays rewritten in place): the handle's graph is
+    # replayed on the new inputs
+    second = reals_for(40)
+    assert all(a.shape == a0.shape and b.shape == b0.shape for (a, b), (a0, b0) in zip(second, first))
+    ref = make(second).compute_c_integral_khat(w, kh, t_end=1.5, n_t=n_t)
+    ens._interior[...] = np.concatenate([a for a, _ in second])
+    ens._exterior[...] = np.concatenate([b for _, b in second])
+    got = ens.compute_c_integral_khat(w, kh, t_end=1.5, n_t=n_t)
+    assert ens.last_timings()["graph_replays"] == 1
+    assert np.array_equal(got, ref)
