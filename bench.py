@@ -349,6 +349,33 @@ def run_b200(args):
                     "algorithmic_tflops": gemm_flops / (tm["gemm_ms"] * 1e-3) / 1e12,
                     "peak_source": "of measured: 2 x MEASURED_PEAKS.json bf16_tflops_sustained (dense int8)",
                     "spectrum_stage": stage, "peaks": peaks}
+        # k_beta against HBM: it writes the four digit bytes of every beta value and reads every
+        # patch's collision delay once (plus one FP64 scale per row); per frame
+        beta_alg = 4.0 * cfg.n_cos * (cfg.n * 2 * S) * cfg.n_t + 8.0 * cfg.n * cfg.n_cos * cfg.n_phi \
+            + 8.0 * cfg.n * cfg.n_cos
+        btraffic = None
+        try:
+            btraffic = json.load(open(tpath)).get(f"config{args.config}:{args.kernel}:k_beta")
+        except Exception:
+            pass
+        if tm["beta_ms"] > 0:
+            b_ach = beta_alg * K / (tm["beta_ms"] * 1e-3) / 1e9
+            beta_roof = {"bound": "hbm", "achieved": b_ach, "peak": mp["hbm_gbs"], "unit": "GB/s",
+                         "frac": b_ach / mp["hbm_gbs"], "kernel": "k_beta",
+                         "traffic": btraffic * fpl if btraffic else None,
+                         "traffic_unit": "DRAM bytes per k_beta launch (per-frame ncu figure x frames per launch)",
+                         "algorithmic_bytes_per_launch": fpl * beta_alg,
+                         "work": "4 digit bytes per beta value written + 8 bytes per patch delay read + 8 bytes "
+                                 "per row scale, per frame",
+                         "peak_source": "of measured: MEASURED_PEAKS.json hbm_gbs",
+                         "note": "issue-bound (about 60% issue active under ncu), not limited by HBM"}
+            # the dominant kernel by device time heads the line; the other is kept beside it
+            if tm["beta_ms"] > tm["gemm_ms"]:
+                beta_roof.update({"spectrum_stage": stage, "peaks": peaks})
+                gemm_roof = {k: v for k, v in roofline.items() if k not in ("spectrum_stage", "peaks")}
+                roofline = dict(beta_roof, second_kernel=gemm_roof)
+            else:
+                roofline["second_kernel"] = beta_roof
     else:
         peak = (p32.value if args.kernel == "mixed_simt" else p64.value) / 1e12
         bound = "fp32" if args.kernel == "mixed_simt" else "fp64"
@@ -382,7 +409,8 @@ def run_b200(args):
                        "l2": "flushed between steps (256 MiB write)", "parallelism": f"khat-shard x{world}",
                        "tables": "time-phase digits rebuilt in every call (inside the timed steps)",
                        "launch_shape": dict(zip(("frames_per_launch", "row_parts"), launch_shape),
-                                            gemm_stages=gemm_stages, autotuned=not args.no_autotune)},
+                                            gemm_stages=gemm_stages, mask_chunking=g.last_mask_chunking(),
+                                            autotuned=not args.no_autotune)},
             "roofline": roofline, "e2e": e2e, "gpu_launches": launches_per_step * args.steps, "clocks": clocks,
             "compare": compare}
     if compare:

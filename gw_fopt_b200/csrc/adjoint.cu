@@ -111,6 +111,26 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_pq(AdjArgs A, const double2
     const int W = A.n_w;
     const int n_rows = A.n_sel * S2;
     const int r0 = rt * kPqRows, k0 = kt * kPqCols;
+    // k_adj_rows reads P and Q only at steps after a row's bubble nucleated: a tile whose steps
+    // all precede that for every bubble of its rows has nothing to compute
+    __shared__ int s_kmin;
+    if (tid == 0) s_kmin = A.n_t;
+    __syncthreads();
+    if (tid < kPqRows / S2) {
+        const int slot = r0 / S2 + tid;
+        if (slot < A.n_sel) {
+            const double ta = A.bub[(size_t)f * A.n_tot + A.sel[slot]].t;
+            int lo = 0, hi = A.n_t;  // first step with t_k - t_a > 0 (monotone in k)
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if (A.t_arr[mid] - ta > 0.0) hi = mid;
+                else lo = mid + 1;
+            }
+            atomicMin(&s_kmin, lo);
+        }
+    }
+    __syncthreads();
+    if (k0 + kPqCols <= s_kmin) return;
     const double ci = A.cos_t[i];
     double P[4][4], Q[4][4];
 #pragma unroll

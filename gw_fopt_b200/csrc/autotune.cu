@@ -14,7 +14,9 @@
 // Choices are keyed by the device (name, multiprocessor count) and every size
 // the launch shapes depend on; they live for the process and, when
 // BGWX_AUTOTUNE_CACHE names a file, are read from and appended to that file
-// (one "key frames row_parts stages" line per shape).
+// (one "key frames row_parts stages mask_chunking" line per shape).  The mask
+// search's chunking (blocks per bubble and frame: 1, 2 or 4 times the automatic
+// number) is timed last, at the chosen shape.
 
 #include <cuda_runtime.h>
 
@@ -54,10 +56,11 @@ void load_locked() {
     while (std::getline(in, line)) {
         std::istringstream ls(line);
         std::string key;
-        long long f = 0, r = 0, st = 0;
+        long long f = 0, r = 0, st = 0, mc = 0;
         if (!(ls >> key >> f >> r) || f < 1 || r < 1 || r > 16) continue;  // malformed lines are skipped
         if (!(ls >> st) || st < 3 || st > 5) st = 0;                       // older lines: automatic stages
-        g_cache[key] = LaunchShape{(size_t)f, (int)r, (int)st};
+        if (!(ls >> mc) || mc < 1 || mc > 4) mc = 0;                       // older lines: automatic chunking
+        g_cache[key] = LaunchShape{(size_t)f, (int)r, (int)st, (int)mc};
     }
 }
 
@@ -65,7 +68,9 @@ void append_locked(const std::string& key, const LaunchShape& s) {
     const char* path = cache_file();
     if (!path) return;
     std::ofstream out(path, std::ios::app);
-    if (out) out << key << ' ' << s.frames_per_launch << ' ' << s.row_parts << ' ' << s.gemm_stages << '\n';
+    if (out)
+        out << key << ' ' << s.frames_per_launch << ' ' << s.row_parts << ' ' << s.gemm_stages << ' '
+            << s.mask_chunking << '\n';
 }
 
 std::string shape_key(const Device* dev, const SpectrumJob& job) {
@@ -180,6 +185,24 @@ LaunchShape autotune_launch_shape(Device* dev, const SpectrumJob& job) {
                     best_ms = ms;
                     best.gemm_stages = stg;
                 }
+            }
+        }
+        // the mask search's chunking at the chosen shape (1 was among the timed runs)
+        best.mask_chunking = 1;
+        sub.frames_per_launch = best.frames_per_launch;
+        sub.row_parts = best.row_parts;
+        sub.gemm_stages = best.gemm_stages;
+        for (int mc : {2, 4}) {
+            sub.mask_chunking = mc;
+            float ms = 0.0f;
+            try {
+                ms = time_run(dev, sub, out);
+            } catch (const Error&) {
+                continue;
+            }
+            if (ms < best_ms) {
+                best_ms = ms;
+                best.mask_chunking = mc;
             }
         }
     } catch (...) {

@@ -67,6 +67,9 @@ struct SpectrumJob {
     size_t frames_per_launch = 0;
     int row_parts = 0;
     int gemm_stages = 0;
+    // mask search: the automatic number of blocks per (bubble, frame) times 1, 2 or 4 (0: 1);
+    // finer direction ranges per block give shorter tails, coarser ones fewer list gathers
+    int mask_chunking = 0;
     // Several realizations in one call (the batched ensemble, factored kernels): `bubbles` holds
     // them one after another (n_tot rows in all; n_int = n_tot), `sel` has one slot per radiating
     // bubble, padded so that each realization starts a GEMM column tile (padding slots hold
@@ -90,6 +93,7 @@ struct LaunchShape {
     size_t frames_per_launch = 0;
     int row_parts = 0;
     int gemm_stages = 0;
+    int mask_chunking = 0;
 };
 
 struct MaskJob {

@@ -35,7 +35,7 @@ struct bgw_generalized_bulk_flow {
     size_t num_threads = 1;
     BgwxKernel kernel = BGWX_KERNEL_FP64_DIRECT;
     // launch shape of spectrum calls: fixed (non-zero), measured (autotune) or automatic
-    size_t frames_per_launch = 0, row_parts = 0, gemm_stages = 0;
+    size_t frames_per_launch = 0, row_parts = 0, gemm_stages = 0, mask_chunking = 0;
     bool autotune = false;
     bgw::Device* dev = nullptr;
     BgwxTimings timings{};
@@ -184,15 +184,17 @@ bgw::SpectrumJob settings_job(const bgw_generalized_bulk_flow* h, const std::vec
 // The handle's launch shape into a spectrum job: a fixed shape when one is
 // set, else the measured one when autotuning is on, else automatic.
 void apply_launch_shape(bgw_generalized_bulk_flow* h, bgw::SpectrumJob& job) {
-    if (h->frames_per_launch || h->row_parts || h->gemm_stages) {
+    if (h->frames_per_launch || h->row_parts || h->gemm_stages || h->mask_chunking) {
         job.frames_per_launch = h->frames_per_launch;
         job.row_parts = (int)h->row_parts;
         job.gemm_stages = (int)h->gemm_stages;
+        job.mask_chunking = (int)h->mask_chunking;
     } else if (h->autotune) {
         const bgw::LaunchShape s = bgw::autotune_launch_shape(device(h), job);
         job.frames_per_launch = s.frames_per_launch;
         job.row_parts = s.row_parts;
         job.gemm_stages = s.gemm_stages;
+        job.mask_chunking = s.mask_chunking;
     }
 }
 
@@ -484,8 +486,9 @@ BgwStatus bgwx_generalized_bulk_flow_compute_ensemble_khat(
             jobs[r].frames_per_launch = h->frames_per_launch;
             jobs[r].row_parts = (int)h->row_parts;
             jobs[r].gemm_stages = (int)h->gemm_stages;
+            jobs[r].mask_chunking = (int)h->mask_chunking;
         }
-        const bool fixed = h->frames_per_launch || h->row_parts || h->gemm_stages;
+        const bool fixed = h->frames_per_launch || h->row_parts || h->gemm_stages || h->mask_chunking;
         h->timings = BgwxTimings{};
         std::vector<double> result(2 * expected, 0.0);
         bgw::run_ensemble(device(h), jobs, result.data(), &h->timings, h->autotune && !fixed);
@@ -837,6 +840,24 @@ BgwStatus bgwx_generalized_bulk_flow_last_gemm_stages(const bgw_generalized_bulk
         if (!bulk_flow) throw Error{"bulk_flow must not be null"};
         if (!out_stages) throw Error{"outputs must not be null"};
         *out_stages = bulk_flow->dev ? (size_t)bgw::last_launch_shape(bulk_flow->dev).gemm_stages : 0;
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_set_mask_chunking(bgw_generalized_bulk_flow* bulk_flow, size_t chunking) {
+    return run_ffi([&] {
+        auto* h = handle(bulk_flow);
+        if (chunking != 0 && chunking != 1 && chunking != 2 && chunking != 4)
+            throw Error{"mask chunking must be 0 (automatic), 1, 2 or 4"};
+        h->mask_chunking = chunking;
+    });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_last_mask_chunking(const bgw_generalized_bulk_flow* bulk_flow,
+                                                        size_t* out_chunking) {
+    return run_ffi([&] {
+        if (!bulk_flow) throw Error{"bulk_flow must not be null"};
+        if (!out_chunking) throw Error{"outputs must not be null"};
+        *out_chunking = bulk_flow->dev ? (size_t)bgw::last_launch_shape(bulk_flow->dev).mask_chunking : 0;
     });
 }
 

@@ -101,6 +101,7 @@ struct Device {
     size_t last_frames_per_launch = 0;               // launch shape of the last spectrum call
     int last_row_parts = 0;
     int last_gemm_stages = 0;
+    int last_mask_chunking = 0;
     // Changes whenever one of this device's buffers is reallocated: a captured CUDA graph holds
     // buffer addresses and stays valid only while the count is unchanged.
     unsigned long long buffers_generation() const {

@@ -441,15 +441,18 @@ __global__ void __launch_bounds__(kMaskListThreads)
       if (item >= n_items) break;
       const size_t strip = item % n_strips, group = item / n_strips;
       const size_t col = strip * 32 + lane;
+      const bool live = col < row_len;
       int seed = -1;
+      // each row's direction is loaded one row ahead, so that its latency overlaps the search
+      D4 x_next = dirs[(r_begin + group * kRowsPerItem) * row_len + (live ? col : 0)];
       for (int rr = 0; rr < kRowsPerItem; ++rr) {
         const size_t rw = r_begin + group * kRowsPerItem + rr;
         if (rw >= r_end) break;  // warp-uniform
         // the barrier reconverges lanes whose searches ended at different steps
         __syncwarp();
-        const bool live = col < row_len;
         const size_t d = rw * row_len + (live ? col : 0);
-        const D4 x = dirs[d];
+        const D4 x = x_next;
+        if (rr + 1 < kRowsPerItem && rw + 1 < r_end) x_next = dirs[d + row_len];
         long result = -1;
         int res_pos = -1;      // list position of the result, when it came from the list
         double res_tau = 0.0;  // tau of the result when it came from the list (same operations)
@@ -465,7 +468,8 @@ __global__ void __launch_bounds__(kMaskListThreads)
         // is within 6.03 u S of the exact value and V_ref within 6.01 u S, where
         // S = |ne| L1(c) + |nc| L1(e); |V| > 32 u S (plus an underflow guard) fixes
         // the sign, otherwise the reference's expression is evaluated.
-        auto verify = [&](int c, const D4& dc, double nc, double theta, int* fails, int& nfail) -> bool {
+        auto verify = [&](int c, const D4& dc, double nc, double theta, int* fails, int& nfail,
+                          int* first_fail = nullptr) -> bool {
             const double dotc = adot(dc);
             const double l1c = fabs(dc.t) + fabs(dc.x) + fabs(dc.y) + fabs(dc.z);
             const double am = 32.0 * 1.1102230246251565e-16 * l1c;
@@ -503,6 +507,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
                             if (nfail < kMaxFail) fails[nfail] = e;
                             ++nfail;
                         } else {
+                            if (first_fail) *first_fail = e;
                             return false;
                         }
                     }
@@ -529,24 +534,28 @@ __global__ void __launch_bounds__(kMaskListThreads)
         // 0. the previous row's result at this column (the neighbouring patch in cos theta
         //    most often has the same first collider): checked against every listed collider up
         //    to its bound and the outliers, stopping at the first failure.  If it passes it is
-        //    the exact answer (the passer is unique); otherwise the direction takes steps 1-3.
+        //    the exact answer (the passer is unique).  If it fails against a listed collider,
+        //    that collider (where the first-collider region most often moved to between the
+        //    rows) is checked the same way.  Otherwise the direction takes steps 1-3.
         bool seeded = false;
+        auto try_seed = [&](int q, int* first_fail) {
+            const D4 dq = s_pos[q];
+            const double dd = mdot(dq, x);
+            if (!(dd > 1e-10)) return false;
+            const double tq = __ddiv_rn(s_nrm[q], dmul(2.0, dd));
+            if (!(tq > 0.0)) return false;
+            const double th = theta_of(q, tq);
+            int dummy = 0;
+            if (!(th < kmax) || !verify(s_idx[q], dq, s_nrm[q], th, nullptr, dummy, first_fail)) return false;
+            result = s_idx[q];
+            res_pos = q;
+            res_tau = tq;
+            return true;
+        };
         if (!full && seed >= 0) {
-            const D4 ds_ = s_pos[seed];
-            const double ds = mdot(ds_, x);
-            if (ds > 1e-10) {
-                const double ts = __ddiv_rn(s_nrm[seed], dmul(2.0, ds));
-                if (ts > 0.0) {
-                    const double th = theta_of(seed, ts);
-                    int dummy = 0;
-                    if (th < kmax && verify(s_idx[seed], ds_, s_nrm[seed], th, nullptr, dummy)) {
-                        result = s_idx[seed];
-                        res_pos = seed;
-                        res_tau = ts;
-                        seeded = true;
-                    }
-                }
-            }
+            int ff = -1;
+            seeded = try_seed(seed, &ff);
+            if (!seeded && ff >= 0) seeded = try_seed(ff, nullptr);
         }
 
         if (!full && !seeded) {
@@ -704,7 +713,7 @@ void launch_masks_with_lists(cudaStream_t stream, const D4* bub, size_t n_int, s
 void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames, size_t n_int, size_t n_tot,
                           const uint32_t* sel, const uint2* ranges, size_t n_sel, const D4* dirs, size_t nd,
                           size_t row_len, size_t kn, double* tau, int32_t* codes, unsigned long long* counters,
-                          bool build_lists, uint64_t* launches) {
+                          bool build_lists, uint64_t* launches, int chunking) {
     if (row_len == 0 || nd % row_len != 0) row_len = nd;
     if (n_tot < 2) {
         // a lone bubble has no collider: every direction is None
@@ -720,7 +729,9 @@ void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames
         CUDA_OK(cudaGetLastError());
         if (launches) ++*launches;
     }
-    const unsigned n_split = mask_split(nd, row_len, n_sel * kn);
+    // the launch shape may ask for 2 or 4 times the automatic number of blocks (at most one row each)
+    const unsigned n_split = (unsigned)std::min<size_t>(
+        nd / row_len, (size_t)mask_split(nd, row_len, n_sel * kn) * (size_t)std::max(1, std::min(chunking, 4)));
     const size_t gx = (size_t)n_split * n_sel;
     if (gx > 0x7fffffffULL || kn > 65535) throw Error{"too many (bubble, patch) pairs for one launch"};
     dim3 grid((unsigned)gx, (unsigned)kn);

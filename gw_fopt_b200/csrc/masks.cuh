@@ -37,6 +37,6 @@ void launch_masks_with_lists(cudaStream_t stream, const D4* bub, size_t n_int, s
 void launch_mask_pipeline(Device* dev, const D4* bub_unrot, const D4* bub_frames, size_t n_int, size_t n_tot,
                           const uint32_t* sel, const uint2* ranges, size_t n_sel, const D4* dirs, size_t nd,
                           size_t row_len, size_t kn, double* tau, int32_t* codes, unsigned long long* counters,
-                          bool build_lists, uint64_t* launches);
+                          bool build_lists, uint64_t* launches, int chunking = 1);
 
 }  // namespace bgw

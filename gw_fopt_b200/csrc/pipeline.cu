@@ -568,6 +568,7 @@ LaunchShape last_launch_shape(const Device* dev) {
     s.frames_per_launch = dev->last_frames_per_launch;
     s.row_parts = dev->last_row_parts;
     s.gemm_stages = dev->last_gemm_stages;
+    s.mask_chunking = dev->last_mask_chunking;
     return s;
 }
 
@@ -682,6 +683,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     dev->last_frames_per_launch = kc;
     dev->last_row_parts = job.kernel == BGWX_KERNEL_FP64_DIRECT ? 1 : 0;  // the factored launch records its own
     dev->last_gemm_stages = 0;
+    dev->last_mask_chunking = job.mask_chunking > 0 ? job.mask_chunking : 1;
     dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
     if (job.kernel == BGWX_KERNEL_FP64_DIRECT) dev->partial.ensure(kc * job.n_sel * per * sizeof(double2));
     double2* final_out = out_is_device ? reinterpret_cast<double2*>(out) : nullptr;
@@ -736,7 +738,8 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
         }
         record_event(dev, cev[0]);
         launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, ranges, job.n_sel, dirs, nd, job.n_phi, kn,
-                             (double*)dev->tau.p, nullptr, (unsigned long long*)dev->counters.p, k0 == 0, &launches);
+                             (double*)dev->tau.p, nullptr, (unsigned long long*)dev->counters.p, k0 == 0, &launches,
+                             job.mask_chunking);
         record_event(dev, cev[1]);
         if (job.kernel == BGWX_KERNEL_FP64_DIRECT) {
             SpecArgs A;
@@ -825,7 +828,7 @@ static std::string batched_key(const SpectrumJob& b) {
     for (double v : {(double)b.kernel, (double)b.n_tot, (double)b.n_sel, (double)b.n_real, (double)b.n_cos,
                      (double)b.n_phi, (double)b.n_t, (double)b.n_w, (double)b.n_sets, (double)b.n_terms,
                      (double)b.has_damping, b.damping, b.dt, (double)b.n_k, (double)b.frames_per_launch,
-                     (double)b.row_parts, (double)b.gemm_stages})
+                     (double)b.row_parts, (double)b.gemm_stages, (double)b.mask_chunking})
         put(v);
     return k;
 }
@@ -936,6 +939,7 @@ void run_ensemble(Device* dev, const std::vector<SpectrumJob>& jobs, double* out
             b.frames_per_launch = s.frames_per_launch;
             b.row_parts = s.row_parts;
             b.gemm_stages = s.gemm_stages;
+            b.mask_chunking = s.mask_chunking;
         }
     }
     dev->ens_out.ensure(R * per_r * sizeof(double2));

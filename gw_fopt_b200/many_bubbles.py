@@ -573,6 +573,18 @@ class GeneralizedBulkFlow:
         _call(L.lib().bgwx_generalized_bulk_flow_last_gemm_stages(self._h, C.byref(n)))
         return int(n.value)
 
+    def set_mask_chunking(self, chunking: int = 0) -> None:
+        """Blocks of the first-collider search per (bubble, k-hat frame): 1, 2 or 4 times the
+        automatic number; 0 keeps the automatic (or measured) choice (B200 extension).  The masks
+        are the same for every choice."""
+        _call(L.lib().bgwx_generalized_bulk_flow_set_mask_chunking(self._h, int(chunking)))
+
+    def last_mask_chunking(self) -> int:
+        """Mask-search chunking of the last spectrum call."""
+        n = C.c_size_t(0)
+        _call(L.lib().bgwx_generalized_bulk_flow_last_mask_chunking(self._h, C.byref(n)))
+        return int(n.value)
+
     # --- geometry -------------------------------------------------------------
     def _require_res(self, name="n_cos_thetax"):
         if self._n_cos is None:

@@ -135,6 +135,17 @@ BgwStatus bgwx_generalized_bulk_flow_set_gemm_stages(bgw_generalized_bulk_flow *
  * kernel's GEMM).  No counterpart in the reference. */
 BgwStatus bgwx_generalized_bulk_flow_last_gemm_stages(const bgw_generalized_bulk_flow *bulk_flow, size_t *out_stages);
 
+/* Chunking of the first-collider search: 1, 2 or 4 times the automatic number
+ * of blocks per (radiating bubble, k-hat frame), each over a range of whole
+ * cos-theta rows (0 = automatic: 1, or the autotuner's measured choice).  The
+ * masks are the same for every choice.  No counterpart in the reference. */
+BgwStatus bgwx_generalized_bulk_flow_set_mask_chunking(bgw_generalized_bulk_flow *bulk_flow, size_t chunking);
+
+/* Mask-search chunking of the last spectrum call.  No counterpart in the
+ * reference. */
+BgwStatus bgwx_generalized_bulk_flow_last_mask_chunking(const bgw_generalized_bulk_flow *bulk_flow,
+                                                        size_t *out_chunking);
+
 /* First-collider codes (-1 None, i Interior(i), -(i+2) Exterior(i)) and the
  * collision delays of compute_delta_tab for interior bubbles [a_begin, a_end)
  * at k-hat = z, computed on the GPU.  out_codes: (a_end-a_begin, n_cos, n_phi)

@@ -71,8 +71,9 @@ def test_autotune_choice_is_kept_and_exact(gpu_available, tmp_path, monkeypatch)
     assert st in (3, 4, 5)
     lines = cache.read_text().splitlines()
     assert len(lines) == 1
-    key, fs, rs, ss = lines[0].split()
-    assert "k2:" in key and (int(fs), int(rs), int(ss)) == (f, r, st)
+    key, fs, rs, ss, ms = lines[0].split()
+    assert "k2:" in key and (int(fs), int(rs), int(ss), int(ms)) == (f, r, st, g.last_mask_chunking())
+    assert int(ms) in (1, 2, 4)
     # the second call of the same shape reuses the choice (nothing new is written)
     out2 = spectrum(c, g)
     np.testing.assert_array_equal(out2, out)
@@ -89,3 +90,21 @@ def test_autotune_choice_is_kept_and_exact(gpu_available, tmp_path, monkeypatch)
         outs[stages] = spectrum(c, g)
         assert g.last_gemm_stages() == stages
     np.testing.assert_array_equal(outs[3], outs[5])
+
+
+@pytest.mark.parametrize("kernel", ["mixed", "fp64_factored"])
+def test_mask_chunking_gives_the_same_spectrum(gpu_available, kernel):
+    """The first-collider search cut into 1, 2 or 4 times the automatic number of blocks per
+    (bubble, frame): every direction is decided exactly whatever seeds its block's rows give, so
+    the masks and the spectrum are the same bits."""
+    c, g = flow(kernel)
+    g.set_launch_shape(2, 2 if kernel == "mixed" else 0)
+    outs = []
+    for mc in (1, 2, 4):
+        g.set_mask_chunking(mc)
+        outs.append(spectrum(c, g))
+        assert g.last_mask_chunking() == mc
+    for o in outs[1:]:
+        np.testing.assert_array_equal(o, outs[0])
+    with pytest.raises(ValueError):
+        g.set_mask_chunking(3)
