@@ -37,6 +37,7 @@
 
 #include <cmath>
 #include <string>
+#include <type_traits>
 
 #include "adjoint.cuh"
 #include "bgw_internal.h"
@@ -66,6 +67,7 @@ struct AdjArgs {
     const double* rot;    // (kn, 9) rotations of the chunk's frames; nullptr = identity
     const double2* gbar;  // (kn, 2, S, W) cotangents of the chunk's frames
     int kn;               // frames in the chunk
+    int f32pq;            // k_adj_pq: FP32 products folded into FP64 every kPqW frequencies (mixed kernels)
     int has_damp;
     double damp;
     double dphi, dcos, dt;
@@ -99,12 +101,17 @@ constexpr int kPqW = 16;      // frequencies per shared-memory stage
 
 // One CTA per (row tile x step tile, cos-theta row i, frame).  Thread
 // (ty, tx) of 16 x 16 owns rows ty + 16 u and steps tx + 16 v (u, v < 4).
-template <int S>
+// F32: the products run in FP32 (H and M rounded to FP32, one FP32 sum per stage of kPqW
+// frequencies), each stage's sums added to FP64 accumulators: about 16 x 2^-24 of the terms
+// per stage instead of FP64 rounding, at twice the FMA rate.
+template <int S, bool F32>
 __global__ void __launch_bounds__(kAdjThreads) k_adj_pq(AdjArgs A, const double2* __restrict__ mt, int row_tiles) {
     constexpr int S2 = 2 * S;
-    __shared__ double2 Hs[kPqW][kPqRows];
-    __shared__ double2 Ms[kPqW][kPqCols];
-    __shared__ double ws[kPqW];
+    using V2 = typename std::conditional<F32, float2, double2>::type;
+    using R = typename std::conditional<F32, float, double>::type;
+    __shared__ V2 Hs[kPqW][kPqRows];
+    __shared__ V2 Ms[kPqW][kPqCols];
+    __shared__ R ws[kPqW];
     const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
     const int rt = blockIdx.x % row_tiles, kt = blockIdx.x / row_tiles;
     const int i = blockIdx.y, f = blockIdx.z;
@@ -138,6 +145,11 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_pq(AdjArgs A, const double2
 #pragma unroll
         for (int v = 0; v < 4; ++v) P[u][v] = Q[u][v] = 0.0;
     for (int w0 = 0; w0 < W; w0 += kPqW) {
+        R Ps[4][4], Qs[4][4];  // this stage's sums
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) Ps[u][v] = Qs[u][v] = R(0);
         __syncthreads();
         // H tile: row r = slot * S2 + gs
         for (int q = tid; q < kPqW * kPqRows; q += blockDim.x) {
@@ -153,31 +165,39 @@ __global__ void __launch_bounds__(kAdjThreads) k_adj_pq(AdjArgs A, const double2
                 // conj(g) * (cs + i sn)
                 h = make_double2(g.x * cs + g.y * sn, g.x * sn - g.y * cs);
             }
-            Hs[wl][rl] = h;
+            Hs[wl][rl] = V2{(R)h.x, (R)h.y};
         }
         for (int q = tid; q < kPqW * kPqCols; q += blockDim.x) {
             const int wl = q / kPqCols, kl = q % kPqCols;
             const int wi = w0 + wl, k = k0 + kl;
-            Ms[wl][kl] = (wi < W && k < A.n_t) ? mt[((size_t)i * W + wi) * A.n_t + k] : make_double2(0.0, 0.0);
+            const double2 m = (wi < W && k < A.n_t) ? mt[((size_t)i * W + wi) * A.n_t + k] : make_double2(0.0, 0.0);
+            Ms[wl][kl] = V2{(R)m.x, (R)m.y};
         }
-        if (tid < kPqW) ws[tid] = w0 + tid < W ? A.w[w0 + tid] : 0.0;
+        if (tid < kPqW) ws[tid] = (R)(w0 + tid < W ? A.w[w0 + tid] : 0.0);
         __syncthreads();
 #pragma unroll 4
         for (int wl = 0; wl < kPqW; ++wl) {
-            double2 h[4], m[4];
+            V2 h[4], m[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) h[u] = Hs[wl][ty + 16 * u];
 #pragma unroll
             for (int v = 0; v < 4; ++v) m[v] = Ms[wl][tx + 16 * v];
-            const double om = ws[wl];
+            const R om = ws[wl];
 #pragma unroll
             for (int u = 0; u < 4; ++u)
 #pragma unroll
                 for (int v = 0; v < 4; ++v) {
-                    P[u][v] = fma(h[u].x, m[v].x, fma(-h[u].y, m[v].y, P[u][v]));
-                    Q[u][v] = fma(om, fma(h[u].x, m[v].y, h[u].y * m[v].x), Q[u][v]);
+                    Ps[u][v] = fma(h[u].x, m[v].x, fma(-h[u].y, m[v].y, Ps[u][v]));
+                    Qs[u][v] = fma(om, fma(h[u].x, m[v].y, h[u].y * m[v].x), Qs[u][v]);
                 }
         }
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int v = 0; v < 4; ++v) {
+                P[u][v] += (double)Ps[u][v];
+                Q[u][v] += (double)Qs[u][v];
+            }
     }
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
@@ -679,7 +699,10 @@ static uint64_t launch_typed(const AdjArgs& A, size_t kn, cudaStream_t st, const
         const int col_tiles = (A.n_t + kPqCols - 1) / kPqCols;
         if ((long)row_tiles * col_tiles > 0x7fffffffL) throw Error{"adjoint grid too large"};
         dim3 g((unsigned)(row_tiles * col_tiles), (unsigned)A.n_cos, (unsigned)kn);
-        k_adj_pq<S><<<g, kAdjThreads, 0, st>>>(A, mt, row_tiles);
+        if (A.f32pq)
+            k_adj_pq<S, true><<<g, kAdjThreads, 0, st>>>(A, mt, row_tiles);
+        else
+            k_adj_pq<S, false><<<g, kAdjThreads, 0, st>>>(A, mt, row_tiles);
         CUDA_OK(cudaGetLastError());
         ++launches;
     }
@@ -767,6 +790,9 @@ uint64_t launch_adjoint_chunk(Device* dev, const SpectrumJob& job, const D4* bub
     A.rot = rot;
     A.gbar = gbar;
     A.kn = (int)kn;
+    // the backward's precision follows the forward's kernel: FP32 products of depth kPqW for the
+    // mixed kernels, FP64 otherwise
+    A.f32pq = (job.kernel == BGWX_KERNEL_MIXED || job.kernel == BGWX_KERNEL_MIXED_SIMT) ? 1 : 0;
     A.has_damp = job.has_damping ? 1 : 0;
     A.damp = job.damping;
     A.dphi = 2.0 * M_PI / (double)job.n_phi;

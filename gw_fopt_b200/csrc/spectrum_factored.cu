@@ -241,15 +241,26 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
         nc += __shfl_down_sync(full, nc, o);
         ns += __shfl_down_sync(full, ns, o);
     }
-    if (lane == 0) {
-        int acc = 0;
-        for (int b = 0; b < NB; ++b) {
-            const int c = boff[b];
-            boff[b] = acc;
-            brun[b] = acc;
-            acc += c;
+    // block counts -> first event of each block: an exclusive warp scan over 32 blocks at a time
+    {
+        int carry = 0;
+        for (int bc = 0; bc < NB; bc += 32) {
+            const int b = bc + lane;
+            const int c = b < NB ? boff[b] : 0;
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(full, incl, o);
+                if (lane >= o) incl += t;
+            }
+            if (b < NB) {
+                boff[b] = carry + incl - c;
+                brun[b] = carry + incl - c;
+            }
+            carry += __shfl_sync(full, incl, 31);
         }
-        boff[NB] = acc;
+        __syncwarp();
+        if (lane == 0) boff[NB] = carry;
     }
     __syncwarp();
     // pass 2: scatter events (stable in j within a block)

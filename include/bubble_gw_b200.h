@@ -208,7 +208,9 @@ BgwStatus bgwx_generalized_bulk_flow_compute_ensemble_khat(
  * dL/d(powers) ((n_sets, n_terms) each) and dL/d(bubbles) ((n_interior +
  * n_exterior, 4), columns (t, x, y, z); a caller whose exterior rows are
  * images of interior rows adds each image row's gradient to its source row).
- * FP64 throughout; the first-collider search is recomputed, phases are
+ * FP64, except that with a mixed kernel selected the depth-n_w products of
+ * the cotangents with the phases run in FP32, folded into FP64 every 16
+ * frequencies; the first-collider search is recomputed, phases are
  * recomputed rather than stored.  Collision status and first-collider identity
  * are piecewise constant in the inputs and carry no gradient.  Differentiates
  * generalized_bulk_flow.rs:481-873 and the delays of :421-471.  No counterpart

@@ -245,3 +245,49 @@ def test_adjoint_bitwise_repeatable(gpu_available):
         again = m.vjp(co, po, c["inter"], G)
         for x, y in zip(first, again):
             assert np.array_equal(x, y)
+
+
+@pytest.mark.gpu
+def test_mixed_adjoint_vs_fp64_adjoint_and_fd(gpu_available):
+    """With a mixed kernel the backward's products P and Q run in FP32 (folded into FP64 every 16
+    frequencies): its gradients match the FP64 adjoint to 1e-5 (measured ~1e-7) for coefficients,
+    powers and bubble rows, and the mixed autograd gradient of the fit loss matches central
+    differences of the FP64 forward to 1e-5."""
+    from gw_fopt_b200.autograd import SurfaceTensionFit, log_power_residual
+    c = small_case(seed=7, n=8)
+    c["n_cos"], c["n_phi"], c["n_t"] = 16, 16, 64
+    c["w"] = np.geomspace(1.0, 200.0, 40)
+    c["kh"] = W.fibonacci_khat(3)
+    co = np.array([[1.0, 0.3]])
+    po = np.array([[5.0, 3.5]])
+    rng = np.random.default_rng(3)
+    G = rng.normal(size=(3, 2, 1, 40)) + 1j * rng.normal(size=(3, 2, 1, 40))
+    got = _library_model(c, kernel="mixed").vjp(co, po, c["inter"], G)
+    ref = _library_model(c, kernel="fp64_factored").vjp(co, po, c["inter"], G)
+    for g_, r_ in zip(got, ref):
+        err = np.abs(g_ - r_).max() / np.abs(r_).max()
+        print(f"mixed vs FP64 adjoint: {err:.2e}")
+        assert err < 1e-5
+    m = _library_model(c, kernel="mixed")
+    m64 = _library_model(c, kernel="fp64_factored")
+    x = torch.tensor(c["inter"], dtype=torch.float64, requires_grad=True)
+    with torch.no_grad():
+        co_t, po_t = SurfaceTensionFit(xi=2.0, alpha=1.0, gamma=0.0, delta=0.0)()
+        target = (m64(co_t, po_t, x) ** 2).sum(-1).sum(1) * 1.1
+    fit = SurfaceTensionFit(xi=1.5, alpha=0.9, gamma=0.3, delta=0.1)
+    cc, pp = fit()
+    log_power_residual(m(cc, pp, x), target).backward()
+    base = dict(xi=1.5, alpha=0.9, gamma=0.3, delta=0.1)
+
+    def f(**kw):
+        with torch.no_grad():
+            a, b = SurfaceTensionFit(**kw)()
+            return float(log_power_residual(m64(a, b, x), target))
+
+    for name in base:
+        p, q = dict(base), dict(base)
+        p[name] += H
+        q[name] -= H
+        fd = (f(**p) - f(**q)) / (2 * H)
+        an = float(getattr(fit, name).grad)
+        assert abs(fd - an) <= FD_TOL * abs(fd), (name, fd, an)
