@@ -353,8 +353,9 @@ __global__ void __launch_bounds__(kMaskListThreads)
     // per listed collider: Delta = x_c - x_a and its Minkowski norm, computed once
     // per block with the reference's operations (direction independent)
     __shared__ D4 s_pos[kList];
-    __shared__ double s_nrm[kList];
-    __shared__ double s_l1[kList];  // |dt| + |dx| + |dy| + |dz|
+    // per listed collider e: its Minkowski norm n_e and |n_e| + L1(Delta_e), the factor of e in
+    // the sign filter's error bound (L1 = |dt| + |dx| + |dy| + |dz|), read together
+    __shared__ double2 s_ns[kList];
     __shared__ double s_thr[kList]; // direction-independent part of the verification bound, see theta_of
     __shared__ double s_key[kList];
     __shared__ int s_idx[kList];
@@ -406,17 +407,18 @@ __global__ void __launch_bounds__(kMaskListThreads)
         s_key[q] = L->key[q];
         const D4 dc = dsub4(B[c], xa);
         s_pos[q] = dc;
-        s_nrm[q] = mdot(dc, dc);
-        s_l1[q] = fabs(dc.t) + fabs(dc.x) + fabs(dc.y) + fabs(dc.z);
+        const double nrm_q = mdot(dc, dc);
+        const double l1_q = fabs(dc.t) + fabs(dc.x) + fabs(dc.y) + fabs(dc.z);
+        s_ns[q] = make_double2(nrm_q, fabs(nrm_q) + l1_q);
         {
             // theta = tau (1 + 1e-12) + 64 u (A rho1 + Q rho2) / dot with 1 / dot = 2 tau / nrm
             // for a collider (nrm > 0): theta = tau (1 + 1e-12 + s_thr)
             const double dx = sqrt(dc.x * dc.x + dc.y * dc.y + dc.z * dc.z);
             const double Ac = fabs(dc.t) + dx, Qc = dc.t * dc.t + dx * dx;
-            s_thr[q] = s_nrm[q] > 0.0 ? 2.0 * (64.0 * 1.1102230246251565e-16) * (Ac * L->rho1 + Qc * L->rho2) / s_nrm[q]
+            s_thr[q] = nrm_q > 0.0 ? 2.0 * (64.0 * 1.1102230246251565e-16) * (Ac * L->rho1 + Qc * L->rho2) / nrm_q
                                       : CUDART_INF;
         }
-        if (!(s_l1[q] < 1e5)) s_big = true;  // benign race: every writer stores true
+        if (!(l1_q < 1e5)) s_big = true;  // benign race: every writer stores true
     }
     for (int q = threadIdx.x; q < no; q += kMaskListThreads) {
         s_oidx[q] = L->outlier[q];
@@ -467,13 +469,15 @@ __global__ void __launch_bounds__(kMaskListThreads)
         //   V = fma(ne, adot(c), -(nc adot(e)))
         // is within 6.03 u S of the exact value and V_ref within 6.01 u S, where
         // S = |ne| L1(c) + |nc| L1(e); |V| > 32 u S (plus an underflow guard) fixes
-        // the sign, otherwise the reference's expression is evaluated.
-        auto verify = [&](int c, const D4& dc, double nc, double theta, int* fails, int& nfail,
+        // the sign, otherwise the reference's expression is evaluated.  The bound is taken as
+        // 32 u max(L1(c), |nc|) (|ne| + L1(e)) >= 32 u S: looser, which only sends a few more
+        // values near zero to the exact evaluation.  c is the candidate's collider index, cpos its
+        // list position (the list holds each collider once).
+        auto verify = [&](int c, int cpos, const D4& dc, double nc, double theta, int* fails, int& nfail,
                           int* first_fail = nullptr) -> bool {
             const double dotc = adot(dc);
             const double l1c = fabs(dc.t) + fabs(dc.x) + fabs(dc.y) + fabs(dc.z);
-            const double am = 32.0 * 1.1102230246251565e-16 * l1c;
-            const double bm = 32.0 * 1.1102230246251565e-16 * fabs(nc);
+            const double mc = 32.0 * 1.1102230246251565e-16 * fmax(l1c, fabs(nc));
             bool ok = true;
             // entries in batches of kBatch: their filter values are independent
             // (instruction-level parallelism); decisions are taken in list order
@@ -485,9 +489,9 @@ __global__ void __launch_bounds__(kMaskListThreads)
                     const int e = min(e0 + j, n - 1);
                     kb[j] = s_key[e];
                     const D4 pe = s_pos[e];
-                    const double ne = s_nrm[e];
-                    vb[j] = fma(ne, dotc, -(nc * adot(pe)));
-                    bb[j] = fma(fabs(ne), am, bm * s_l1[e]) + 1e-300;
+                    const double2 ns = s_ns[e];
+                    vb[j] = fma(ns.x, dotc, -(nc * adot(pe)));
+                    bb[j] = fma(ns.y, mc, 1e-300);
                 }
 #pragma unroll
                 for (int j = 0; j < kBatch; ++j) {
@@ -496,11 +500,11 @@ __global__ void __launch_bounds__(kMaskListThreads)
                         done = true;
                         break;
                     }
-                    if (s_idx[e] == c) continue;
+                    if (e == cpos) continue;
                     bool pass;
                     if (vb[j] > bb[j]) pass = true;
                     else if (vb[j] < -bb[j]) pass = false;
-                    else pass = check_pre(dc, nc, s_pos[e], s_nrm[e], x);
+                    else pass = check_pre(dc, nc, s_pos[e], s_ns[e].x, x);
                     if (!pass) {
                         ok = false;
                         if (fails) {
@@ -542,11 +546,11 @@ __global__ void __launch_bounds__(kMaskListThreads)
             const D4 dq = s_pos[q];
             const double dd = mdot(dq, x);
             if (!(dd > 1e-10)) return false;
-            const double tq = __ddiv_rn(s_nrm[q], dmul(2.0, dd));
+            const double tq = __ddiv_rn(s_ns[q].x, dmul(2.0, dd));
             if (!(tq > 0.0)) return false;
             const double th = theta_of(q, tq);
             int dummy = 0;
-            if (!(th < kmax) || !verify(s_idx[q], dq, s_nrm[q], th, nullptr, dummy, first_fail)) return false;
+            if (!(th < kmax) || !verify(s_idx[q], q, dq, s_ns[q].x, th, nullptr, dummy, first_fail)) return false;
             result = s_idx[q];
             res_pos = q;
             res_tau = tq;
@@ -572,7 +576,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
                 for (int j = 0; j < kBatch; ++j) {
                     const int e = min(e0 + j, n - 1);
                     kb[j] = s_key[e];
-                    nb[j] = s_nrm[e];
+                    nb[j] = s_ns[e].x;
                     db[j] = 2.0 * adot(s_pos[e]);
                 }
 #pragma unroll
@@ -596,21 +600,21 @@ __global__ void __launch_bounds__(kMaskListThreads)
             if (bi >= 0) {
                 // the candidate's tau with the reference's operations (compute_delta_tab)
                 dotm = mdot(s_pos[bi], x);
-                if (dotm > 1e-10) best = __ddiv_rn(s_nrm[bi], dmul(2.0, dotm));
+                if (dotm > 1e-10) best = __ddiv_rn(s_ns[bi].x, dmul(2.0, dotm));
                 if (!(dotm > 1e-10) || !(best > 0.0)) full = true;  // not a collider by the exact test
             }
             if (!full && ended && !(kmax > best * (1.0 + 1e-11))) full = !(bi < 0 && kmax == CUDART_INF);
             if (!full && bi >= 0) {
                 // 2. verify the candidate
                 const D4 dm = s_pos[bi];
-                const double nm = s_nrm[bi];
+                const double nm = s_ns[bi].x;
                 const double th = theta_of(bi, best);
                 if (!(th < kmax)) {
                     full = true;
                 } else {
                     int fails[kMaxFail];
                     int nfail = 0;
-                    if (verify(s_idx[bi], dm, nm, th, fails, nfail)) {
+                    if (verify(s_idx[bi], bi, dm, nm, th, fails, nfail)) {
                         result = s_idx[bi];
                         res_pos = bi;
                         res_tau = best;
@@ -623,7 +627,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
                             const D4 dc = s_pos[e];
                             const double dot = mdot(dc, x);
                             if (!(dot > 1e-10)) continue;
-                            const double nc = s_nrm[e];
+                            const double nc = s_ns[e].x;
                             const double tau = __ddiv_rn(nc, dmul(2.0, dot));
                             if (!(tau > 0.0)) continue;
                             const double thf = theta_of(e, tau);
@@ -632,7 +636,7 @@ __global__ void __launch_bounds__(kMaskListThreads)
                                 break;
                             }
                             int dummy = 0;
-                            if (verify(s_idx[e], dc, nc, thf, nullptr, dummy)) {
+                            if (verify(s_idx[e], e, dc, nc, thf, nullptr, dummy)) {
                                 result = s_idx[e];
                                 res_pos = e;
                                 res_tau = tau;
