@@ -62,6 +62,7 @@ SIGNATURES = {
     "bgwx_generalized_bulk_flow_set_gemm_stages": (C.c_int, [_hp, C.c_size_t]),
     "bgwx_generalized_bulk_flow_last_gemm_stages": (C.c_int, [_hp, C.POINTER(C.c_size_t)]),
     "bgwx_generalized_bulk_flow_set_mask_chunking": (C.c_int, [_hp, C.c_size_t]),
+    "bgwx_generalized_bulk_flow_set_keep_masks": (C.c_int, [_hp, C.c_bool]),
     "bgwx_generalized_bulk_flow_last_mask_chunking": (C.c_int, [_hp, C.POINTER(C.c_size_t)]),
     "bgwx_generalized_bulk_flow_last_launch_shape": (C.c_int, [_hp, C.POINTER(C.c_size_t),
                                                                 C.POINTER(C.c_size_t)]),

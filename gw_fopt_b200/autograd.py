@@ -74,12 +74,15 @@ class BulkFlowSpectrum:
     """C(coefficients, powers, interior): (K, 2, S, W, 2) float64 (real, imaginary last).
 
     ``kernel`` selects the forward kernel ('fp64_direct', 'fp64_factored' or
-    'mixed'); the backward pass is the FP64 adjoint.
+    'mixed'); the backward pass is the adjoint, FP64 with an FP64 kernel and with
+    FP32 products folded into FP64 with a mixed one.  With ``keep_masks`` the
+    forward keeps its collision masks on the device and a backward on the same
+    bubbles reads them (the same gradients, one mask search fewer).
     """
 
     def __init__(self, *, n_cos: int, n_phi: int, w, khat, t_end: float, n_t: int, t_begin: float = 0.0,
                  box: Optional[float] = 1.0, time_cutoff=None, damping: Optional[float] = None,
-                 kernel: str = "fp64_factored"):
+                 kernel: str = "fp64_factored", keep_masks: bool = True):
         self.w = np.ascontiguousarray(np.asarray(w, dtype=np.float64).ravel())
         self.khat = np.ascontiguousarray(np.asarray(khat, dtype=np.float64).reshape(-1, 3))
         self.n_cos, self.n_phi = int(n_cos), int(n_phi)
@@ -94,6 +97,9 @@ class BulkFlowSpectrum:
         k = {"fp64_direct": L.KERNEL_FP64_DIRECT, "fp64_factored": L.KERNEL_FP64_FACTORED,
              "mixed": L.KERNEL_MIXED, "mixed_simt": L.KERNEL_MIXED_SIMT}[kernel]
         _call(L.lib().bgwx_generalized_bulk_flow_set_kernel(h, k))
+        # the backward of a forward on the same bubbles reads the forward's masks instead of
+        # searching again (when every frame's masks fit on the device)
+        _call(L.lib().bgwx_generalized_bulk_flow_set_keep_masks(h, bool(keep_masks)))
         self.last_forward_ms = 0.0
         self.last_backward_ms = 0.0
 

@@ -70,6 +70,9 @@ struct SpectrumJob {
     // mask search: the automatic number of blocks per (bubble, frame) times 1, 2 or 4 (0: 1);
     // finer direction ranges per block give shorter tails, coarser ones fewer list gathers
     int mask_chunking = 0;
+    // keep every frame's collision delays and first-collider codes on the device (when they fit in
+    // the mask budget) for a following adjoint call on the same bubbles, directions and grid
+    bool keep_masks = false;
     // Several realizations in one call (the batched ensemble, factored kernels): `bubbles` holds
     // them one after another (n_tot rows in all; n_int = n_tot), `sel` has one slot per radiating
     // bubble, padded so that each realization starts a GEMM column tile (padding slots hold

@@ -37,6 +37,7 @@ struct bgw_generalized_bulk_flow {
     // launch shape of spectrum calls: fixed (non-zero), measured (autotune) or automatic
     size_t frames_per_launch = 0, row_parts = 0, gemm_stages = 0, mask_chunking = 0;
     bool autotune = false;
+    bool keep_masks = false;  // spectrum calls keep their masks for a following adjoint call
     bgw::Device* dev = nullptr;
     BgwxTimings timings{};
     ~bgw_generalized_bulk_flow() {
@@ -178,6 +179,7 @@ bgw::SpectrumJob settings_job(const bgw_generalized_bulk_flow* h, const std::vec
     job.rot = rot;
     job.n_k = n_k;
     job.kernel = h->kernel;
+    job.keep_masks = h->keep_masks;
     return job;
 }
 
@@ -859,6 +861,10 @@ BgwStatus bgwx_generalized_bulk_flow_last_mask_chunking(const bgw_generalized_bu
         if (!out_chunking) throw Error{"outputs must not be null"};
         *out_chunking = bulk_flow->dev ? (size_t)bgw::last_launch_shape(bulk_flow->dev).mask_chunking : 0;
     });
+}
+
+BgwStatus bgwx_generalized_bulk_flow_set_keep_masks(bgw_generalized_bulk_flow* bulk_flow, bool enabled) {
+    return run_ffi([&] { handle(bulk_flow)->keep_masks = enabled; });
 }
 
 BgwStatus bgwx_generalized_bulk_flow_set_autotune(bgw_generalized_bulk_flow* bulk_flow, bool enabled) {

@@ -98,6 +98,11 @@ struct Device {
     bool last_factored = false;
     bool tc_atab_valid = false;  // tc_atab holds the current call's time-phase digits
     DevBuf adj_gbar, adj_scratch, adj_grad, adj_mtab; // adjoint: cotangents, work arrays, gradients, phases
+    // masks kept by a spectrum call for the adjoint: (K, n_sel, n_cos n_phi) delays and codes, and the
+    // inputs they were computed from (bubbles, rotations, selection, grid sizes)
+    DevBuf kept_tau, kept_codes;
+    std::vector<unsigned char> kept_key;
+    bool kept_valid = false;
     size_t last_frames_per_launch = 0;               // launch shape of the last spectrum call
     int last_row_parts = 0;
     int last_gemm_stages = 0;

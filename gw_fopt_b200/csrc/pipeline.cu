@@ -607,6 +607,22 @@ void run_masks(Device* dev, const MaskJob& job, int32_t* out_codes, double* out_
     }
 }
 
+// The inputs the masks of a job depend on: bubbles, frame rotations, radiating selection, interior
+// count and angular grid (the direction table follows from the grid).
+static std::vector<unsigned char> masks_key(const SpectrumJob& job) {
+    std::vector<unsigned char> k;
+    auto put = [&](const void* p, size_t bytes) {
+        const unsigned char* b = static_cast<const unsigned char*>(p);
+        k.insert(k.end(), b, b + bytes);
+    };
+    const size_t sizes[6] = {job.n_int, job.n_tot, job.n_sel, job.n_cos, job.n_phi, job.rot ? job.n_k : 0};
+    put(sizes, sizeof sizes);
+    put(job.bubbles, 4 * job.n_tot * sizeof(double));
+    put(job.sel, job.n_sel * sizeof(uint32_t));
+    if (job.rot) put(job.rot, 9 * job.n_k * sizeof(double));
+    return k;
+}
+
 // Per-stage device times of the last run_spectrum's launch chunks (masks, then
 // spectrum = beta + GEMM for the factored kernels), once its work is complete.
 static void add_stage_times(Device* dev, BgwxTimings* tm) {
@@ -684,7 +700,16 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
     dev->last_row_parts = job.kernel == BGWX_KERNEL_FP64_DIRECT ? 1 : 0;  // the factored launch records its own
     dev->last_gemm_stages = 0;
     dev->last_mask_chunking = job.mask_chunking > 0 ? job.mask_chunking : 1;
-    dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
+    // masks kept for an adjoint call: every frame's delays and codes, written in place
+    const bool keep = job.keep_masks && !batched && !job.tensor &&
+                      K * job.n_sel * nd * (sizeof(double) + sizeof(int32_t)) <= mask_budget_bytes();
+    if (keep) {
+        dev->kept_valid = false;
+        dev->kept_tau.ensure(K * job.n_sel * nd * sizeof(double));
+        dev->kept_codes.ensure(K * job.n_sel * nd * sizeof(int32_t));
+    } else {
+        dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
+    }
     if (job.kernel == BGWX_KERNEL_FP64_DIRECT) dev->partial.ensure(kc * job.n_sel * per * sizeof(double2));
     double2* final_out = out_is_device ? reinterpret_cast<double2*>(out) : nullptr;
     if (!final_out) {
@@ -737,8 +762,10 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             fb = (const D4*)dev->bubrot.p;
         }
         record_event(dev, cev[0]);
+        double* tau_k = keep ? (double*)dev->kept_tau.p + k0 * job.n_sel * nd : (double*)dev->tau.p;
+        int32_t* codes_k = keep ? (int32_t*)dev->kept_codes.p + k0 * job.n_sel * nd : nullptr;
         launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, ranges, job.n_sel, dirs, nd, job.n_phi, kn,
-                             (double*)dev->tau.p, nullptr, (unsigned long long*)dev->counters.p, k0 == 0, &launches,
+                             tau_k, codes_k, (unsigned long long*)dev->counters.p, k0 == 0, &launches,
                              job.mask_chunking);
         record_event(dev, cev[1]);
         if (job.kernel == BGWX_KERNEL_FP64_DIRECT) {
@@ -747,7 +774,7 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             A.n_tot = job.n_tot;
             A.sel = sel;
             A.n_sel = job.n_sel;
-            A.tau = (const double*)dev->tau.p;
+            A.tau = tau_k;
             A.n_cos = (int)job.n_cos;
             A.n_phi = (int)job.n_phi;
             A.cos_thetax = cos_t;
@@ -783,12 +810,16 @@ void run_spectrum(Device* dev, const SpectrumJob& job, double* out, bool out_is_
             CUDA_OK(cudaGetLastError());
             ++launches;
         } else {
-            launches += launch_factored(dev, job, fb, sel, (const double*)dev->tau.p, cos_t, sin2, cos2, coeffs,
+            launches += launch_factored(dev, job, fb, sel, tau_k, cos_t, sin2, cos2, coeffs,
                                         powers, t_arr, cutw, w, k0, kn, final_out, real_tiles, &dev->fact_ev[3 * ci]);
         }
         record_event(dev, cev[2]);
     }
     record_event(dev, dev->ev[5]);
+    if (keep) {
+        dev->kept_key = masks_key(job);
+        dev->kept_valid = true;
+    }
     dev->last_n_chunks = n_chunks;
     dev->last_factored = job.kernel != BGWX_KERNEL_FP64_DIRECT;
     if (out_is_device) {
@@ -1004,8 +1035,13 @@ void run_adjoint(Device* dev, const SpectrumJob& job, const double* gbar, double
     size_t kc = std::max<size_t>(1, std::min(K, mask_budget_bytes() / std::max<size_t>(per_k, 1)));
     kc = std::min<size_t>(kc, 65535);
     const size_t rows = job.n_sel * job.n_cos;
-    dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
-    dev->codes.ensure(kc * job.n_sel * nd * sizeof(int32_t));
+    // the masks kept by the last spectrum call on the same inputs are reused (same stream, so that
+    // call's kernels have finished before this call's read them)
+    const bool reuse = dev->kept_valid && dev->kept_key == masks_key(job);
+    if (!reuse) {
+        dev->tau.ensure(kc * job.n_sel * nd * sizeof(double));
+        dev->codes.ensure(kc * job.n_sel * nd * sizeof(int32_t));
+    }
     // the fixed-point gradient sums of a chunk hold fewer than 2^31 contributions
     const size_t per_frame_contrib = 2 * job.n_sel * nd + job.n_sel;
     kc = std::max<size_t>(1, std::min(kc, ((size_t)1 << 31) / std::max<size_t>(per_frame_contrib, 1)));
@@ -1046,9 +1082,14 @@ void run_adjoint(Device* dev, const SpectrumJob& job, const double* gbar, double
             ++launches;
             fb = (const D4*)dev->bubrot.p;
         }
-        launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, nullptr, job.n_sel, dirs, nd, job.n_phi, kn, (double*)dev->tau.p,
-                             (int32_t*)dev->codes.p, (unsigned long long*)dev->counters.p, k0 == 0, &launches);
-        launches += launch_adjoint_chunk(dev, job, fb, sel, (const double*)dev->tau.p, (const int32_t*)dev->codes.p,
+        const double* tau_k = reuse ? (const double*)dev->kept_tau.p + k0 * job.n_sel * nd : (const double*)dev->tau.p;
+        const int32_t* codes_k =
+            reuse ? (const int32_t*)dev->kept_codes.p + k0 * job.n_sel * nd : (const int32_t*)dev->codes.p;
+        if (!reuse)
+            launch_mask_pipeline(dev, bub, fb, job.n_int, job.n_tot, sel, nullptr, job.n_sel, dirs, nd, job.n_phi, kn,
+                                 (double*)dev->tau.p, (int32_t*)dev->codes.p, (unsigned long long*)dev->counters.p,
+                                 k0 == 0, &launches);
+        launches += launch_adjoint_chunk(dev, job, fb, sel, tau_k, codes_k,
                                          dirs, cos_t, sin2, cos2, coeffs, powers, t_arr, cutw, w,
                                          rot ? rot + 9 * k0 : nullptr, gb + k0 * per, kn, sc, mt, tt, d_gbub,
                                          d_gpar);

@@ -146,6 +146,14 @@ BgwStatus bgwx_generalized_bulk_flow_set_mask_chunking(bgw_generalized_bulk_flow
 BgwStatus bgwx_generalized_bulk_flow_last_mask_chunking(const bgw_generalized_bulk_flow *bulk_flow,
                                                         size_t *out_chunking);
 
+/* With `enabled`, each k-hat spectrum call keeps every frame's collision
+ * delays and first-collider codes on the device (when they fit in a third of
+ * the free device memory), and a following
+ * bgwx_generalized_bulk_flow_spectrum_vjp on the same bubbles, selection,
+ * directions and grid reads them instead of searching again.  The gradients
+ * are the same bits either way.  No counterpart in the reference. */
+BgwStatus bgwx_generalized_bulk_flow_set_keep_masks(bgw_generalized_bulk_flow *bulk_flow, bool enabled);
+
 /* First-collider codes (-1 None, i Interior(i), -(i+2) Exterior(i)) and the
  * collision delays of compute_delta_tab for interior bubbles [a_begin, a_end)
  * at k-hat = z, computed on the GPU.  out_codes: (a_end-a_begin, n_cos, n_phi)

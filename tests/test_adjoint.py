@@ -291,3 +291,33 @@ def test_mixed_adjoint_vs_fp64_adjoint_and_fd(gpu_available):
         fd = (f(**p) - f(**q)) / (2 * H)
         an = float(getattr(fit, name).grad)
         assert abs(fd - an) <= FD_TOL * abs(fd), (name, fd, an)
+
+
+@pytest.mark.gpu
+def test_kept_masks_give_the_same_gradients(gpu_available):
+    """A backward after a forward on the same bubbles reads the forward's masks (keep_masks): the
+    gradients are the same bits as with the masks searched again, and after the bubbles move the
+    kept masks no longer match and are not used."""
+    c = small_case(seed=9, n=8)
+    c["n_cos"], c["n_phi"], c["n_t"] = 16, 16, 64
+    c["w"] = np.geomspace(1.0, 200.0, 12)
+    c["kh"] = W.fibonacci_khat(3)
+    co = np.array([[1.0, 0.3]])
+    po = np.array([[5.0, 3.5]])
+    rng = np.random.default_rng(4)
+    G = rng.normal(size=(3, 2, 1, 12)) + 1j * rng.normal(size=(3, 2, 1, 12))
+    for kernel in ("fp64_factored", "mixed"):
+        fresh = _library_model(c, kernel=kernel)
+        ref = fresh.vjp(co, po, c["inter"], G)
+        kept = _library_model(c, kernel=kernel)
+        kept._forward(co, po, c["inter"])
+        got = kept.vjp(co, po, c["inter"], G)
+        for g_, r_ in zip(got, ref):
+            np.testing.assert_array_equal(g_, r_)
+        moved = c["inter"].copy()
+        moved[:, 1] += 1e-3
+        kept._forward(co, po, c["inter"])
+        got2 = kept.vjp(co, po, moved, G)
+        ref2 = _library_model(c, kernel=kernel).vjp(co, po, moved, G)
+        for g_, r_ in zip(got2, ref2):
+            np.testing.assert_array_equal(g_, r_)
