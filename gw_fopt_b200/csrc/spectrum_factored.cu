@@ -647,7 +647,8 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
         if (lane == 0) A.scale[row] = vmax;
         const double inv = vmax > 0.0 ? 1.0 / vmax : 0.0;
         const double rinv = rf * inv;
-        // digits.  Event blocks: lane = step; a quad of lanes transposes its packed digit
+        // digits (streaming stores: the GEMM reads them back from DRAM).  Event blocks: lane = step; a
+        // quad of lanes transposes its packed digit
         // words so that lane 4q + d holds digit d of steps 4q .. 4q + 3.  Blocks without
         // events: 4 steps per lane (8 lanes a block, 4 blocks at a time), transposed in
         // registers.  Either way a store instruction fills whole 32-byte rows of the blocks.
@@ -682,8 +683,8 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
                     }
                     const uint32_t wc = quad_transpose(i8_digits(xc * inv));
                     const uint32_t ws = quad_transpose(i8_digits(xs * inv));
-                    *reinterpret_cast<uint32_t*>(blk + i8_swz(nbase + 2 * s2, s4)) = wc;
-                    *reinterpret_cast<uint32_t*>(blk + i8_swz(nbase + 2 * s2 + 1, s4)) = ws;
+                    __stcs(reinterpret_cast<unsigned int*>(blk + i8_swz(nbase + 2 * s2, s4)), wc);
+                    __stcs(reinterpret_cast<unsigned int*>(blk + i8_swz(nbase + 2 * s2 + 1, s4)), ws);
                 }
             }
             const int sub = lane >> 3, s0 = (lane & 7) * 4;
@@ -743,8 +744,8 @@ __global__ void __launch_bounds__(256, std::is_same<Real, int8_t>::value ? 3 : 1
                     const int oc = i8_swz(nbase + 2 * s2, s0), os = i8_swz(nbase + 2 * s2 + 1, s0);
 #pragma unroll
                     for (int d = 0; d < kI8Slices; ++d) {
-                        *reinterpret_cast<uint32_t*>(blk + d * kI8Block + oc) = wc[d];
-                        *reinterpret_cast<uint32_t*>(blk + d * kI8Block + os) = ws[d];
+                        __stcs(reinterpret_cast<unsigned int*>(blk + d * kI8Block + oc), wc[d]);
+                        __stcs(reinterpret_cast<unsigned int*>(blk + d * kI8Block + os), ws[d]);
                     }
                 }
             }
