@@ -372,7 +372,9 @@ __global__ void __launch_bounds__(kMaskListThreads)
     const size_t d_begin = r_begin * row_len, d_end = r_end * row_len;
     const int lane = threadIdx.x & 31;
     constexpr int kBatch = 2;
-    constexpr int kRowsPerItem = 8;  // rows walked by a warp in one strip item
+    // rows walked by a warp in one strip item; an item's first row has no seed, so longer items miss
+    // fewer seeds (16 rows with 8192-direction blocks: 5 % faster than 8 rows with 4096)
+    constexpr int kRowsPerItem = 16;
     const D4* B = bub + (size_t)k * n_tot;  // frame k
     uint32_t a = sel[slot];
     const NbList* L = lists + slot;
@@ -680,12 +682,13 @@ __global__ void __launch_bounds__(kMaskListThreads)
     if (n_full) atomicAdd(counters, n_full);
 }
 
-// Blocks per radiating bubble and frame: whole rows of about four thousand
-// directions per block amortise the list gather; ranges shrink (to one row at
-// least) when there are too few blocks to fill the GPU.
+// Blocks per radiating bubble and frame: whole rows of about eight thousand
+// directions per block amortise the list gather and keep the seed chains long;
+// ranges shrink (to one row at least) when there are too few blocks to fill the
+// GPU.
 static unsigned mask_split(size_t nd, size_t row_len, size_t n_pairs) {
     const size_t n_rows = nd / row_len;
-    size_t rpb = std::max<size_t>(1, 4096 / row_len);
+    size_t rpb = std::max<size_t>(1, 8192 / row_len);
     size_t split = (n_rows + rpb - 1) / rpb;
     const size_t want = 148 * 16;  // blocks for about four waves of resident blocks
     while (split * n_pairs < want && split * 2 <= n_rows) split *= 2;
